@@ -1,0 +1,460 @@
+/*
+ * CPU oracle for the delta-encoded Ising anneal path.  TEST INFRASTRUCTURE ONLY:
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg call this file as the
+ * checker (and as the timed CPU restatement).  The product path never links it.
+ *
+ * Every function restates a reference algorithm in plain C, with the reference file:line
+ * it follows.  Paths are relative to the reference project root (skethz/Arpeggio).
+ *
+ *  orc_philox_batch  Philox4x32-10 (Salmon et al., SC'11), as arpeggio/mimo/chordfx.py:39-49
+ *                    and arpeggio/rtl/cycle_checks/rtl_a59/src/arpeggio_ref59.py:14-21.
+ *  orc_anneal_dd     integer anneal on the compressed dDI coupling G (D x D):
+ *                    policy 0 = first accept (arpeggio_ref59.py:41-85 mode 'arpeggio',
+ *                    the contract of arpeggio/sim/arpeggio_fx.cu:35-100), policy 1 = Chord's
+ *                    snapshot round (arpeggio_ref59.py:72-82 mode 'par', plus the Onsager term
+ *                    of arpeggio/mimo/chordfx.py:105).
+ *  orc_anneal_chord  Chord on a full N x N int16 coupling: arpeggio/mimo/chordfx.py:80-118
+ *                    (chord_fx), modes 'chains' and 'best'.
+ *  orc_anneal_dd_f32 the same two policies with FP32 fields (no reference kernel exists; the
+ *                    rule is the integer rule of arpeggio_ref59.py:62 with the float decision
+ *                    of arpeggio/sim/arpx55.py:65, written out operation by operation below).
+ *
+ * Parity pins: tests/golden (KATs of chordfx.py:53-56, outputs of arpeggio_ref59.anneal and
+ * chordfx.chord_fx produced by importing the reference, generator committed beside them).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_M0 0xD2511F53u
+#define ORC_M1 0xCD9E8D57u
+#define ORC_W0 0x9E3779B9u
+#define ORC_W1 0xBB67AE85u
+
+static void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int i = 0; i < 10; i++) {
+    if (i) {
+      k0 += ORC_W0;
+      k1 += ORC_W1;
+    }
+    uint64_t p0 = (uint64_t)ORC_M0 * c[0];
+    uint64_t p1 = (uint64_t)ORC_M1 * c[2];
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+    uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+    c[1] = (uint32_t)p1;
+    c[3] = (uint32_t)p0;
+    c[0] = n0;
+    c[2] = n2;
+  }
+}
+
+static uint32_t philox_word(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
+                            int w) {
+  uint32_t c[4] = {c0, c1, c2, c3};
+  philox10(c, k0, k1);
+  return c[w];
+}
+
+/* in: n x 6 words (counter c0..c3, key k0, k1) -> out: n x 4 words. */
+int orc_philox_batch(const uint32_t* in, uint32_t* out, int n) {
+  for (int t = 0; t < n; t++) {
+    uint32_t c[4] = {in[6 * t], in[6 * t + 1], in[6 * t + 2], in[6 * t + 3]};
+    philox10(c, in[6 * t + 4], in[6 * t + 5]);
+    memcpy(out + 4 * t, c, sizeof c);
+  }
+  return 0;
+}
+
+/* The i-th P-bit word with P/2 ones, counted in increasing order (arpeggio_ref59.py:31-38). */
+static int bal_pat(int P, uint32_t i) {
+  uint32_t n = 0;
+  for (int v = 0; v < (1 << P); v++)
+    if (__builtin_popcount(v) == P / 2) {
+      if (n == i) return v;
+      n++;
+    }
+  return 0;
+}
+
+static int bal_count(int P) { return P == 2 ? 2 : (P == 4 ? 6 : 20); }
+
+/* ------------------------------------------------------------------ thread pool over anneals */
+typedef void (*orc_job_fn)(void* ctx, long idx);
+typedef struct {
+  orc_job_fn fn;
+  void* ctx;
+  long n;
+  long next;
+  pthread_mutex_t mu;
+} orc_pool;
+
+static void* orc_worker(void* a) {
+  orc_pool* p = (orc_pool*)a;
+  for (;;) {
+    pthread_mutex_lock(&p->mu);
+    long i = p->next++;
+    pthread_mutex_unlock(&p->mu);
+    if (i >= p->n) break;
+    p->fn(p->ctx, i);
+  }
+  return NULL;
+}
+
+static void orc_run(orc_job_fn fn, void* ctx, long n, int nthreads) {
+  if (nthreads <= 1 || n <= 1) {
+    for (long i = 0; i < n; i++) fn(ctx, i);
+    return;
+  }
+  orc_pool p = {fn, ctx, n, 0, PTHREAD_MUTEX_INITIALIZER};
+  pthread_t th[256];
+  if (nthreads > 256) nthreads = 256;
+  for (int t = 0; t < nthreads; t++) pthread_create(&th[t], NULL, orc_worker, &p);
+  for (int t = 0; t < nthreads; t++) pthread_join(th[t], NULL);
+}
+
+/* ------------------------------------------------------------------ integer anneal, compressed G */
+typedef struct {
+  const int32_t *G, *h, *T, *c;
+  int B, D, P, R, L;
+  int32_t q;
+  const uint32_t* inst;
+  uint32_t k0, k1;
+  int start, policy;
+  int8_t* out_s;
+  int64_t *out_de, *out_st;
+} dd_ctx;
+
+/* Start spins of one anneal (arpeggio_ref59.py:44-49, arpeggio_fx.cu:48-57). s is P x D. */
+static void start_spins(int start, int P, int D, uint32_t r, uint32_t inst, uint32_t k0, uint32_t k1,
+                        int8_t* s) {
+  if (start == 0) {
+    for (int p = 0; p < P; p++)
+      for (int j = 0; j < D; j++)
+        s[p * D + j] = philox_word(0xFFFFFFFFu, (uint32_t)(p * D + j), r, inst, k0, k1, 0) >= 0x80000000u ? 1 : -1;
+  } else {
+    uint64_t C = (uint64_t)bal_count(P);
+    for (int j = 0; j < D; j++) {
+      uint32_t w0 = philox_word(0xFFFFFFFFu, (uint32_t)j, r, inst, k0, k1, 0);
+      int pat = bal_pat(P, (uint32_t)(((uint64_t)w0 * C) >> 32));
+      for (int p = 0; p < P; p++) s[p * D + j] = ((pat >> p) & 1) ? 1 : -1;
+    }
+  }
+}
+
+static void dd_job(void* vctx, long t) {
+  const dd_ctx* x = (const dd_ctx*)vctx;
+  const int D = x->D, P = x->P, R = x->R;
+  const long b = t / R;
+  const uint32_t r = (uint32_t)(t % R), inst = x->inst[b];
+  const int32_t* G = x->G + (size_t)b * D * D; /* G[i * D + j] */
+  const int32_t* h = x->h + (size_t)b * D;
+  int8_t s[6 * 128], bs[6 * 128];
+  uint8_t pf[6 * 128];
+  int64_t w[128];
+  uint8_t F[128];
+  start_spins(x->start, P, D, r, inst, x->k0, x->k1, s);
+  memcpy(bs, s, (size_t)P * D);
+  memset(pf, 0, sizeof pf);
+  for (int i = 0; i < D; i++) { /* w_i = h_i - 2 sum_j G_ij m_j (arpeggio_ref59.py:50-51) */
+    int64_t acc = 0;
+    for (int j = 0; j < D; j++) {
+      int m = 0;
+      for (int p = 0; p < P; p++) m += s[p * D + j];
+      acc += (int64_t)G[i * D + j] * m;
+    }
+    w[i] = h[i] - 2 * acc;
+  }
+  int64_t de = 0, best = (int64_t)1 << 62, flips = 0, tests = 0;
+  for (int k = 0; k < x->L; k++) {
+    const int p = k % P;
+    const uint32_t n = (uint32_t)(k / P);
+    const __int128 A = (__int128)4 * x->T[k];
+    const int64_t Bk = (int64_t)x->q + 2 * (int64_t)x->T[k];
+    int8_t* sp = s + p * D;
+    if (x->policy == 0) { /* first accept: a flip updates every field before the next lane (:59-71) */
+      int64_t tt = 1;
+      for (int j = 0; j < D; j++) {
+        uint32_t u = philox_word(n >> 2, (uint32_t)(p * D + j), r, inst, x->k0, x->k1, (int)(n & 3));
+        int64_t dj = G[j * D + j];
+        __int128 lhs = (__int128)u * A;
+        __int128 rhs = ((__int128)sp[j] * w[j] + 2 * (__int128)dj + Bk) * ((__int128)1 << 32);
+        if (lhs > rhs) {
+          int so = sp[j];
+          de += 4 * (int64_t)so * w[j] + 8 * dj;
+          for (int i = 0; i < D; i++) w[i] += 4 * (int64_t)so * G[i * D + j];
+          sp[j] = (int8_t)(-so);
+          flips++;
+          if (j < D - 1) tt++;
+        }
+      }
+      tests += tt;
+    } else { /* Chord's round: every lane tests the snapshot, then the flips commit in order (:72-82) */
+      const int64_t ck = x->c ? (int64_t)x->c[k] : 0;
+      for (int j = 0; j < D; j++) {
+        uint32_t u = philox_word(n >> 2, (uint32_t)(p * D + j), r, inst, x->k0, x->k1, (int)(n & 3));
+        int64_t dj = G[j * D + j];
+        int64_t sgn = pf[p * D + j] ? -1 : 1;
+        __int128 lhs = (__int128)u * A;
+        __int128 rhs = ((__int128)sp[j] * w[j] + 2 * (__int128)dj + Bk - ck * sgn) * ((__int128)1 << 32);
+        F[j] = lhs > rhs;
+      }
+      memset(pf, 0, (size_t)P * D);
+      for (int j = 0; j < D; j++) {
+        if (!F[j]) continue;
+        int so = sp[j];
+        int64_t dj = G[j * D + j];
+        de += 4 * (int64_t)so * w[j] + 8 * dj;
+        for (int i = 0; i < D; i++) w[i] += 4 * (int64_t)so * G[i * D + j];
+        sp[j] = (int8_t)(-so);
+        pf[p * D + j] = 1;
+        flips++;
+      }
+      tests += 1;
+    }
+    if (de < best) { /* best state after each pass (:83-84) */
+      best = de;
+      memcpy(bs, s, (size_t)P * D);
+    }
+  }
+  memcpy(x->out_s + (size_t)t * P * D, bs, (size_t)P * D);
+  x->out_de[t] = best;
+  x->out_st[2 * t] = flips;
+  x->out_st[2 * t + 1] = tests;
+}
+
+/* G (B, D, D) row-major G[b][i][j]; h (B, D); T (L) one temperature per pass (pass k tests copy k % P);
+ * c (L) Onsager terms or NULL (policy 1 only); start 0 = 'rand', 1 = 'bal'; policy 0 = first accept,
+ * 1 = Chord round.  Outputs: best spins (B, R, P*D) copy-major, best energy change (B, R), and
+ * (flips, tests) per anneal (B, R, 2). */
+int orc_anneal_dd(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T,
+                  const int32_t* c, int L, int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1, int start,
+                  int policy, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
+  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
+    return 1;
+  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st};
+  orc_run(dd_job, &x, (long)B * R, nthreads);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ Chord on a full int16 J (chord_fx) */
+typedef struct {
+  const int16_t* J;
+  const int32_t *h, *h0, *T, *c;
+  int q, S, P, R, N, B;
+  uint32_t k0, k1, inst0;
+  int64_t* e_all;  /* (B, R) */
+  int8_t* s_all;   /* (B, R, N) */
+} ch_ctx;
+
+static void ch_job(void* vctx, long t) {
+  const ch_ctx* x = (const ch_ctx*)vctx;
+  const int N = x->N, P = x->P, R = x->R;
+  const long b = t / R;
+  const uint32_t r = (uint32_t)(t % R), m = x->inst0 + (uint32_t)b;
+  const int16_t* J = x->J + (size_t)b * N * N;
+  const int32_t* h = x->h + (size_t)b * N;
+  const int32_t* h0 = x->h0 + (size_t)b * N;
+  int8_t s[256], bs[256], pf[256], fl[256];
+  int64_t u[256];
+  for (int i = 0; i < N; i++) /* start (chordfx.py:93-94) */
+    s[i] = philox_word(0xFFFFFFFFu, (uint32_t)i, r, m, x->k0, x->k1, 0) >= 0x80000000u ? 1 : -1;
+  for (int i = 0; i < N; i++) { /* u = h + 2 J s (:95-96), row i of J */
+    int64_t acc = 0;
+    for (int j = 0; j < N; j++) acc += (int64_t)J[i * N + j] * s[j];
+    u[i] = h[i] + 2 * acc;
+  }
+  memset(pf, 0, sizeof pf);
+  memcpy(bs, s, (size_t)N);
+  int64_t best = (int64_t)1 << 62;
+  const int per = N / P;
+  for (int k = 0; k < x->S; k++) {
+    const int p = k % P, n = k / P;
+    const __int128 A = (__int128)4 * x->T[k];
+    for (int i = 0; i < N; i++) { /* decision (:104-106) */
+      uint32_t xr = philox_word((uint32_t)(n / 4), (uint32_t)i, r, m, x->k0, x->k1, n % 4);
+      int64_t z = (int64_t)s[i] * u[i] + x->q - (int64_t)x->c[k] * (pf[i] ? -1 : 1);
+      fl[i] = ((__int128)xr * A > ((__int128)z + 2 * (__int128)x->T[k]) * ((__int128)1 << 32)) && (i / per == p);
+    }
+    for (int i = 0; i < N; i++) { /* s flips; u = h + 2 J s follows exactly by column updates */
+      pf[i] = fl[i];
+      if (!fl[i]) continue;
+      int so = s[i];
+      s[i] = (int8_t)(-so);
+      for (int a = 0; a < N; a++) u[a] -= 4 * (int64_t)so * J[a * N + i];
+    }
+    int64_t e = 0; /* 2 E0 = sum s (h - 2 h0 - u) (:110) */
+    for (int i = 0; i < N; i++) e += (int64_t)s[i] * ((int64_t)h[i] - 2 * (int64_t)h0[i] - u[i]);
+    if (e < best) {
+      best = e;
+      memcpy(bs, s, (size_t)N);
+    }
+  }
+  x->e_all[t] = best;
+  memcpy(x->s_all + (size_t)t * N, bs, (size_t)N);
+}
+
+/* Contract of chordfx.chord_fx (arpeggio/mimo/chordfx.py:80-118).  mode 0 ('chains'): out_e (B, R),
+ * out_s (B, R, N); mode 1 ('best'): the first anneal with the lowest energy, out_e (B), out_s (B, N). */
+int orc_anneal_chord(const int16_t* J, const int32_t* h, const int32_t* h0, const int32_t* T, const int32_t* c,
+                     int q, int S, int P, int R, int N, int B, uint32_t k0, uint32_t k1, uint32_t inst0, int mode,
+                     int64_t* out_e, int8_t* out_s, int nthreads) {
+  if (N < 1 || N > 256 || P < 1 || N % P || S < 1 || R < 1) return 1;
+  int64_t* e_all = out_e;
+  int8_t* s_all = out_s;
+  if (mode == 1) {
+    e_all = (int64_t*)malloc(sizeof(int64_t) * (size_t)B * R);
+    s_all = (int8_t*)malloc((size_t)B * R * N);
+  }
+  ch_ctx x = {J, h, h0, T, c, q, S, P, R, N, B, k0, k1, inst0, e_all, s_all};
+  orc_run(ch_job, &x, (long)B * R, nthreads);
+  if (mode == 1) {
+    for (int b = 0; b < B; b++) {
+      int im = 0;
+      for (int r = 1; r < R; r++)
+        if (e_all[(size_t)b * R + r] < e_all[(size_t)b * R + im]) im = r;
+      out_e[b] = e_all[(size_t)b * R + im];
+      memcpy(out_s + (size_t)b * N, s_all + ((size_t)b * R + im) * N, (size_t)N);
+    }
+    free(e_all);
+    free(s_all);
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------ FP32 fields, compressed G */
+/* The float rule, one IEEE single operation per line (no contraction; compile with
+ * -ffp-contract=off):
+ *   rr   = (float)(x >> 8) * 2^-24                    exact, in [0, 1)
+ *   thr  = (rr - 0.5f) * (4 T_k)                      one rounding
+ *   z    = ((s * w_j) + 2 G_jj) + q_k                 two roundings (q_k = q - c_k sgn for Chord)
+ *   flip iff z < thr
+ *   de  += (4 s w_j) + 8 G_jj                         two roundings
+ *   w_i += (4 s) G_ij  (i = 0..D-1)                   one rounding each
+ * Fields start as w_i = h_i - 2 sum_j G_ij m_j, summed in j order. */
+typedef struct {
+  const float *G, *h, *T, *c;
+  int B, D, P, R, L;
+  float q;
+  const uint32_t* inst;
+  uint32_t k0, k1;
+  int start, policy;
+  int8_t* out_s;
+  float* out_de;
+  int64_t* out_st;
+} f32_ctx;
+
+static float orc_thr(uint32_t x, float A) {
+  volatile float rr = (float)(x >> 8) * 5.9604644775390625e-08f;
+  volatile float d = rr - 0.5f;
+  volatile float t = d * A;
+  return t;
+}
+
+static void f32_job(void* vctx, long t) {
+  const f32_ctx* x = (const f32_ctx*)vctx;
+  const int D = x->D, P = x->P, R = x->R;
+  const long b = t / R;
+  const uint32_t r = (uint32_t)(t % R), inst = x->inst[b];
+  const float* G = x->G + (size_t)b * D * D;
+  const float* h = x->h + (size_t)b * D;
+  int8_t s[6 * 128], bs[6 * 128];
+  uint8_t pf[6 * 128], F[128];
+  float w[128];
+  start_spins(x->start, P, D, r, inst, x->k0, x->k1, s);
+  memcpy(bs, s, (size_t)P * D);
+  memset(pf, 0, sizeof pf);
+  for (int i = 0; i < D; i++) {
+    volatile float acc = 0.0f;
+    for (int j = 0; j < D; j++) {
+      int m = 0;
+      for (int p = 0; p < P; p++) m += s[p * D + j];
+      volatile float prod = G[i * D + j] * (float)m; /* exact: |m| <= 6 */
+      acc = acc + prod;
+    }
+    volatile float two = 2.0f * acc;
+    w[i] = h[i] - two;
+  }
+  volatile float de = 0.0f;
+  float best = INFINITY;
+  int64_t flips = 0, tests = 0;
+  for (int k = 0; k < x->L; k++) {
+    const int p = k % P;
+    const uint32_t n = (uint32_t)(k / P);
+    const float A = 4.0f * x->T[k];
+    const float ck = (x->policy == 1 && x->c) ? x->c[k] : 0.0f;
+    int8_t* sp = s + p * D;
+    if (x->policy == 0) {
+      int64_t tt = 1;
+      for (int j = 0; j < D; j++) {
+        uint32_t u = philox_word(n >> 2, (uint32_t)(p * D + j), r, inst, x->k0, x->k1, (int)(n & 3));
+        float thr = orc_thr(u, A);
+        float g = G[j * D + j];
+        volatile float a = (float)sp[j] * w[j];
+        volatile float bb = a + 2.0f * g;
+        volatile float z = bb + x->q;
+        if (z < thr) {
+          int so = sp[j];
+          volatile float e1 = (float)(4 * so) * w[j];
+          volatile float e2 = e1 + 8.0f * g;
+          de = de + e2;
+          for (int i = 0; i < D; i++) {
+            volatile float inc = (float)(4 * so) * G[i * D + j];
+            w[i] = w[i] + inc;
+          }
+          sp[j] = (int8_t)(-so);
+          flips++;
+          if (j < D - 1) tt++;
+        }
+      }
+      tests += tt;
+    } else {
+      for (int j = 0; j < D; j++) {
+        uint32_t u = philox_word(n >> 2, (uint32_t)(p * D + j), r, inst, x->k0, x->k1, (int)(n & 3));
+        float thr = orc_thr(u, A);
+        float g = G[j * D + j];
+        volatile float qk = x->q - ck * (pf[p * D + j] ? -1.0f : 1.0f);
+        volatile float a = (float)sp[j] * w[j];
+        volatile float bb = a + 2.0f * g;
+        volatile float z = bb + qk;
+        F[j] = z < thr;
+      }
+      memset(pf, 0, (size_t)P * D);
+      for (int j = 0; j < D; j++) {
+        if (!F[j]) continue;
+        int so = sp[j];
+        float g = G[j * D + j];
+        volatile float e1 = (float)(4 * so) * w[j];
+        volatile float e2 = e1 + 8.0f * g;
+        de = de + e2;
+        for (int i = 0; i < D; i++) {
+          volatile float inc = (float)(4 * so) * G[i * D + j];
+          w[i] = w[i] + inc;
+        }
+        sp[j] = (int8_t)(-so);
+        pf[p * D + j] = 1;
+        flips++;
+      }
+      tests += 1;
+    }
+    if (de < best) {
+      best = de;
+      memcpy(bs, s, (size_t)P * D);
+    }
+  }
+  memcpy(x->out_s + (size_t)t * P * D, bs, (size_t)P * D);
+  x->out_de[t] = best;
+  x->out_st[2 * t] = flips;
+  x->out_st[2 * t + 1] = tests;
+}
+
+int orc_anneal_dd_f32(const float* G, const float* h, int B, int D, int P, int R, const float* T, const float* c,
+                      int L, float q, const uint32_t* inst, uint32_t k0, uint32_t k1, int start, int policy,
+                      int8_t* out_s, float* out_de, int64_t* out_st, int nthreads) {
+  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
+    return 1;
+  f32_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st};
+  orc_run(f32_job, &x, (long)B * R, nthreads);
+  return 0;
+}

@@ -1,0 +1,254 @@
+"""CPU oracle for the delta-encoded Ising MIMO detector path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module, and only
+as the checker (or as the timed CPU restatement of the reference's algorithm).  The product path
+(arpeggio_b200) never imports it and fails loudly when its CUDA library is missing.
+
+Two halves:
+  * ctypes bindings of arp_oracle.c (Philox4x32-10, integer and FP32 anneals, chord_fx);
+  * numpy restatements of the host-side mapping and readout of arpeggio/mimo/mimo.py and
+    arpeggio/mimo/chordfx.py, each citing the reference function it follows.
+
+Parity pins: tests/golden/*.npz were produced by importing the reference itself
+(tests/golden/make_golden.py); tests/test_oracle_golden.py checks this module against them.
+"""
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, 'liboracle.so')
+MASK = 0xFFFFFFFF
+QSCALE = 4096
+_lib = None
+
+_P = ctypes.c_void_p
+
+
+def build():
+    subprocess.check_call(['make', '-s', '-C', HERE], stdout=subprocess.DEVNULL)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, 'arp_oracle.c')):
+            build()
+        L = ctypes.CDLL(LIB)
+        L.orc_philox_batch.argtypes = [_P, _P, ctypes.c_int]
+        L.orc_anneal_dd.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
+                                    ctypes.c_int, ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                    ctypes.c_int, _P, _P, _P, ctypes.c_int]
+        L.orc_anneal_chord.argtypes = [_P, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.c_int, _P, _P, ctypes.c_int]
+        L.orc_anneal_dd_f32.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
+                                        ctypes.c_int, ctypes.c_float, _P, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+# ---------------------------------------------------------------- RNG
+def philox(words):
+    """words (n, 6) uint32: counter c0..c3, key k0, k1 -> (n, 4) uint32 (chordfx.py:39-49)."""
+    w = np.ascontiguousarray(np.asarray(words, dtype=np.uint64) & MASK, dtype=np.uint32)
+    out = np.zeros((w.shape[0], 4), dtype=np.uint32)
+    lib().orc_philox_batch(_ptr(w), _ptr(out), w.shape[0])
+    return out
+
+
+# ---------------------------------------------------------------- anneals
+def anneal_dd(G, h, P, R, T, q, inst, key, start, policy='arpeggio', c=None, nthreads=1):
+    """Integer anneal on the compressed dDI problem; contract of arpeggiofx.solve
+    (arpeggio/sim/arpeggiofx.py:22-44) and arpeggio_ref59.anneal (rtl_a59/src/arpeggio_ref59.py:41-85).
+    Returns spins (B, R, P*D) int8 copy-major, best energy change (B, R) int64, (B, R, 2) [flips, tests]."""
+    G = np.ascontiguousarray(G, dtype=np.int32)
+    h = np.ascontiguousarray(h, dtype=np.int32)
+    B, D, _ = G.shape
+    T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
+    cc = None if c is None else np.ascontiguousarray([int(x) for x in c], dtype=np.int32)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    out_s = np.zeros((B, R, P * D), dtype=np.int8)
+    out_de = np.zeros((B, R), dtype=np.int64)
+    out_st = np.zeros((B, R, 2), dtype=np.int64)
+    rc = lib().orc_anneal_dd(_ptr(G), _ptr(h), B, D, P, R, _ptr(T), _ptr(cc), len(T), int(q), _ptr(it),
+                             key & MASK, (key >> 32) & MASK, 0 if start == 'rand' else 1,
+                             0 if policy == 'arpeggio' else 1, _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_dd: unsupported shape')
+    return out_s, out_de, out_st
+
+
+def anneal_dd_f32(G, h, P, R, T, q, inst, key, start, policy='arpeggio', c=None, nthreads=1):
+    """FP32-field anneal on the compressed dDI problem (float rule written out in arp_oracle.c)."""
+    G = np.ascontiguousarray(G, dtype=np.float32)
+    h = np.ascontiguousarray(h, dtype=np.float32)
+    B, D, _ = G.shape
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    cc = None if c is None else np.ascontiguousarray(c, dtype=np.float32)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    out_s = np.zeros((B, R, P * D), dtype=np.int8)
+    out_de = np.zeros((B, R), dtype=np.float32)
+    out_st = np.zeros((B, R, 2), dtype=np.int64)
+    rc = lib().orc_anneal_dd_f32(_ptr(G), _ptr(h), B, D, P, R, _ptr(T), _ptr(cc), len(T), float(q), _ptr(it),
+                                 key & MASK, (key >> 32) & MASK, 0 if start == 'rand' else 1,
+                                 0 if policy == 'arpeggio' else 1, _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_dd_f32: unsupported shape')
+    return out_s, out_de, out_st
+
+
+def chord_fx(J, h, h0, T, c, q, S, P, R, seed, inst0=0, mode='chains', nthreads=1):
+    """chordfx.chord_fx (arpeggio/mimo/chordfx.py:80-118) on int16 J (B, N, N), int32 h/h0 (B, N).
+    Returns (spins int8 (B, R, N) or (B, N), 2 E0 int64 (B, R) or (B,))."""
+    J = np.ascontiguousarray(J, dtype=np.int16)
+    h = np.ascontiguousarray(h, dtype=np.int32)
+    h0 = np.ascontiguousarray(h0, dtype=np.int32)
+    B, N = h.shape
+    T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
+    c = np.ascontiguousarray([int(x) for x in c], dtype=np.int32)
+    if mode == 'best':
+        out_e = np.zeros(B, dtype=np.int64)
+        out_s = np.zeros((B, N), dtype=np.int8)
+    else:
+        out_e = np.zeros((B, R), dtype=np.int64)
+        out_s = np.zeros((B, R, N), dtype=np.int8)
+    rc = lib().orc_anneal_chord(_ptr(J), _ptr(h), _ptr(h0), _ptr(T), _ptr(c), int(q), int(S), P, R, N, B,
+                                seed & MASK, (seed >> 32) & MASK, inst0 & MASK, 1 if mode == 'best' else 0,
+                                _ptr(out_e), _ptr(out_s), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_chord: unsupported shape')
+    return out_s, out_e
+
+
+# ---------------------------------------------------------------- constellation (mimo.py:19-51)
+PAM = {4: dict(levels=[-1, 1], a=1 / math.sqrt(2), bits=1),
+       16: dict(levels=[-3, -1, 1, 3], a=1 / math.sqrt(10), bits=2)}
+
+
+def levels_to_bits(l, M):
+    """mimo.levels_to_bits (mimo.py:45-51): per dimension MSB first."""
+    l = np.asarray(l)
+    if M == 4:
+        return (l > 0).astype(np.int8)
+    b1 = (l > 0).astype(np.int8)
+    b2 = (np.abs(l) == 1).astype(np.int8)
+    return np.stack([b1, b2], -1).reshape(*l.shape[:-1], -1)
+
+
+def quantize_levels(z, M):
+    """mimo.quantize_levels (mimo.py:86-88): nearest level, first on ties."""
+    lv = np.asarray(PAM[M]['levels'], dtype=z.dtype)
+    return lv[np.abs(z[..., None] - lv).argmin(-1)]
+
+
+# ---------------------------------------------------------------- MMSE and dDI mapping (float64)
+def mmse(H, y, N0, M):
+    """mimo.mmse (mimo.py:98-109) and mimo._mu (:176-182) in float64: z, mu, hard guess x_q."""
+    H = np.asarray(H, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    lv = np.asarray(PAM[M]['levels'], dtype=np.float64)
+    el2 = float((lv ** 2).mean())
+    G = np.einsum('bki,bkj->bij', H, H)
+    D = G.shape[-1]
+    A = G + (N0 / 2) / el2 * np.eye(D)
+    z = np.linalg.solve(A, np.einsum('bki,bk->bi', H, y)[..., None])[..., 0]
+    mu = np.diagonal(np.linalg.solve(A, G), axis1=-2, axis2=-1)
+    return z, mu, quantize_levels(z / mu, M)
+
+
+def ising_delta_compressed(H, y, xg):
+    """mimo.ising_delta_at (mimo.py:506-523) for any K, in compressed form: the N x N coupling is
+    J = -offdiag(Q (x) 1 1^T) with Q = H^T H, so G = Q/scale and h = 2 H^T (y - H xg)/scale;
+    scale = max(|h|_inf, |Q|_inf) (every entry of Q, the diagonal included, is an off-diagonal
+    entry of J once K >= 1).  Returns float64 (G, h, scale)."""
+    H = np.asarray(H, dtype=np.float64)
+    yb = np.asarray(y, dtype=np.float64) - np.einsum('bij,bj->bi', H, np.asarray(xg, dtype=np.float64))
+    h = 2 * np.einsum('bij,bi->bj', H, yb)
+    Q = np.einsum('bki,bkj->bij', H, H)
+    scale = np.maximum(np.abs(h).max(-1), np.abs(Q).reshape(Q.shape[0], -1).max(-1))
+    scale = np.maximum(scale, 1e-12)
+    return Q / scale[:, None, None], h / scale[:, None], scale
+
+
+def geom(t0, t1, S):
+    """mimo.geom (mimo.py:199-201): float64 schedule rounded once to float32."""
+    k = np.arange(S, dtype=np.float64)
+    return (t0 * (t1 / t0) ** (k / max(1, S - 1))).astype(np.float32)
+
+
+def arpeggio_schedule(T0, T1, S, q, K, Q=QSCALE):
+    """run_a513.arpeggio_schedule (sim/local_code_a513/run_a513.py:83-87): S sweeps x P passes."""
+    Tsw = [int(round(float(v) * Q)) for v in geom(T0, T1, S).astype(np.float64)]
+    return [t for t in Tsw for _ in range(2 * K)], int(round(q * Q))
+
+
+def chord_schedule(S, t0, t1, q, kappa=0.0, ramp=True, Q=QSCALE):
+    """The schedule half of chordfx.to_fixed (chordfx.py:66-76): T, c (S,) int32 and q."""
+    T = geom(t0, t1, S).astype(np.float64)
+    rho = np.ones(S)
+    if ramp:
+        t = np.arange(S, dtype=np.float64)
+        rho = np.where(t >= 0.7 * S, (S - 1 - t) / max(1.0, S - 1 - 0.7 * S), 1.0)
+    c = np.zeros(S)
+    c[1:] = kappa * T[:-1] * rho[1:]
+    return (np.round(T * Q).astype(np.int32), np.round(c * Q).astype(np.int32), int(round(q * Q)))
+
+
+def quantize_compressed(Gf, hf, Q=QSCALE):
+    """chordfx.to_fixed + chord_ref.compress (chordfx.py:60-65, chord_ref.py:47-59) on the compressed
+    form: the symmetrised G rounded half-to-even (torch.round) to int16, h to int32."""
+    Gs = (Gf + np.swapaxes(Gf, 1, 2)) / 2
+    return np.round(Gs * Q).astype(np.int32), np.round(hf * Q).astype(np.int32)
+
+
+def expand(G, h, K):
+    """chord_ref.expand (chord_ref.py:62-69): compressed (G, h) -> int16 J (B, N, N), int32 h (B, N)."""
+    B, D, _ = G.shape
+    N = 2 * K * D
+    J = -np.tile(G, (1, 2 * K, 2 * K))
+    J[:, np.arange(N), np.arange(N)] = 0
+    return J.astype(np.int16), np.tile(h, (1, 2 * K)).astype(np.int32)
+
+
+# ---------------------------------------------------------------- readout (mimo.py:185-190, 416-431)
+def spins_to_levels_delta(S, xq, K, M):
+    S = np.asarray(S)
+    D = xq.shape[-1]
+    d = S.reshape(*S.shape[:-1], 2 * K, D).astype(np.int64).sum(-2)
+    lv = PAM[M]['levels']
+    return np.clip(xq[:, None, :] + d, lv[0], lv[-1])
+
+
+def dist(H, y, L):
+    """||y - H l||^2 for candidates L (B, C, D) (mimo.dist)."""
+    r = np.asarray(y, dtype=np.float64)[:, None, :] - np.einsum('bij,bkj->bki', np.asarray(H, dtype=np.float64), L)
+    return (r ** 2).sum(-1)
+
+
+def select(H, y, cand, guess):
+    """mimo.select (mimo.py:421-425): the lowest distance among the candidates and the guess."""
+    allc = np.concatenate([cand, guess[:, None, :]], 1)
+    d = dist(H, y, allc)
+    im = d.argmin(1)
+    return allc[np.arange(allc.shape[0]), im], d[np.arange(allc.shape[0]), im]
+
+
+def energy_dd(G, h, S, K):
+    """Ising energy E0 = -h0.s - s^T J s of dDI spins S (B, R, 2K D) in the compressed form:
+    E0 = -h.m + m^T G m - P tr(G), m = sum over copies (mimo.energy0, mimo.py:193-195). float64."""
+    G = np.asarray(G, dtype=np.float64)
+    h = np.asarray(h, dtype=np.float64)
+    B, D, _ = G.shape
+    P = 2 * K
+    m = np.asarray(S, dtype=np.float64).reshape(S.shape[0], S.shape[1], P, D).sum(2)
+    tr = np.trace(G, axis1=1, axis2=2)
+    return -(m * h[:, None]).sum(-1) + np.einsum('brj,bjk,brk->br', m, G, m) - P * tr[:, None]

@@ -1,0 +1,197 @@
+#!/usr/bin/env python3
+"""Generates the golden fixtures in this folder by importing the reference (skethz/Arpeggio) itself.
+
+Run in a container that has the reference tree (read-only; no bytecode is written there):
+    python tests/golden/make_golden.py /root/reference
+
+Fixtures (all small, numpy .npz):
+  golden_philox.npz   Random123 KATs (arpeggio/mimo/chordfx.py:53-56) and 256 further counter/key
+                      words pushed through chordfx.philox (chordfx.py:39-49).
+  golden_arpeggio.npz integer anneals on compressed dDI problems built by the reference's own chain
+                      (arpx.draw -> mimo.mmse -> mimo.ising_delta_at -> chordfx.to_fixed ->
+                      chord_ref.compress), answered by arpeggio_ref59.anneal
+                      (rtl/cycle_checks/rtl_a59/src/arpeggio_ref59.py:41-85), modes 'arpeggio' and 'par'.
+  golden_chord.npz    chordfx.chord_fx (chordfx.py:80-118) on the cases of arpeggio/mimo/test_kernel.py:213-221
+                      (CPU generator, fewer instances), modes 'chains' and 'best'.
+  golden_mapping.npz  the float chain: draws, MMSE guess, ising_delta_at scale, to_fixed/compress
+                      integers, spins_to_levels_delta, dist and select on fixed spin sets.
+"""
+import math
+import os
+import random
+import sys
+
+sys.dont_write_bytecode = True
+REF = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+OUT = os.path.dirname(os.path.abspath(__file__))
+for sub in ('arpeggio/mimo', 'arpeggio/sim', 'arpeggio/sim/x3model', 'arpeggio/sim/local_code_a513'):
+    sys.path.insert(0, os.path.join(REF, sub))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+torch.set_num_threads(4)
+import mimo  # noqa: E402
+import chordfx  # noqa: E402
+import chord_ref  # noqa: E402
+import arpx  # noqa: E402
+
+M64 = 0xFFFFFFFFFFFFFFFF
+
+
+def load_ref59():
+    """Exec-load arpeggio_ref59.py without its command-line tail, as gate_a513.load_ref does."""
+    path = os.path.join(REF, 'arpeggio/rtl/cycle_checks/rtl_a59/src/arpeggio_ref59.py')
+    src = open(path).read()
+    cut = src.index("\nif sys.argv[1] == 'gen':")
+    ns = {'__name__': 'arpeggio_ref59'}
+    exec(compile(src[:cut], path, 'exec'), ns)
+    return ns
+
+
+def philox_fixture():
+    kat_in = np.array([list(c) + list(k) for c, k, _ in chordfx.KAT], dtype=np.uint32)
+    kat_out = np.array([list(w) for _, _, w in chordfx.KAT], dtype=np.uint32)
+    rnd = np.random.default_rng(7).integers(0, 2 ** 32, size=(256, 6), dtype=np.uint64)
+    t = [torch.tensor(rnd[:, i].astype(np.int64)) for i in range(4)]
+    outs = []
+    for i in range(256):
+        o = chordfx.philox(*[x[i:i + 1] for x in t], int(rnd[i, 4]), int(rnd[i, 5]))
+        outs.append([int(v) for v in o])
+    np.savez_compressed(os.path.join(OUT, 'golden_philox.npz'), kat_in=kat_in, kat_out=kat_out,
+                        rnd_in=rnd.astype(np.uint32), rnd_out=np.array(outs, dtype=np.uint32))
+    print('philox: 3 KATs, 256 random words')
+
+
+def dd_problem(nt, snr, K, B, seed, bi=0, M=16):
+    """A batch of compressed integer dDI sub-problems from the reference's own chain, around the MMSE guess."""
+    b = arpx.draw(seed, snr, bi, B, nt, M, dev='cpu')
+    z, _, _ = mimo.mmse(b)
+    lm = mimo.quantize_levels(z / mimo._mu(b, z), M)
+    I = mimo.ising_delta_at(b, lm, K)
+    F = chordfx.to_fixed(I, 8 * 2 * K, 0.3, 0.3, 0.4, 0.0)
+    G, h = chord_ref.compress(F, K)
+    return G.numpy().astype(np.int32), h.numpy().astype(np.int32)
+
+
+def sched(S, T0, T1, q, K):
+    Q = chordfx.QSCALE
+    Tsw = [int(round(v * Q)) for v in mimo.geom(T0, T1, S, 'cpu').double().tolist()]
+    return [t for t in Tsw for _ in range(2 * K)], int(round(q * Q))
+
+
+def arpeggio_fixture():
+    ns = load_ref59()
+    rnd = random.Random(513)
+    cases = [  # name, (nt, snr, K, B, seed), R, (S, T0, T1, q), start, key, inst base
+        ('x16_K1_pick_rand', (16, 20.0, 1, 4, 9600), 3, (64, 0.1, 0.1, 0.0), 'rand', rnd.getrandbits(64), 0),
+        ('x16_K1_hot_bal', (16, 12.0, 1, 3, 9601), 2, (8, 1.2, 0.1, 0.2), 'bal', 0x1234567890ABCDEF, 2 ** 32 - 2),
+        ('x16_K2_pick_bal', (16, 20.0, 2, 3, 9602), 2, (16, 0.1, 0.1, 0.0), 'bal', rnd.getrandbits(64), 1000),
+        ('x16_K3_hot_rand', (16, 16.0, 3, 2, 9603), 2, (8, 1.2, 0.1, 0.2), 'rand', rnd.getrandbits(64), 3000),
+        ('x32_K1_pick_rand', (32, 22.0, 1, 3, 9604), 2, (32, 0.1, 0.1, 0.0), 'rand', rnd.getrandbits(64), 7),
+        ('x32_K2_hot_bal', (32, 14.0, 2, 2, 9605), 2, (6, 0.8, 0.1, 0.1), 'bal', rnd.getrandbits(64), 50),
+        ('x64_K1_pick_bal', (64, 22.0, 1, 2, 9606), 2, (16, 0.1, 0.1, 0.0), 'bal', rnd.getrandbits(64), 0),
+        ('x10_K1_ragged_rand', (10, 10.0, 1, 3, 9607), 3, (20, 0.6, 0.05, 0.1), 'rand', rnd.getrandbits(64), 11),
+        ('x50_K1_ragged_bal', (50, 18.0, 1, 2, 9608), 2, (8, 0.5, 0.1, 0.0), 'bal', rnd.getrandbits(64), 99),
+        ('x40_K3_ragged_rand', (40, 20.0, 3, 1, 9609), 2, (3, 0.3, 0.1, 0.0), 'rand', rnd.getrandbits(64), 5),
+    ]
+    out = {}
+    for name, (nt, snr, K, B, seed), R, (S, T0, T1, q), start, key, ib in cases:
+        G, h = dd_problem(nt, snr, K, B, seed)
+        P = 2 * K
+        D = G.shape[1]
+        T, qi = sched(S, T0, T1, q, K)
+        inst = np.array([(ib + b) & 0xFFFFFFFF for b in range(B)], dtype=np.int64)
+        ns['SEED'] = key
+        for mode in ('arpeggio', 'par'):
+            sp = np.zeros((B, R, P * D), dtype=np.int8)
+            de = np.zeros((B, R), dtype=np.int64)
+            st = np.zeros((B, R, 2), dtype=np.int64)
+            for b in range(B):
+                Gl, hl = [[int(v) for v in row] for row in G[b]], [int(v) for v in h[b]]
+                for r in range(R):
+                    a = ns['anneal'](Gl, hl, P, T, qi, r, int(inst[b]), start, mode)
+                    for p in range(P):
+                        bits = a['bs'][p]
+                        for j in range(D):
+                            sp[b, r, p * D + j] = 1 if bits[D - 1 - j] == '1' else -1
+                    de[b, r] = a['best']
+                    st[b, r, 0] = len(a['acc'])
+                    st[b, r, 1] = sum(a['tests'])
+            k = '%s/%s' % (name, mode)
+            out[k + '/spins'], out[k + '/de'], out[k + '/st'] = sp, de, st
+        out[name + '/G'], out[name + '/h'] = G, h
+        out[name + '/T'] = np.array(T, dtype=np.int32)
+        out[name + '/meta'] = np.array([P, R, qi, key & 0xFFFFFFFF, key >> 32, 0 if start == 'rand' else 1], dtype=np.int64)
+        out[name + '/inst'] = inst
+        print('arpeggio', name, 'D', D, 'P', P, 'passes', len(T), 'flips', int(out[name + '/arpeggio/st'][..., 0].sum()))
+    out['names'] = np.array([c[0] for c in cases])
+    np.savez_compressed(os.path.join(OUT, 'golden_arpeggio.npz'), **out)
+
+
+def chord_fixture():
+    cases = [  # name, (Nt, M, snr, B, kind, K), R, S, t0, t1, q, kappa, P, seed, inst0 (test_kernel.py:213-221)
+        ('16x16_QPSK_RI', (16, 4, 10.0, 6, 'ri', 1), 16, 128, 0.7, 0.5, 0.6, 0.0, 1, 7, 0),
+        ('16x16_QPSK_RI_kappa', (16, 4, 10.0, 6, 'ri', 1), 16, 128, 2.0, 0.05, 0.5, 0.3, 1, 8, 1000),
+        ('16x16_16QAM_dDI_K1', (16, 16, 20.0, 6, 'ddi', 1), 16, 256, 0.3, 0.3, 0.4, 0.0, 2, 9, 0),
+        ('32x32_16QAM_dDI_K1_kappa', (32, 16, 22.0, 3, 'ddi', 1), 8, 128, 0.3, 0.2, 0.4, 0.3, 2, 10, 77),
+        ('16x16_16QAM_dDI_K3', (16, 16, 18.0, 3, 'ddi', 3), 4, 96, 0.3, 0.3, 0.4, 0.0, 6, 11, 5),
+        ('64x64_16QAM_dDI_K1', (64, 16, 24.0, 2, 'ddi', 1), 3, 32, 0.3, 0.3, 0.4, 0.0, 2, 12, 0),
+        ('16x16_QPSK_RI_40anneals', (16, 4, 12.0, 3, 'ri', 1), 40, 64, 0.7, 0.5, 0.6, 0.0, 1, 2 ** 40 + 3, 123456),
+    ]
+    out = {}
+    for name, (Nt, M, snr, B, kind, K), R, S, t0, t1, q, kappa, P, seed, inst0 in cases:
+        g = torch.Generator(device='cpu')
+        g.manual_seed(seed + 100)
+        b = mimo.make_batch(B, Nt, Nt, M, snr, g, device='cpu')
+        z, Ai, _ = mimo.mmse(b)
+        I = mimo.ising(b, z) if kind == 'ri' else mimo.ising_delta_at(b, mimo.mmse_hard(b, z, Ai), K)
+        F = chordfx.to_fixed(I, S, t0, t1, q, kappa)
+        rs, re = chordfx.chord_fx(F, R, seed, P=P, inst0=inst0)
+        bs, be = chordfx.chord_fx(F, R, seed, P=P, inst0=inst0, mode='best')
+        for k, v in (('J', F['J']), ('h', F['h']), ('h0', F['h0']), ('T', F['T']), ('c', F['c']),
+                     ('chains_s', rs), ('chains_e', re), ('best_s', bs), ('best_e', be)):
+            out[name + '/' + k] = v.numpy()
+        out[name + '/meta'] = np.array([F['q'], S, P, R, seed & 0xFFFFFFFF, seed >> 32, inst0], dtype=np.int64)
+        print('chord', name, 'N', F['h'].shape[1], 'best e', be.tolist()[:3])
+    out['names'] = np.array([c[0] for c in cases])
+    np.savez_compressed(os.path.join(OUT, 'golden_chord.npz'), **out)
+
+
+def mapping_fixture():
+    out = {}
+    rng = np.random.default_rng(11)
+    for nt, snr, B, seed in ((16, 12.0, 16, 9700), (32, 16.0, 8, 9701), (64, 20.0, 4, 9702)):
+        tag = 'x%d' % nt
+        b = arpx.draw(seed, snr, 0, B, nt, 16, dev='cpu')
+        z, Ai, _ = mimo.mmse(b)
+        mu = mimo._mu(b, z)
+        lm = mimo.quantize_levels(z / mu, 16)
+        out[tag + '/H'], out[tag + '/y'], out[tag + '/l'] = b['H'].numpy(), b['y'].numpy(), b['l'].numpy()
+        out[tag + '/N0'] = np.array([b['N0']])
+        out[tag + '/z'], out[tag + '/mu'], out[tag + '/xq'] = z.numpy(), mu.numpy(), lm.numpy()
+        for K in (1, 2):
+            I = mimo.ising_delta_at(b, lm, K)
+            F = chordfx.to_fixed(I, 8 * 2 * K, 0.3, 0.3, 0.4, 0.0)
+            G, h = chord_ref.compress(F, K)
+            out['%s/K%d/scale' % (tag, K)] = I['scale'].numpy()
+            out['%s/K%d/G' % (tag, K)] = G.numpy().astype(np.int32)
+            out['%s/K%d/h' % (tag, K)] = h.numpy().astype(np.int32)
+            S = torch.from_numpy(rng.choice([-1.0, 1.0], size=(B, 5, 2 * K * 2 * nt)).astype(np.float32))
+            Lc = mimo.spins_to_levels_delta(S, I, 16)
+            dd = mimo.dist(b, Lc)
+            lh, _, _ = mimo.select(b, Lc, lm)
+            out['%s/K%d/S' % (tag, K)] = S.numpy().astype(np.int8)
+            out['%s/K%d/Lc' % (tag, K)] = Lc.numpy().astype(np.int8)
+            out['%s/K%d/dist' % (tag, K)] = dd.numpy()
+            out['%s/K%d/sel' % (tag, K)] = lh.numpy().astype(np.int8)
+            out['%s/K%d/bits' % (tag, K)] = mimo.levels_to_bits(lh, 16).numpy()
+        print('mapping', tag)
+    np.savez_compressed(os.path.join(OUT, 'golden_mapping.npz'), **out)
+
+
+if __name__ == '__main__':
+    philox_fixture()
+    arpeggio_fixture()
+    chord_fixture()
+    mapping_fixture()

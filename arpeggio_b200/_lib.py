@@ -1,0 +1,67 @@
+"""ctypes binding of the in-tree C-ABI library libarpeggio_b200.so (declarations: include/arpeggio_b200.h).
+
+There is no fallback: if the library is missing or a call fails, an exception is raised."""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, 'libarpeggio_b200.so')
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_U = ctypes.c_uint32
+_F = ctypes.c_float
+
+# name -> argtypes, in the order of include/arpeggio_b200.h
+SIGNATURES = {
+    'arp_version': [],
+    'arp_status_string': [_I],
+    'arp_philox_kat': [_P, _P, _I, _P],
+    'arp_philox_rate': [_P, _I, _I, _I, _P],
+    'arp_anneal_first_accept': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
+    'arp_anneal_chord_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
+    'arp_anneal_dd_f32': [_I, _P, _P, _P, _P, _I, _F, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
+    'arp_anneal_chord': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _U, _U, _U, _I, _I, _P, _P, _P, _P, _P],
+    'arp_map_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P],
+    'arp_readout_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P],
+}
+
+_lib = None
+
+
+class ArpError(RuntimeError):
+    pass
+
+
+def lib():
+    """Loads the library (building it first when only the sources are present)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            from . import build
+            build.build()
+        if not os.path.exists(LIB):
+            raise ArpError('libarpeggio_b200.so is missing; run python -m arpeggio_b200.build')
+        L = ctypes.CDLL(LIB)
+        for name, argt in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = argt
+            f.restype = ctypes.c_char_p if name in ('arp_version', 'arp_status_string') else ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != 0:
+        raise ArpError('%s failed: %s (code %d)' % (what, lib().arp_status_string(rc).decode(), rc))
+
+
+def ptr(t):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)

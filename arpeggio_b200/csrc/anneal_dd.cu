@@ -1,0 +1,416 @@
+// Anneals on compressed dDI problems: first accept (Arpeggio) and the Chord round, integer or FP32 fields.
+//
+// Problem (arpeggio_ref59.py:41-85, chord_ref.py:72-123): the dDI coupling over N = P D spins is
+// J = -offdiag(G (x) 1 1^T), so one lane field per coordinate, w_j = h_j - 2 (G m)_j with m = sum of the P
+// copies, serves every copy: the field of spin (p, j) is w_j + 2 G_jj s_pj.
+//
+// Mapping (one warp = one anneal, lanes across threads): thread `lane` owns coordinates j = t*32 + lane for
+// t < NS = ceil(D/32); its fields w[t] live in registers; spins are warp-uniform bit masks Sm[p][t]; G sits
+// in shared memory transposed and zero-padded to NS*32 columns (Gs[j][i] = G[i][j]) so a flip of lane j
+// streams one contiguous row.  A block holds one problem and W warps that take anneals r = w, w + W, ...
+//
+// First accept, exactly the reference's index-order scan: every remaining lane of the active copy tests
+// against the current fields at once, a ballot + ffs picks the first accepted lane j, the flip commits
+// (rank-1 update of every field from row j), and lanes after j re-test with the same draws.  Lanes that
+// rejected before j stay rejected, as in the sequential scan, because their decision came before the flip.
+// Chord: one snapshot test of the active copy, then the accepted lanes commit in index order.
+//
+// RNG: Philox4x32-10 with the reference's counters -- start (2^32-1, p*D+j, r, inst) word 0 ('rand') or
+// (2^32-1, j, r, inst) ('bal'); pass k = n*P + p uses word n&3 of block (n>>2, p*D+j, r, inst).  One block
+// serves four sweeps, so each quad of sweeps computes P*NS blocks per thread once (registers) instead of
+// one block per test (the reference's arpeggio_fx.cu:75).
+//
+// Integer decision: u*4T > (s w + 2 G_jj + q + 2T) * 2^32 (arpeggio_fx.cu:76-79) is evaluated as
+// s w < ceil(u*4T / 2^32) - 2 G_jj - q - 2T, a 32-bit compare; the entry points bound |G|, |h|, |T|, |q|
+// so that every field and threshold fits 32 bits (ARP_ERR_RANGE otherwise).
+#include <climits>
+#include <type_traits>
+
+#include "arp_common.cuh"
+
+namespace arp {
+
+struct DDParams {
+  const void* Gt;  // (B, D, D) int32 or float, Gt[b][j][i] = G[b][i][j]
+  const void* h;   // (B, D)
+  const void* T;   // (L)
+  const void* c;   // (L) Onsager terms or null
+  int L;
+  int32_t qi;
+  float qf;
+  int R, D, B;
+  const uint32_t* inst;
+  uint32_t k0, k1;
+  int start;
+  int8_t* out_s;
+  void* out_de;
+  int64_t* out_st;
+  int32_t* status;
+};
+
+constexpr int32_t kMaxG = 1 << 18, kMaxH = 1 << 28, kMaxT = 1 << 26;
+
+template <int NS, int P, bool CHORD, bool FLT, bool CACHE>
+__global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
+  using FT = typename std::conditional<FLT, float, int32_t>::type;
+  using ET = typename std::conditional<FLT, float, long long>::type;
+  constexpr int DP = NS * 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  FT* Gs = reinterpret_cast<FT*>(smem);
+  __shared__ int s_bad;
+  const int D = a.D, L = a.L, R = a.R;
+  const int b = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  {
+    const FT* Gg = reinterpret_cast<const FT*>(a.Gt) + (size_t)b * D * D;
+    bool bad = false;
+    for (int x = threadIdx.x; x < D * DP; x += blockDim.x) {
+      const int j = x / DP, i = x - j * DP;
+      const FT v = i < D ? Gg[(size_t)j * D + i] : FT(0);
+      if constexpr (!FLT) bad |= (v > kMaxG || v < -kMaxG);
+      Gs[x] = v;
+    }
+    if constexpr (!FLT) {
+      const int32_t* hg = reinterpret_cast<const int32_t*>(a.h) + (size_t)b * D;
+      for (int x = threadIdx.x; x < D; x += blockDim.x) bad |= (hg[x] > kMaxH || hg[x] < -kMaxH);
+      const int32_t* Tg = reinterpret_cast<const int32_t*>(a.T);
+      const int32_t* cg = reinterpret_cast<const int32_t*>(a.c);
+      for (int x = threadIdx.x; x < L; x += blockDim.x) {
+        bad |= (Tg[x] > kMaxT || Tg[x] < -kMaxT);
+        if (cg) bad |= (cg[x] > kMaxT || cg[x] < -kMaxT);
+      }
+      bad |= (a.qi > kMaxT || a.qi < -kMaxT);
+    }
+    if (bad) s_bad = 1;
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (threadIdx.x == 0) set_status(a.status, ARP_ERR_RANGE);
+    return;
+  }
+  const uint32_t inst = a.inst[b];
+  FT dg[NS], hv[NS];
+  uint32_t vmask[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    const int j = t * 32 + lane;
+    const int nv = D - t * 32;
+    vmask[t] = nv >= 32 ? ARP_FULL : (nv > 0 ? (1u << nv) - 1u : 0u);
+    dg[t] = j < D ? Gs[j * DP + j] : FT(0);
+    hv[t] = j < D ? reinterpret_cast<const FT*>(a.h)[(size_t)b * D + j] : FT(0);
+  }
+  const FT* Tg = reinterpret_cast<const FT*>(a.T);
+  const FT* cg = reinterpret_cast<const FT*>(a.c);
+
+  for (int r = wid; r < R; r += W) {
+    uint32_t Sm[P][NS], Bm[P][NS];
+    // ---- start state (arpeggio_fx.cu:48-57)
+    if (a.start == 0) {
+#pragma unroll
+      for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+          uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+          philox10(c0, c1, c2, c3, a.k0, a.k1);
+          Sm[p][t] = __ballot_sync(ARP_FULL, c0 >= 0x80000000u) & vmask[t];
+        }
+    } else {
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)(t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+        philox10(c0, c1, c2, c3, a.k0, a.k1);
+        const int pat = bal_pattern(P, (uint32_t)(((uint64_t)c0 * (uint64_t)bal_choose(P)) >> 32));
+#pragma unroll
+        for (int p = 0; p < P; ++p) Sm[p][t] = __ballot_sync(ARP_FULL, (pat >> p) & 1) & vmask[t];
+      }
+    }
+    // ---- lane fields w = h - 2 G m (arpeggio_fx.cu:58-66); float: sum in j order, one rounding per op
+    FT w[NS];
+    FT acc[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) acc[t] = FT(0);
+#pragma unroll
+    for (int tj = 0; tj < NS; ++tj) {
+      for (int l = 0; l < 32; ++l) {
+        const int j = tj * 32 + l;
+        if (j >= D) break;
+        int m = 0;
+#pragma unroll
+        for (int p = 0; p < P; ++p) m += ((Sm[p][tj] >> l) & 1u) ? 1 : -1;
+        if (m == 0) continue;
+        const FT* gr = Gs + j * DP + lane;
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+          if constexpr (FLT)
+            acc[t] = __fadd_rn(acc[t], __fmul_rn(gr[t * 32], (float)m));
+          else
+            acc[t] += gr[t * 32] * m;
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      if constexpr (FLT)
+        w[t] = __fsub_rn(hv[t], __fmul_rn(2.0f, acc[t]));
+      else
+        w[t] = hv[t] - 2 * acc[t];
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int t = 0; t < NS; ++t) Bm[p][t] = Sm[p][t];
+
+    ET de = ET(0), best;
+    if constexpr (FLT)
+      best = __int_as_float(0x7f800000);
+    else
+      best = 1LL << 62;
+    long long flips = 0, tests = 0;
+    const int nquad = (L + 4 * P - 1) / (4 * P);
+    for (int q4 = 0; q4 < nquad; ++q4) {
+      uint32_t cw[CACHE ? P : 1][CACHE ? NS : 1][4];
+      if constexpr (CACHE) {
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int t = 0; t < NS; ++t) {
+            uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+            philox10(c0, c1, c2, c3, a.k0, a.k1);
+            cw[p][t][0] = c0;
+            cw[p][t][1] = c1;
+            cw[p][t][2] = c2;
+            cw[p][t][3] = c3;
+          }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const int k = (q4 * 4 + i) * P + p;
+          if (k >= L) break;
+          // ---- per-lane thresholds for this pass
+          FT th[NS];
+          FT qk;
+          if constexpr (FLT) {
+            const float A = __fmul_rn(4.0f, Tg[k]);
+            qk = (CHORD && cg) ? __fsub_rn(a.qf, cg[k]) : a.qf;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+              uint32_t u;
+              if constexpr (CACHE) {
+                u = cw[p][t][i];
+              } else {
+                uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+                philox10(c0, c1, c2, c3, a.k0, a.k1);
+                u = i == 0 ? c0 : (i == 1 ? c1 : (i == 2 ? c2 : c3));
+              }
+              th[t] = __fmul_rn(__fsub_rn(unit24(u), 0.5f), A);
+            }
+          } else {
+            const int32_t Tk = Tg[k];
+            const long long A = 4LL * Tk;
+            const int32_t Bk = a.qi + 2 * Tk - ((CHORD && cg) ? cg[k] : 0);
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+              uint32_t u;
+              if constexpr (CACHE) {
+                u = cw[p][t][i];
+              } else {
+                uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+                philox10(c0, c1, c2, c3, a.k0, a.k1);
+                u = i == 0 ? c0 : (i == 1 ? c1 : (i == 2 ? c2 : c3));
+              }
+              th[t] = ((vmask[t] >> lane) & 1u) ? (int32_t)ceil_shift32(u, A) - 2 * dg[t] - Bk : INT_MIN;
+            }
+            qk = 0;
+          }
+          // ---- the test of one lane against the current fields
+          auto accept = [&](int t) -> bool {
+            const FT sw = ((Sm[p][t] >> lane) & 1u) ? w[t] : -w[t];
+            if constexpr (FLT)
+              return __fadd_rn(__fadd_rn(sw, __fmul_rn(2.0f, dg[t])), qk) < th[t];
+            else
+              return sw < th[t];
+          };
+          // ---- commit a flip of lane l of slot t (fields after earlier commits)
+          auto commit = [&](FT wsel, FT dsel, uint32_t sbits, int j, int l) {
+            const FT wj = __shfl_sync(ARP_FULL, wsel, l);
+            const FT dj = __shfl_sync(ARP_FULL, dsel, l);
+            const int so = ((sbits >> l) & 1u) ? 1 : -1;
+            if constexpr (FLT)
+              de = __fadd_rn(de, __fadd_rn(__fmul_rn((float)(4 * so), wj), __fmul_rn(8.0f, dj)));
+            else
+              de += 4LL * so * wj + 8LL * dj;
+            const FT* gr = Gs + j * DP + lane;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+              if constexpr (FLT)
+                w[t] = __fadd_rn(w[t], __fmul_rn((float)(4 * so), gr[t * 32]));
+              else
+                w[t] += 4 * so * gr[t * 32];
+            }
+            ++flips;
+          };
+          if constexpr (!CHORD) {
+            uint32_t rem[NS];
+#pragma unroll
+            for (int t = 0; t < NS; ++t) rem[t] = vmask[t];
+            long long tt = 1;
+            for (;;) {
+              uint32_t am[NS];
+#pragma unroll
+              for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, accept(t)) & rem[t];
+              int ts = -1;
+              uint32_t m = 0;
+#pragma unroll
+              for (int t = NS - 1; t >= 0; --t)
+                if (am[t]) {
+                  ts = t;
+                  m = am[t];
+                }
+              if (ts < 0) break;
+              const int l = __ffs(m) - 1;
+              FT wsel = w[0], dsel = dg[0];
+              uint32_t sbits = Sm[p][0];
+#pragma unroll
+              for (int t = 1; t < NS; ++t)
+                if (ts == t) {
+                  wsel = w[t];
+                  dsel = dg[t];
+                  sbits = Sm[p][t];
+                }
+              const int j = ts * 32 + l;
+              commit(wsel, dsel, sbits, j, l);
+              const uint32_t bit = 1u << l;
+#pragma unroll
+              for (int t = 0; t < NS; ++t) {
+                if (t == ts) {
+                  Sm[p][t] ^= bit;
+                  rem[t] &= ~((bit << 1) - 1u);
+                } else if (t < ts) {
+                  rem[t] = 0;
+                }
+              }
+              if (j < D - 1) ++tt;
+            }
+            tests += tt;
+          } else {
+            uint32_t am[NS];
+#pragma unroll
+            for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, accept(t)) & vmask[t];
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+              uint32_t m = am[t];
+              while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1u;
+                commit(w[t], dg[t], Sm[p][t], t * 32 + l, l);
+              }
+              Sm[p][t] ^= am[t];
+            }
+            tests += 1;
+          }
+          if (de < best) {  // best state after each pass (arpeggio_fx.cu:90-93)
+            best = de;
+#pragma unroll
+            for (int pp = 0; pp < P; ++pp)
+#pragma unroll
+              for (int t = 0; t < NS; ++t) Bm[pp][t] = Sm[pp][t];
+          }
+        }
+      }
+    }
+    // ---- outputs (arpeggio_fx.cu:95-99)
+    const size_t ar = (size_t)b * R + r;
+    int8_t* os = a.out_s + ar * P * D;
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        const int j = t * 32 + lane;
+        if (j < D) os[p * D + j] = ((Bm[p][t] >> lane) & 1u) ? 1 : -1;
+      }
+    if (lane == 0) {
+      reinterpret_cast<ET*>(a.out_de)[ar] = best;
+      a.out_st[2 * ar] = flips;
+      a.out_st[2 * ar + 1] = tests;
+    }
+  }
+}
+
+template <int NS, int P, bool CHORD, bool FLT>
+static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
+  constexpr bool CACHE = P * NS <= 8;
+  auto kern = k_anneal_dd<NS, P, CHORD, FLT, CACHE>;
+  const size_t smem = (size_t)a.D * NS * 32 * 4;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<a.B, warps * 32, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <bool CHORD, bool FLT>
+static cudaError_t launch_dd(const DDParams& a, int P, int warps, cudaStream_t st) {
+  const int NS = (a.D + 31) / 32;
+#define ARP_CASE(ns, pp) \
+  if (NS == ns && P == pp) return launch_ns_p<ns, pp, CHORD, FLT>(a, warps, st);
+  ARP_CASE(1, 2) ARP_CASE(1, 4) ARP_CASE(1, 6)
+  ARP_CASE(2, 2) ARP_CASE(2, 4) ARP_CASE(2, 6)
+  ARP_CASE(3, 2) ARP_CASE(3, 4) ARP_CASE(3, 6)
+  ARP_CASE(4, 2) ARP_CASE(4, 4) ARP_CASE(4, 6)
+#undef ARP_CASE
+  return cudaErrorInvalidValue;
+}
+
+static int check_dd(const void* Gt, const void* h, const void* T, int L, int P, int R, int D, int B,
+                    const uint32_t* inst, int start, const int8_t* out_s, const void* out_de, const int64_t* out_st) {
+  if (B < 0 || R < 1 || D < 1 || D > 128 || L < 1 || !(P == 2 || P == 4 || P == 6)) return ARP_ERR_SHAPE;
+  if (start != 0 && start != 1) return ARP_ERR_ARG;
+  if (B > 0 && (!Gt || !h || !T || !inst || !out_s || !out_de || !out_st)) return ARP_ERR_ARG;
+  return ARP_OK;
+}
+
+static int default_warps(int R) { return R < 8 ? R : 8; }
+
+}  // namespace arp
+
+using namespace arp;
+
+extern "C" int arp_anneal_first_accept(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P,
+                                       int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                                       int start, int8_t* out_s, int64_t* out_de, int64_t* out_st,
+                                       int32_t* status, void* stream) {
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  DDParams a{Gt, h, T, nullptr, L, q, 0.0f, R, D, B, inst, k0, k1, start, out_s, out_de, out_st, status};
+  return launch_dd<false, false>(a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
+                                                                                              : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L,
+                                   int q, int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                                   int start, int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status,
+                                   void* stream) {
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  DDParams a{Gt, h, T, c, L, q, 0.0f, R, D, B, inst, k0, k1, start, out_s, out_de, out_st, status};
+  return launch_dd<true, false>(a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
+                                                                                             : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, const float* T, const float* c, int L,
+                                 float q, int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                                 int start, int8_t* out_s, float* out_de, int64_t* out_st, int32_t* status,
+                                 void* stream) {
+  if (policy != 0 && policy != 1) return ARP_ERR_ARG;
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  DDParams a{Gt, h, T, c, L, 0, q, R, D, B, inst, k0, k1, start, out_s, out_de, out_st, status};
+  cudaError_t e = policy == 0 ? launch_dd<false, true>(a, P, default_warps(R), (cudaStream_t)stream)
+                              : launch_dd<true, true>(a, P, default_warps(R), (cudaStream_t)stream);
+  return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}

@@ -1,0 +1,59 @@
+// Shared device helpers: Philox4x32-10, warp masks, status reporting.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/arpeggio_b200.h"
+
+#define ARP_FULL 0xffffffffu
+
+namespace arp {
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of two 32x32->64 multiplies,
+// Weyl key increments 0x9E3779B9 / 0xBB67AE85.  Counter (c0..c3) in place, key (k0, k1).
+// The counter layout each caller uses is the reference's (arpeggio_fx.cu:51,75; chord_kernel.cu:288,321).
+__device__ __forceinline__ void philox10(uint32_t& c0, uint32_t& c1, uint32_t& c2, uint32_t& c3, uint32_t k0,
+                                         uint32_t k1) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+// ceil(u * A / 2^32) for u < 2^32 and |A| < 2^31, as a signed 64-bit floor shift.  For an integer z,
+// u * A > z * 2^32  <=>  z < ceil(u * A / 2^32): the reference's exact int64/bignum decision
+// (arpeggio_fx.cu:76-79, arpeggio_ref59.py:62) becomes one 32-bit compare once the threshold is known.
+__device__ __forceinline__ int64_t ceil_shift32(uint32_t u, int64_t A) {
+  return ((int64_t)u * A + 0xFFFFFFFFLL) >> 32;
+}
+
+// Uniform float in [0, 1) with 24 exact bits: (x >> 8) * 2^-24.
+__device__ __forceinline__ float unit24(uint32_t x) { return __fmul_rn((float)(x >> 8), 5.9604644775390625e-08f); }
+
+__device__ __forceinline__ void set_status(int32_t* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+// Index (within [0, C(P, P/2))) -> the P-bit pattern with P/2 ones, in increasing order
+// (arpeggio_ref59.py:31-38).  Tables for P = 2, 4, 6.
+__device__ __forceinline__ int bal_pattern(int P, uint32_t i) {
+  int n = 0;
+  for (int v = 0; v < (1 << P); ++v)
+    if (__popc(v) == P / 2) {
+      if (n == (int)i) return v;
+      ++n;
+    }
+  return 0;
+}
+
+__host__ __device__ __forceinline__ int bal_choose(int P) { return P == 2 ? 2 : (P == 4 ? 6 : 20); }
+
+}  // namespace arp

@@ -1,0 +1,225 @@
+"""The detector call: channel H, received y, constellation, SNR, flip policy, anneals, cycle budget and seed in;
+hard bits and final energies out.
+
+One `Detector` owns every device buffer for a maximum batch, so a call allocates nothing: map
+(Gram/field formation and the MMSE guess, arp_map_dd) -> anneal (arp_anneal_first_accept /
+arp_anneal_chord_dd / arp_anneal_dd_f32) -> readout (arp_readout_dd), three launches on one stream.
+This is the one-stage dDI detection of the reference's arpeggio/mimo/fxdetect.py:24-43 (dDI around the
+hard MMSE guess, every anneal's best state and the guess go to the distance selection) with either flip
+policy, and the sub-problem solve of arpeggio/sim/local_code_a513/run_a513.py:107-128.
+
+`solver_protocol` returns a callable with the reference's solver interface solver(I, na, K) -> spins
+(n, na, 2K D) (arpeggio/mimo/mdi_solvers.py:1-3, called at mimo.py:587), so the reference's own MDI wrapper
+can drive these kernels."""
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .chordfx import QSCALE, geom
+
+PAM = {4: dict(levels=(-1, 1), a=1 / math.sqrt(2), bits=1),
+       16: dict(levels=(-3, -1, 1, 3), a=1 / math.sqrt(10), bits=2)}
+# Budgets the reference runs: Arpeggio picks abl_far_<S>_<T0>_<T1>_<q>_<start>_<Ns> (run_a513.py:35-39,
+# data/results/a513_fixed) and Chord's MDI schedule MDICHORD (mdi_solvers.py:18: 128 steps per copy pair).
+ARPEGGIO_PICKS = {16: dict(sweeps=64, T0=0.1, T1=0.1, q=0.0, start='rand'),
+                  32: dict(sweeps=32, T0=0.1, T1=0.1, q=0.0, start='rand'),
+                  64: dict(sweeps=64, T0=0.1, T1=0.1, q=0.0, start='bal')}
+CHORD_DEFAULT = dict(steps_per_copy_pair=128, T0=0.3, T1=0.3, q=0.4, kappa=0.0)
+M32 = 0xFFFFFFFF
+
+
+def el2(M):
+    lv = np.asarray(PAM[M]['levels'], dtype=np.float64)
+    return float((lv ** 2).mean())
+
+
+def arpeggio_schedule(sweeps, T0, T1, q, K, precision='int'):
+    """One temperature per pass, S sweeps x P passes (run_a513.py:83-87); integers in units of 1/4096."""
+    Tsw = geom(T0, T1, sweeps).double()
+    if precision == 'int':
+        Ts = [int(round(float(v) * QSCALE)) for v in Tsw]
+        return [t for t in Ts for _ in range(2 * K)], int(round(q * QSCALE)), None
+    Ts = [float(v) for v in Tsw.float()]
+    return [t for t in Ts for _ in range(2 * K)], float(q), None
+
+
+def chord_schedule(steps, T0, T1, q, kappa=0.0, ramp=True, precision='int'):
+    """Chord's per-step T and Onsager c (chordfx.py:66-76)."""
+    T = geom(T0, T1, steps).double()
+    rho = torch.ones(steps, dtype=torch.float64)
+    if ramp:
+        t = torch.arange(steps, dtype=torch.float64)
+        rho = torch.where(t >= 0.7 * steps, (steps - 1 - t) / max(1.0, steps - 1 - 0.7 * steps), torch.ones_like(t))
+    c = torch.zeros(steps, dtype=torch.float64)
+    c[1:] = kappa * T[:-1] * rho[1:]
+    if precision == 'int':
+        return ([int(v) for v in torch.round(T * QSCALE).tolist()], int(round(q * QSCALE)),
+                [int(v) for v in torch.round(c * QSCALE).tolist()])
+    return [float(v) for v in T.float()], float(q), [float(v) for v in c.float()]
+
+
+class Detector:
+    """Preallocated one-stage dDI detector for up to `B` channel uses of nt users x nr antennas."""
+
+    def __init__(self, B, nt, nr=None, M=16, policy='arpeggio', anneals=32, K=1, sweeps=None, T0=None, T1=None,
+                 q=None, start=None, kappa=0.0, precision='int', device='cuda'):
+        if policy not in ('arpeggio', 'chord'):
+            raise ValueError("policy must be 'arpeggio' or 'chord'")
+        if precision not in ('int', 'f32'):
+            raise ValueError("precision must be 'int' or 'f32'")
+        nr = nt if nr is None else nr
+        self.B, self.nt, self.nr, self.M, self.K = B, nt, nr, M, K
+        self.D, self.NR2, self.P, self.R = 2 * nt, 2 * nr, 2 * K, anneals
+        self.policy, self.precision = policy, precision
+        dev = torch.device(device)
+        self.device = dev
+        if policy == 'arpeggio':
+            pk = dict(ARPEGGIO_PICKS.get(nt, ARPEGGIO_PICKS[32]))
+            for k, v in (('sweeps', sweeps), ('T0', T0), ('T1', T1), ('q', q), ('start', start)):
+                if v is not None:
+                    pk[k] = v
+            T, qq, c = arpeggio_schedule(pk['sweeps'], pk['T0'], pk['T1'], pk['q'], K, precision)
+            self.start = pk['start']
+        else:
+            steps = sweeps * 2 * K if sweeps is not None else CHORD_DEFAULT['steps_per_copy_pair'] * 2 * K
+            T, qq, c = chord_schedule(steps, CHORD_DEFAULT['T0'] if T0 is None else T0,
+                                      CHORD_DEFAULT['T1'] if T1 is None else T1,
+                                      CHORD_DEFAULT['q'] if q is None else q, kappa, precision=precision)
+            self.start = 'rand' if start is None else start
+        self.schedule = dict(T=T, q=qq, c=c)
+        f32 = precision == 'f32'
+        tdt = torch.float32 if f32 else torch.int32
+        self.T = torch.tensor(T, dtype=tdt, device=dev)
+        self.c = None if c is None else torch.tensor(c, dtype=tdt, device=dev)
+        self.q = qq
+        D, R, P, NR2 = self.D, self.R, self.P, self.NR2
+        self.G = torch.empty(B, D, D, dtype=tdt, device=dev)
+        self.h = torch.empty(B, D, dtype=tdt, device=dev)
+        self.xq = torch.empty(B, D, dtype=torch.int8, device=dev)
+        self.scale = torch.empty(B, dtype=torch.float32, device=dev)
+        self.sigma2 = torch.empty(B, dtype=torch.float32, device=dev)
+        self.inst = torch.empty(B, dtype=torch.int32, device=dev)
+        self.spins = torch.empty(B, R, P * D, dtype=torch.int8, device=dev)
+        self.de = torch.empty(B, R, dtype=torch.float32 if f32 else torch.int64, device=dev)
+        self.st = torch.empty(B, R, 2, dtype=torch.int64, device=dev)
+        self.levels = torch.empty(B, D, dtype=torch.int8, device=dev)
+        self.bits = torch.empty(B, D * PAM[M]['bits'], dtype=torch.int8, device=dev)
+        self.dist = torch.empty(B, dtype=torch.float32, device=dev)
+        self.pick = torch.empty(B, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._inst_base = None
+
+    def set_noise(self, snr_db=None, N0=None, n=None):
+        """sigma2 = (N0/2)/E[l^2] per use; N0 = Nt/10^(SNR/10) (mimo.py:79) unless given."""
+        n = self.B if n is None else n
+        if N0 is None:
+            snr = torch.as_tensor(snr_db, dtype=torch.float64).reshape(-1)
+            N0 = self.nt / (10 ** (snr / 10))
+        N0 = torch.as_tensor(N0, dtype=torch.float64).reshape(-1)
+        s2 = (N0 / 2) / el2(self.M)
+        self.sigma2[:n].copy_(s2.float().expand(n) if s2.numel() == 1 else s2.float(), non_blocking=True)
+
+    def run(self, H, y, seed, n=None, inst0=0, stream=None, events=None):
+        """Stream-ordered detection of the first n uses; H (n, NR2, D) and y (n, NR2) float32 on the device.
+        Returns views of the device outputs (bits, levels, dist); nothing is synchronised.  events: optional
+        four CUDA events recorded before map, anneal, readout and after readout (per-stage timing)."""
+        ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
+        n = self.B if n is None else n
+        if self._inst_base != (inst0, n):
+            iv = (np.arange(inst0, inst0 + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
+            self.inst[:n].copy_(torch.from_numpy(iv))
+            self._inst_base = (inst0, n)
+        L = _lib.lib()
+        sp = _lib.stream_ptr(stream)
+        D, NR2, P, R = self.D, self.NR2, self.P, self.R
+        f32 = self.precision == 'f32'
+        ev(0)
+        _lib.check(L.arp_map_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.sigma2), n, NR2, D, self.M, 0 if f32 else 1,
+                                _lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.xq), _lib.ptr(self.scale),
+                                _lib.ptr(self.status), sp), 'map')
+        k0, k1, sv = seed & M32, (seed >> 32) & M32, 0 if self.start == 'rand' else 1
+        ev(1)
+        outs = (_lib.ptr(self.spins), _lib.ptr(self.de), _lib.ptr(self.st), _lib.ptr(self.status), sp)
+        Lt = int(self.T.shape[0])
+        if f32:
+            rc = L.arp_anneal_dd_f32(0 if self.policy == 'arpeggio' else 1, _lib.ptr(self.G), _lib.ptr(self.h),
+                                     _lib.ptr(self.T), _lib.ptr(self.c), Lt, float(self.q), P, R, D, n,
+                                     _lib.ptr(self.inst), k0, k1, sv, *outs)
+        elif self.policy == 'arpeggio':
+            rc = L.arp_anneal_first_accept(_lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.T), Lt, int(self.q), P,
+                                           R, D, n, _lib.ptr(self.inst), k0, k1, sv, *outs)
+        else:
+            rc = L.arp_anneal_chord_dd(_lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.T), _lib.ptr(self.c), Lt,
+                                       int(self.q), P, R, D, n, _lib.ptr(self.inst), k0, k1, sv, *outs)
+        _lib.check(rc, 'anneal')
+        ev(2)
+        _lib.check(L.arp_readout_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.xq), _lib.ptr(self.spins), n, NR2, D, P,
+                                    R, self.M, _lib.ptr(self.levels), _lib.ptr(self.bits), _lib.ptr(self.dist),
+                                    _lib.ptr(self.pick), sp), 'readout')
+        ev(3)
+        return self.bits[:n], self.levels[:n], self.dist[:n]
+
+    def check(self):
+        _lib.check(int(self.status.item()), 'device check')
+
+
+def detect(H, y, M=16, snr_db=None, N0=None, policy='arpeggio', anneals=32, K=1, seed=0, precision='int',
+           inst0=0, **budget):
+    """One call of the drop-in detector on host or device arrays H (B, 2 nr, 2 nt), y (B, 2 nr).
+    Returns numpy dict(bits, levels, dist=final ||y - H x||^2, pick, de=best energy change per anneal)."""
+    H = torch.as_tensor(H, dtype=torch.float32)
+    y = torch.as_tensor(y, dtype=torch.float32)
+    B, NR2, D = H.shape
+    det = Detector(B, D // 2, NR2 // 2, M, policy, anneals, K, precision=precision, **budget)
+    det.set_noise(snr_db, N0)
+    bits, levels, dist = det.run(H.cuda().contiguous(), y.cuda().contiguous(), seed, inst0=inst0)
+    torch.cuda.synchronize()
+    det.check()
+    return dict(bits=bits.cpu().numpy(), levels=levels.cpu().numpy(), dist=dist.cpu().numpy(),
+                pick=det.pick.cpu().numpy(), de=det.de.cpu().numpy(), xq=det.xq.cpu().numpy())
+
+
+def solver_protocol(policy='arpeggio', precision='int', seed=0, key_step=0xD1B54A32D192ED03, **budget):
+    """A solver(I, na, K) -> spins (n, na, 2K D) float for the reference's MDI wrapper (mimo.mdi, mimo.py:553-602).
+    I is the float dict of mimo.ising_delta_at; the compressed G and h are taken from its J and h exactly as
+    chordfx.to_fixed + chord_ref.compress do; each call uses key seed + call * key_step."""
+    calls = [0]
+
+    def solver(I, na, K, meta=None):
+        ci = calls[0]
+        calls[0] += 1
+        h0 = I['h'].float()
+        B, N = h0.shape
+        D = N // (2 * K)
+        J = I['J'].float()
+        Js = (J + J.transpose(1, 2)) / 2
+        Gf = -Js[:, :D, D:2 * D]
+        hf = h0[:, :D]
+        if policy == 'arpeggio':
+            pk = dict(ARPEGGIO_PICKS.get(D // 2, ARPEGGIO_PICKS[32]))
+            pk.update({k: v for k, v in budget.items() if k in pk})
+            T, q, c = arpeggio_schedule(pk['sweeps'], pk['T0'], pk['T1'], pk['q'], K, precision)
+            start = pk['start']
+        else:
+            steps = budget.get('steps_per_copy_pair', CHORD_DEFAULT['steps_per_copy_pair']) * 2 * K
+            T, q, c = chord_schedule(steps, budget.get('T0', CHORD_DEFAULT['T0']), budget.get('T1', CHORD_DEFAULT['T1']),
+                                     budget.get('q', CHORD_DEFAULT['q']), budget.get('kappa', 0.0), precision=precision)
+            start = budget.get('start', 'rand')
+        dev = torch.device('cuda')
+        if precision == 'int':
+            Gt = torch.round(Gf * QSCALE).to(torch.int32).to(dev).contiguous()
+            hh = torch.round(hf * QSCALE).to(torch.int32).to(dev).contiguous()
+            tdt = torch.int32
+        else:
+            Gt, hh, tdt = Gf.to(dev).contiguous(), hf.to(dev).contiguous(), torch.float32
+        idx = meta['idx'] if meta is not None and 'idx' in meta else torch.arange(B)
+        inst = torch.as_tensor(np.asarray(idx, dtype=np.int64) & M32).to(torch.int32).to(dev)
+        from .arpeggiofx import anneal, check_status
+        s_, de, st, status = anneal(Gt, hh, 2 * K, na, torch.tensor(T, dtype=tdt, device=dev), q, inst,
+                                    (seed + ci * key_step) & 0xFFFFFFFFFFFFFFFF, start, policy,
+                                    None if c is None else torch.tensor(c, dtype=tdt, device=dev), precision)
+        check_status(status)
+        return s_.float().to(I['h'].device)
+    return solver

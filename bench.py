@@ -1,0 +1,333 @@
+#!/usr/bin/env python3
+"""Benchmark of the delta-encoded Ising MIMO detector path on B200.
+
+Workload (one step = one pass of the hot path over one batch): 32 users x 32 antennas, 16-QAM, 65536 seeded
+i.i.d. Rayleigh channel uses with SNR 6-22 dB in 2 dB steps (round robin over the batch), one-stage dDI
+(K = 1, 128 spins) around the hard MMSE guess, 32 anneals per use, Arpeggio first-accept in fixed point at
+the reference's x32 budget (abl_far_32_0.1_0.1_0_rand_8: 32 sweeps x 2 passes, T 0.1, q 0, random start),
+then the distance readout: map (Gram + MMSE + quantise) -> anneal -> readout, three launches.
+
+metric: detections/s (whole job, all ranks), inputs resident in HBM (1.07 GB of channels per rank: larger
+than L2, no flush needed).  e2e: the same through Detector with pinned host buffers (H, y copied in, bits and
+distances copied out, inside the timed region).  Under torchrun each rank detects its own batch (weak
+scaling, no collective on the data path).  --impl reference times the CPU restatement of the reference's
+chain (oracle) on this box's host cores on a bounded sample per step."""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(nt=32, nr=32, M=16, batch=65536, snrs=list(range(6, 23, 2)), anneals=32, K=1, policy='arpeggio',
+                precision='int', sweeps=32, T0=0.1, T1=0.1, q=0.0, start='rand')
+METRIC = 'detections/s (16-QAM 32x32, 32 anneals, Arpeggio fixed point)'
+
+
+def config(args):
+    w = WORKLOAD
+    return {'workload': 'x32 one-stage dDI detection: %d users x %d antennas 16-QAM, %d channels/rank, SNR %d-%d dB '
+                        'step 2, %d anneals, Arpeggio first-accept fixed point S=%d T=%g q=%g start=%s, K=%d (128 spins)'
+                        % (w['nt'], w['nr'], args.batch, w['snrs'][0], w['snrs'][-1], args.anneals, w['sweeps'],
+                           w['T0'], w['q'], w['start'], w['K']),
+            'batch_per_rank': args.batch, 'anneals': args.anneals, 'users': w['nt'], 'antennas': w['nr'],
+            'modulation': '16-QAM', 'policy': w['policy'], 'fields': 'int32 fixed point (Q=4096)',
+            'l2': 'inputs larger than L2 (H is %.2f GB per rank), no flush' % (args.batch * 4 * 64 * 64 / 1e9),
+            'parallelism': 'replicas x%d' % args.world}
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu):
+        self.gpu, self.p, self.f = gpu, None, None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+            self.p = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.Q,
+                                       '--format=csv,noheader,nounits', '-lms', '200'], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(', ') for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({n for r in rows if len(r) >= 9 for n, v in zip(names, r[5:9]) if v.strip() == 'Active'})
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(sm)}
+
+
+# ---------------------------------------------------------------- CPU chain (oracle restatement of the reference)
+def cpu_chain(H, y, N0, R, seed, nthreads):
+    """Float64 MMSE guess + dDI mapping + to_fixed/compress (numpy), the oracle's first-accept anneal on all
+    threads, then select: the reference's chain restated on the CPU (test infrastructure, timed as baseline)."""
+    from oracle import oracle as O
+    from arpeggio_b200.detector import arpeggio_schedule
+    w = WORKLOAD
+    B = H.shape[0]
+    lv = np.asarray([-3, -1, 1, 3], dtype=np.float64)
+    el2 = float((lv ** 2).mean())
+    Hd = H.astype(np.float64)
+    Gm = np.einsum('bki,bkj->bij', Hd, Hd)
+    A = Gm + ((N0 / 2) / el2)[:, None, None] * np.eye(Hd.shape[-1])
+    z = np.linalg.solve(A, np.einsum('bki,bk->bi', Hd, y.astype(np.float64))[..., None])[..., 0]
+    mu = np.diagonal(np.linalg.solve(A, Gm), axis1=-2, axis2=-1)
+    xq = O.quantize_levels(z / mu, 16)
+    Gf, hf, _ = O.ising_delta_compressed(H, y, xq)
+    G, h = O.quantize_compressed(Gf, hf)
+    T, q, _ = arpeggio_schedule(w['sweeps'], w['T0'], w['T1'], w['q'], w['K'])
+    s, _, _ = O.anneal_dd(G, h, 2 * w['K'], R, T, q, np.arange(B), seed, w['start'], nthreads=nthreads)
+    cand = O.spins_to_levels_delta(s, xq, w['K'], 16)
+    sel, _ = O.select(H, y, cand, xq)
+    return O.levels_to_bits(sel, 16)
+
+
+def cpu_sample(args, nthreads, target_s):
+    """Sized sample of the same workload for the CPU chain: returns (detections/s, sample description)."""
+    import torch
+    from arpeggio_b200 import channel
+    w = WORKLOAD
+    n = 32
+    rate = None
+    while True:
+        snr = torch.tensor([w['snrs'][i % len(w['snrs'])] for i in range(n)], dtype=torch.float32)
+        d = channel.draw_device(4321, snr, n, w['nt'], w['M'], dev='cpu')
+        H, y, N0 = d['H'].numpy(), d['y'].numpy(), d['N0'].double().numpy()
+        t0 = time.perf_counter()
+        cpu_chain(H, y, N0, args.anneals, 7, nthreads)
+        dt = time.perf_counter() - t0
+        rate = n / dt
+        if dt >= 0.5 * target_s or n >= args.batch:
+            return rate, n, dt
+        n = int(min(args.batch, max(2 * n, rate * target_s)))
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from arpeggio_b200 import _lib, channel, detector
+    rank, world, local = args.rank, args.world, args.local
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    w = WORKLOAD
+    B = args.batch
+    snr = torch.tensor([w['snrs'][i % len(w['snrs'])] for i in range(B)], dtype=torch.float32)
+    data = channel.draw_device(1234 + rank, snr, B, w['nt'], w['M'], dev=dev)
+    det = detector.Detector(B, w['nt'], w['nr'], w['M'], w['policy'], args.anneals, w['K'], sweeps=w['sweeps'],
+                            T0=w['T0'], T1=w['T1'], q=w['q'], start=w['start'], precision=w['precision'], device=dev)
+    det.set_noise(N0=data['N0'])
+    H, y = data['H'], data['y']
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        det.run(H, y, seed=1000 + i)
+    torch.cuda.synchronize()
+    det.check()
+    barrier()
+    K = args.steps
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(K):
+        det.run(H, y, seed=2000 + i, events=evs[i])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ck = clocks.stop()
+    det.check()
+    ms = t_start.elapsed_time(t_end) / K
+    stage = [sum(evs[i][s].elapsed_time(evs[i][s + 1]) for i in range(K)) / K for s in range(3)]
+    st = det.st.sum((0, 1)).tolist()  # flips, tests of the last step
+
+    # ---- end to end through the public API with pinned host buffers
+    Hh = H.cpu().pin_memory()
+    yh = y.cpu().pin_memory()
+    bits_h = torch.empty(det.bits.shape, dtype=torch.int8).pin_memory()
+    dist_h = torch.empty(B, dtype=torch.float32).pin_memory()
+    Hd, yd = torch.empty_like(H), torch.empty_like(y)
+
+    def e2e_step(seed):
+        Hd.copy_(Hh, non_blocking=True)
+        yd.copy_(yh, non_blocking=True)
+        bits, _, dd = det.run(Hd, yd, seed)
+        bits_h.copy_(bits, non_blocking=True)
+        dist_h.copy_(dd, non_blocking=True)
+
+    for i in range(max(1, args.warmup // 2)):
+        e2e_step(3000 + i)
+    torch.cuda.synchronize()
+    barrier()
+    Ke = max(1, min(K, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(Ke):
+        e2e_step(4000 + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    det.check()
+    ms_e2e = e0.elapsed_time(e1) / Ke
+
+    # ---- integer-issue peak (calibration kernel) and the anneal kernel's algorithmic work
+    L = _lib.lib()
+    buf = torch.zeros(1, dtype=torch.int32, device=dev)
+    nb, nth, it = 148 * 16, 256, 256
+    L.arp_philox_rate(_lib.ptr(buf), nb, nth, 8, _lib.stream_ptr())
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    _lib.check(L.arp_philox_rate(_lib.ptr(buf), nb, nth, it, _lib.stream_ptr()), 'philox_rate')
+    c1.record(stream)
+    torch.cuda.synchronize()
+    peak_blocks = nb * nth * it / (c0.elapsed_time(c1) / 1e3)
+
+    ms_all = torch.tensor([ms, ms_e2e] + stage, dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms_all, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = float(ms_all[0]), float(ms_all[1])
+    stage = [float(v) for v in ms_all[2:]]
+    if rank != 0:
+        return None
+    D, P, R = 2 * w['nt'], 2 * w['K'], args.anneals
+    Lp = len(det.schedule['T'])
+    nquad = -(-Lp // (4 * P))
+    blocks = B * R * (P * D * nquad + (P * D if w['start'] == 'rand' else D))
+    ops = 100.0 * blocks + 5.0 * B * R * D * Lp + 3.0 * D * st[0]
+    t_anneal = stage[1] / 1e3
+    peak_ops = 100.0 * peak_blocks
+    traffic = None
+    tf = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(tf):
+        tj = json.load(open(tf)).get('anneal_first_accept_x32')
+        if tj:
+            traffic = tj['bytes_per_detection'] * B
+    alg_bytes = B * (D * D * 4 + D * 4) + B * R * (P * D + 24)
+    peaks = {}
+    pf = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(pf):
+        peaks = json.load(open(pf))
+    hbm_peak = peaks.get('hbm_gbs', 6650.0)
+    line = {
+        'metric': METRIC, 'value': world * B / (ms / 1e3), 'unit': 'detections/s', 'n_gpus': world,
+        'steps': K, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'int32', 'data': 'synthetic (seeded Rayleigh draws on the device)',
+        'config': config(args),
+        'e2e': {'value': world * B / (ms_e2e / 1e3), 'unit': 'detections/s',
+                'h2d_bytes_per_step': int(H.numel() * 4 + y.numel() * 4),
+                'd2h_bytes_per_step': int(det.bits.numel() + B * 4), 'ms_per_step': ms_e2e, 'steps': Ke},
+        'stages_ms': {'map': stage[0], 'anneal': stage[1], 'readout': stage[2]},
+        'roofline': {'bound': 'int_issue', 'achieved': ops / t_anneal / 1e9, 'peak': peak_ops / 1e9,
+                     'unit': 'Gop/s', 'frac': ops / t_anneal / peak_ops, 'traffic': traffic,
+                     'kernel': 'k_anneal_dd<2,2,first-accept,int32>',
+                     'ops_model': '100 per Philox4x32-10 block + 5 per lane decision + 3 per field update',
+                     'peak_source': 'measured in this run: arp_philox_rate (chained Philox blocks, all SMs); '
+                                    'MEASURED_PEAKS.json has no integer peak'},
+        'roofline_hbm': {'bound': 'hbm', 'achieved': alg_bytes / t_anneal / 1e9, 'peak': hbm_peak, 'unit': 'GB/s',
+                         'frac': alg_bytes / t_anneal / 1e9 / hbm_peak,
+                         'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if peaks else 'fallback'},
+        'anneal_counters': {'flips': int(st[0]), 'tests': int(st[1]), 'anneals': B * R, 'philox_blocks': blocks},
+        'gpu_launches': 3 * K,
+        'clocks': ck,
+    }
+    if world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        rate, n, dt = cpu_sample(args, nthreads, 12.0)
+        line['cpu_baseline'] = {'value': rate, 'unit': 'detections/s', 'cores': nthreads, 'kind': 'port',
+                                'sample': '%d channel uses of the same workload (same SNR mix, 32 anneals), full CPU '
+                                          'chain (float64 MMSE + mapping, oracle first-accept anneal on %d threads, '
+                                          'select), %.1f s' % (n, nthreads, dt)}
+    return line
+
+
+def run_reference(args):
+    """CPU restatement of the reference's chain, rank 0 only, each step a bounded sample of the workload."""
+    if args.rank != 0:
+        return None
+    nthreads = os.cpu_count() or 1
+    rate, n, dt = cpu_sample(args, nthreads, 4.0)
+    import torch
+    from arpeggio_b200 import channel
+    w = WORKLOAD
+    snr = torch.tensor([w['snrs'][i % len(w['snrs'])] for i in range(n)], dtype=torch.float32)
+    d = channel.draw_device(999, snr, n, w['nt'], w['M'], dev='cpu')
+    H, y, N0 = d['H'].numpy(), d['y'].numpy(), d['N0'].double().numpy()
+    for i in range(args.warmup):
+        cpu_chain(H[:max(1, n // 8)], y[:max(1, n // 8)], N0[:max(1, n // 8)], args.anneals, i, nthreads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        cpu_chain(H, y, N0, args.anneals, 100 + i, nthreads)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = n / dt
+    return {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'detections/s', 'n_gpus': args.world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': dt * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int32', 'data': 'synthetic', 'config': config(args),
+            'cpu_baseline': {'value': v, 'unit': 'detections/s', 'cores': nthreads, 'kind': 'port',
+                             'sample': '%d channel uses per step of the same workload' % n},
+            'e2e': {'value': v, 'unit': 'detections/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--batch', type=int, default=WORKLOAD['batch'])
+    ap.add_argument('--anneals', type=int, default=WORKLOAD['anneals'])
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    args.rank = int(os.environ.get('RANK', 0))
+    args.world = int(os.environ.get('WORLD_SIZE', 1))
+    args.local = int(os.environ.get('LOCAL_RANK', 0))
+    if args.impl == 'reference':
+        line = run_reference(args)
+    else:
+        if args.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(args.local)
+            dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+        line = run_ours(args)
+        if args.world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == '__main__':
+    main()

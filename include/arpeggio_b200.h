@@ -1,0 +1,110 @@
+/*
+ * arpeggio_b200 -- C ABI of the B200 (sm_100a) delta-encoded Ising MIMO detector path.
+ *
+ * Plain pointers and sizes; every array argument is DEVICE memory unless stated otherwise.  No entry
+ * point allocates memory.  Every entry point is stream-ordered on `stream` (a cudaStream_t, or NULL
+ * for the legacy default stream) and returns without synchronising.  Return value: ARP_OK or an
+ * ARP_ERR_* code for errors found on the host (shapes, arguments, launch).  Errors that only the
+ * device can see (coefficients beyond the exact 32-bit field range) are written to `status`
+ * (one int32 in device memory, may be NULL; set to the first error code, never cleared here).
+ *
+ * Citations name the reference interface each entry point replaces (skethz/Arpeggio, path:line).
+ */
+#ifndef ARPEGGIO_B200_H
+#define ARPEGGIO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum arp_status_code {
+  ARP_OK = 0,
+  ARP_ERR_SHAPE = 1,     /* unsupported D, P, N, R, B or L */
+  ARP_ERR_RANGE = 2,     /* coefficients or schedule beyond the exact 32-bit field range */
+  ARP_ERR_ARG = 3,       /* null pointer or bad enum value */
+  ARP_ERR_LAUNCH = 4,    /* CUDA launch or configuration error */
+  ARP_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+  ARP_ERR_WORKSPACE = 6  /* caller's workspace smaller than arp_*_workspace_bytes() */
+};
+
+/* Library version string and a message for a status code (host only). */
+const char* arp_version(void);
+const char* arp_status_string(int code);
+
+/* Philox4x32-10 known-answer check on the device: in (n x 6 words: counter c0..c3, key k0, k1),
+ * out (n x 4 words).  Replaces chord_kernel.cu:26-32 `philox_kat` (launched by
+ * arpeggio/mimo/chordfx.py:180-187). */
+int arp_philox_kat(const uint32_t* in, uint32_t* out, int n, void* stream);
+
+/* Integer-issue calibration: blocks x threads threads each run `iters` chained Philox4x32-10 blocks (the
+ * anneal's dominant integer work).  `out` (one word) is written only by a one-in-2^32 coincidence.  No
+ * reference counterpart: it measures the peak the benchmark's integer roofline divides by. */
+int arp_philox_rate(uint32_t* out, int blocks, int threads, int iters, void* stream);
+
+/* Fixed-point first-accept anneal (Arpeggio) on compressed dDI problems.
+ * Replaces arpeggio/sim/arpeggio_fx.cu:35-37 `arpeggio_fx` as launched by arpeggio/sim/arpeggiofx.py:40-42,
+ * same argument meaning: Gt (B, D, D) int32 transposed (Gt[b][j][i] = G[b][i][j]), h (B, D), T (L) one
+ * temperature per pass (pass k tests copy k % P), q, P in {2, 4, 6}, R anneals per problem, D <= 128,
+ * inst (B) instance numbers, Philox key (k0 = low, k1 = high word), start 0 = 'rand' / 1 = 'bal'.
+ * Outputs: out_s (B, R, P*D) int8 best spins copy-major, out_de (B, R) best energy change,
+ * out_st (B, R, 2) [flips, tests].  Bit-exact with the reference kernel and arpeggio_ref59.anneal. */
+int arp_anneal_first_accept(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P, int R,
+                            int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1, int start,
+                            int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);
+
+/* Fixed-point Chord round (snapshot test of the active copy, then in-order commits) on compressed dDI
+ * problems, with the Onsager term c (L, may be NULL).  Same arguments and outputs as
+ * arp_anneal_first_accept (tests = one per pass).  Replaces the compressed Chord of
+ * arpeggio/sim/x3model/chord_ref.py:72-123 (rng='philox') and mode 'par' of
+ * arpeggio/rtl/cycle_checks/rtl_a59/src/arpeggio_ref59.py:72-82; equals chordfx.chord_fx on the
+ * expanded problem (its 2 E0 minus the start state's). */
+int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L, int q,
+                        int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1, int start,
+                        int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);
+
+/* FP32-field anneal on compressed dDI problems: policy 0 = first accept, 1 = Chord round.  Gt, h, T, c
+ * (c may be NULL), q in float; out_de (B, R) float.  The float rule is the integer rule with the
+ * decision z < thr, z = (s w_j + 2 G_jj) + q, thr = ((x >> 8) 2^-24 - 1/2) 4 T, one IEEE rounding per
+ * operation.  The reference has no FP32 Philox kernel; the float semantics follow
+ * arpeggio/sim/arpx55.py:28-99 (arpeggio_seq, rule (2)). */
+int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, const float* T, const float* c, int L, float q,
+                      int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1, int start,
+                      int8_t* out_s, float* out_de, int64_t* out_st, int32_t* status, void* stream);
+
+/* Fixed-point Chord on a full int16 coupling J (B, N, N), h and h0 (B, N), Tq and Cq (S), with P phases.
+ * Replaces arpeggio/mimo/chord_kernel.cu:177-184 `chord_m{1,2,3,4,6,8}` as launched by
+ * arpeggio/mimo/chordfx.py:189-208 (Kernel.chord): N % 32 == 0, (N / P) % 32 == 0, N <= 256;
+ * mode 0 ('chains'): out_e (B, R), out_s (B, R, N); mode 1 ('best'): out_e (B), out_s (B, N).
+ * out_e is 2 E0 (int64).  stats (4 counters: flips, energy evaluations, Philox blocks, steps x anneals)
+ * may be NULL.  warps = anneals per block in flight (the reference's `warps`, <= 8). */
+int arp_anneal_chord(const int16_t* J, const int32_t* h, const int32_t* h0, const int32_t* Tq, const int32_t* Cq,
+                     int q, int S, int P, int R, int N, int B, uint32_t k0, uint32_t k1, uint32_t inst0, int mode,
+                     int warps, int64_t* out_e, int8_t* out_s, unsigned long long* stats, int32_t* status,
+                     void* stream);
+
+/* Gram / field formation with the MMSE guess, per channel use (one block each).  H (B, NR2, D) float32
+ * real-lifted channels [[Re, -Im], [Im, Re]] scaled by the constellation factor, y (B, NR2), sigma2 (B)
+ * the MMSE regulariser (N0/2)/E[l^2], M in {4, 16}.  Outputs: G (B, D, D) = H^T H / scale (symmetric, so
+ * also its own transpose Gt), h (B, D) = 2 H^T (y - H x_q) / scale, x_q (B, D) int8 hard MMSE guess,
+ * scale (B).  quantize != 0: G and h are int32 round(x * 4096) (the integer problem); else float32.
+ * Replaces the host chain mimo.mmse / mimo._mu / quantize_levels (arpeggio/mimo/mimo.py:86-109, 176-182),
+ * mimo.ising_delta_at (mimo.py:506-523), chordfx.to_fixed (chordfx.py:60-76) and chord_ref.compress
+ * (arpeggio/sim/x3model/chord_ref.py:47-59) as run_a513.detect calls them (run_a513.py:107-111). */
+int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M, int quantize,
+               void* G, void* h, int8_t* xq, float* scale, int32_t* status, void* stream);
+
+/* Readout: candidate levels clip(x_q + sum_p s_p) of each anneal's best spins (B, R, P*D), their distance
+ * ||y - H x||^2, the first minimum over the R candidates and then the guess, Gray bits (MSB first per
+ * dimension).  Outputs levels (B, D) int8, bits (B, D * log2(M)/2) int8, dist (B) float32, pick (B) int32
+ * (index of the winner, R = the guess; may be NULL).  Replaces mimo.spins_to_levels_delta, mimo.dist,
+ * mimo.select and mimo.levels_to_bits (arpeggio/mimo/mimo.py:185-190, 416-425, 45-51). */
+int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D,
+                   int P, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARPEGGIO_B200_H */

@@ -20,7 +20,6 @@ namespace arp {
 
 constexpr int kMapThreads = 256;
 constexpr int kChunk = 32;
-constexpr int kMaxE = 64;  // Gram entries per thread: D^2 / 256 for D <= 128
 
 struct MapParams {
   const float* H;       // (B, NR2, D)
@@ -50,121 +49,192 @@ __device__ __forceinline__ float nearest_level(float v, int M) {
   return best;
 }
 
+// Half-warp sum (the 16 threads that share a tile row).
+__device__ __forceinline__ float hsum16(float v) {
+#pragma unroll
+  for (int o = 8; o; o >>= 1) v += __shfl_xor_sync(ARP_FULL, v, o);
+  return v;
+}
+
+// The D x D work is tiled over a 16 x 16 thread grid: thread (ty, tx) owns rows ty*TB .. ty*TB+TB-1 and
+// columns tx*TB .. tx*TB+TB-1 of Q and of the inverse, in registers.  Dp = 16 TB >= D; padded rows and
+// columns of H are zero and the padded diagonal of A is 1, so the inverse's D x D block is unchanged.
+template <int TB>
 __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
+  constexpr int Dp = 16 * TB, QP = Dp + 4;
   extern __shared__ __align__(16) float sm[];
-  const int D = a.D, NR2 = a.NR2, DP = D + 1;
-  float* Hc = sm;                 // kChunk x D
-  float* Qs = Hc + kChunk * D;    // D x DP
-  float* Ai = Qs + D * DP;        // D x DP
-  float* gv = Ai + D * DP;        // D
-  float* xv = gv + D;             // D
-  float* rk = xv + D;             // D
-  float* ck = rk + D;             // D
-  float* red = ck + D;            // 32
-  const int tid = threadIdx.x, b = blockIdx.x;
+  float* Hc = sm;                 // kChunk x Dp
+  float* Qs = Hc + kChunk * Dp;   // Dp x QP
+  float* rk = Qs + Dp * QP;       // 2 x Dp (double-buffered row k)
+  float* ck = rk + 2 * Dp;        // 2 x Dp (double-buffered column k)
+  float* gv = ck + 2 * Dp;        // Dp
+  float* xv = gv + Dp;            // Dp
+  float* red = xv + Dp;           // 8
+  const int D = a.D, NR2 = a.NR2, b = blockIdx.x;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4, lane = tid & 31;
   const float* Hb = a.H + (size_t)b * NR2 * D;
   const float* yb = a.y + (size_t)b * NR2;
-  float acc[kMaxE];
+  float A[TB][TB];
 #pragma unroll
-  for (int m = 0; m < kMaxE; ++m) acc[m] = 0.0f;
+  for (int i = 0; i < TB; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) A[i][j] = 0.0f;
   float gacc = 0.0f;
+  // ---- Q = H^T H and g = H^T y over 32-row chunks (every Q_ij, Q_ji is the same ordered fma chain)
   for (int r0 = 0; r0 < NR2; r0 += kChunk) {
     const int nr = min(kChunk, NR2 - r0);
     __syncthreads();
-    for (int x = tid; x < nr * D; x += kMapThreads) Hc[x] = Hb[(size_t)r0 * D + x];
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < kMaxE; ++m) {
-      const int e = tid + m * kMapThreads;
-      if (e < D * D) {
-        const int i = e / D, j = e - (e / D) * D;
-        float s = acc[m];
-        for (int r = 0; r < nr; ++r) s = __fmaf_rn(Hc[r * D + i], Hc[r * D + j], s);
-        acc[m] = s;
-      }
+    for (int x = tid; x < kChunk * Dp; x += kMapThreads) {
+      const int r = x / Dp, j = x - r * Dp;
+      Hc[x] = (r < nr && j < D) ? Hb[(size_t)(r0 + r) * D + j] : 0.0f;
     }
-    if (tid < D)
-      for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * D + tid], yb[r0 + r], gacc);
+    __syncthreads();
+    for (int r = 0; r < nr; ++r) {
+      float ai[TB], bj[TB];
+#pragma unroll
+      for (int i = 0; i < TB; ++i) {
+        ai[i] = Hc[r * Dp + ty * TB + i];
+        bj[i] = Hc[r * Dp + tx * TB + i];
+      }
+#pragma unroll
+      for (int i = 0; i < TB; ++i)
+#pragma unroll
+        for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(ai[i], bj[j], A[i][j]);
+    }
+    if (tid < Dp)
+      for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * Dp + tid], yb[r0 + r], gacc);
   }
   float qmax = 0.0f;
+  const float s2 = a.sigma2[b];
 #pragma unroll
-  for (int m = 0; m < kMaxE; ++m) {
-    const int e = tid + m * kMapThreads;
-    if (e < D * D) {
-      const int i = e / D, j = e - (e / D) * D;
-      Qs[i * DP + j] = acc[m];
-      Ai[i * DP + j] = i == j ? __fadd_rn(acc[m], a.sigma2[b]) : acc[m];
-      qmax = fmaxf(qmax, fabsf(acc[m]));
+  for (int i = 0; i < TB; ++i)
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      const int gi = ty * TB + i, gj = tx * TB + j;
+      Qs[gi * QP + gj] = A[i][j];
+      qmax = fmaxf(qmax, fabsf(A[i][j]));
+      if (gi == gj) A[i][j] = gi < D ? __fadd_rn(A[i][j], s2) : 1.0f;
     }
+  if (tid < Dp) gv[tid] = gacc;
+  // ---- in-place Gauss-Jordan inverse of A = Q + sigma2 I (SPD, no pivoting), one barrier per step
+  for (int k = 0; k < Dp; ++k) {
+    const int kt = k / TB, kr = k - kt * TB, buf = (k & 1) * Dp;
+    if (ty == kt) {
+#pragma unroll
+      for (int j = 0; j < TB; ++j)
+        rk[buf + tx * TB + j] = A[kr][j];
+    }
+    if (tx == kt) {
+#pragma unroll
+      for (int i = 0; i < TB; ++i) ck[buf + ty * TB + i] = A[i][kr];
+    }
+    __syncthreads();
+    const float inv = __frcp_rn(rk[buf + k]);
+    float f[TB], rj[TB];
+#pragma unroll
+    for (int i = 0; i < TB; ++i) {
+      f[i] = __fmul_rn(ck[buf + ty * TB + i], inv);
+      rj[i] = rk[buf + tx * TB + i];
+    }
+#pragma unroll
+    for (int i = 0; i < TB; ++i)
+#pragma unroll
+      for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(-f[i], rj[j], A[i][j]);
+    if (ty == kt) {
+#pragma unroll
+      for (int j = 0; j < TB; ++j) A[kr][j] = __fmul_rn(rj[j], inv);
+    }
+    if (tx == kt) {
+#pragma unroll
+      for (int i = 0; i < TB; ++i) A[i][kr] = -f[i];
+    }
+    if (ty == kt && tx == kt) A[kr][kr] = inv;
   }
-  if (tid < D) gv[tid] = gacc;
-  // ---- in-place Gauss-Jordan inverse of A (SPD, no pivoting)
-  for (int k = 0; k < D; ++k) {
-    __syncthreads();
-    if (tid < D) {
-      rk[tid] = Ai[k * DP + tid];
-      ck[tid] = Ai[tid * DP + k];
+  // ---- z = A^-1 g, mu = diag(A^-1 Q) (Q symmetric: sum_j Ainv_ij Q_ij), x_q
+  float zp[TB], mp[TB];
+#pragma unroll
+  for (int i = 0; i < TB; ++i) {
+    zp[i] = 0.0f;
+    mp[i] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      zp[i] = __fmaf_rn(A[i][j], gv[tx * TB + j], zp[i]);
+      mp[i] = __fmaf_rn(A[i][j], Qs[(ty * TB + i) * QP + tx * TB + j], mp[i]);
     }
-    __syncthreads();
-    const float inv = __frcp_rn(rk[k]);
-    for (int e = tid; e < D * D; e += kMapThreads) {
-      const int i = e / D, j = e - (e / D) * D;
-      float v;
-      if (i == k)
-        v = j == k ? inv : __fmul_rn(rk[j], inv);
-      else if (j == k)
-        v = -__fmul_rn(ck[i], inv);
-      else
-        v = __fmaf_rn(-__fmul_rn(ck[i], inv), rk[j], Ai[i * DP + j]);
-      Ai[i * DP + j] = v;
+    zp[i] = hsum16(zp[i]);
+    mp[i] = hsum16(mp[i]);
+  }
+  if (tx == 0) {
+#pragma unroll
+    for (int i = 0; i < TB; ++i) {
+      const int gi = ty * TB + i;
+      const float lv = gi < D ? nearest_level(__fdiv_rn(zp[i], mp[i]), a.M) : 0.0f;
+      xv[gi] = lv;
+      if (gi < D) a.xq[(size_t)b * D + gi] = (int8_t)lv;
     }
   }
   __syncthreads();
-  // ---- z = A^-1 g, mu = diag(A^-1 Q), x_q
-  if (tid < D) {
-    float z = 0.0f, mu = 0.0f;
-    for (int j = 0; j < D; ++j) {
-      z = __fmaf_rn(Ai[tid * DP + j], gv[j], z);
-      mu = __fmaf_rn(Ai[tid * DP + j], Qs[j * DP + tid], mu);
-    }
-    const float lv = nearest_level(__fdiv_rn(z, mu), a.M);
-    xv[tid] = lv;
-    a.xq[(size_t)b * D + tid] = (int8_t)lv;
-  }
-  __syncthreads();
-  // ---- h = 2 (g - Q x_q), scale
-  float hval = 0.0f;
-  if (tid < D) {
-    float s = 0.0f;
-    for (int j = 0; j < D; ++j) s = __fmaf_rn(Qs[tid * DP + j], xv[j], s);
-    hval = __fmul_rn(2.0f, __fsub_rn(gv[tid], s));
-    qmax = fmaxf(qmax, fabsf(hval));
+  // ---- h = 2 (g - Q x_q), scale = max(|h|, |Q|)
+  float hp[TB];
+#pragma unroll
+  for (int i = 0; i < TB; ++i) {
+    hp[i] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < TB; ++j) hp[i] = __fmaf_rn(Qs[(ty * TB + i) * QP + tx * TB + j], xv[tx * TB + j], hp[i]);
+    hp[i] = hsum16(hp[i]);
+    hp[i] = __fmul_rn(2.0f, __fsub_rn(gv[ty * TB + i], hp[i]));
+    if (ty * TB + i < D) qmax = fmaxf(qmax, fabsf(hp[i]));
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) qmax = fmaxf(qmax, __shfl_xor_sync(ARP_FULL, qmax, o));
-  if ((tid & 31) == 0) red[tid >> 5] = qmax;
+  if (lane == 0) red[tid >> 5] = qmax;
   __syncthreads();
   float sc = 0.0f;
+#pragma unroll
   for (int w = 0; w < kMapThreads / 32; ++w) sc = fmaxf(sc, red[w]);
   sc = fmaxf(sc, 1e-12f);
   if (tid == 0) a.scale[b] = sc;
-  // ---- outputs
-  if (a.qscale > 0.0f) {
-    int32_t* Go = reinterpret_cast<int32_t*>(a.G) + (size_t)b * D * D;
-    for (int e = tid; e < D * D; e += kMapThreads) {
-      const int i = e / D, j = e - (e / D) * D;
-      Go[e] = (int32_t)rintf(__fmul_rn(__fdiv_rn(Qs[i * DP + j], sc), a.qscale));
+  // ---- outputs: G = Q / scale (x 4096, rounded half to even), h likewise
+  const bool quant = a.qscale > 0.0f;
+#pragma unroll
+  for (int i = 0; i < TB; ++i) {
+    const int gi = ty * TB + i;
+    if (gi >= D) continue;
+#pragma unroll
+    for (int j = 0; j < TB; ++j) {
+      const int gj = tx * TB + j;
+      if (gj >= D) continue;
+      const float v = __fdiv_rn(Qs[gi * QP + gj], sc);
+      if (quant)
+        reinterpret_cast<int32_t*>(a.G)[((size_t)b * D + gi) * D + gj] = (int32_t)rintf(__fmul_rn(v, a.qscale));
+      else
+        reinterpret_cast<float*>(a.G)[((size_t)b * D + gi) * D + gj] = v;
     }
-    if (tid < D)
-      reinterpret_cast<int32_t*>(a.h)[(size_t)b * D + tid] = (int32_t)rintf(__fmul_rn(__fdiv_rn(hval, sc), a.qscale));
-  } else {
-    float* Go = reinterpret_cast<float*>(a.G) + (size_t)b * D * D;
-    for (int e = tid; e < D * D; e += kMapThreads) {
-      const int i = e / D, j = e - (e / D) * D;
-      Go[e] = __fdiv_rn(Qs[i * DP + j], sc);
+    if (tx == 0) {
+      const float v = __fdiv_rn(hp[i], sc);
+      if (quant)
+        reinterpret_cast<int32_t*>(a.h)[(size_t)b * D + gi] = (int32_t)rintf(__fmul_rn(v, a.qscale));
+      else
+        reinterpret_cast<float*>(a.h)[(size_t)b * D + gi] = v;
     }
-    if (tid < D) reinterpret_cast<float*>(a.h)[(size_t)b * D + tid] = __fdiv_rn(hval, sc);
   }
+}
+
+template <int TB>
+static size_t map_smem() {
+  constexpr int Dp = 16 * TB;
+  return sizeof(float) * ((size_t)kChunk * Dp + (size_t)Dp * (Dp + 4) + 6 * (size_t)Dp + 8);
+}
+
+template <int TB>
+static cudaError_t launch_map(const MapParams& a, cudaStream_t st) {
+  const size_t smem = map_smem<TB>();
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_map_dd<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_map_dd<TB><<<a.B, kMapThreads, smem, st>>>(a);
+  return cudaGetLastError();
 }
 
 struct ReadParams {
@@ -181,39 +251,76 @@ struct ReadParams {
 
 constexpr int kReadThreads = 256;
 
+// One block per channel use.  H is staged transposed with a padded stride (Hs[j][i], NR2 + 1) so that the
+// 32 lanes of a warp, which own rows i = lane + 32 m, read consecutive words.  r0 = y - H x_q is formed once;
+// candidate c's residual is r0 - sum_j H[:, j] e_j over the few coordinates where its clipped level differs
+// from the guess (e = x - x_q), and its distance is ||r||^2.
 __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a) {
   extern __shared__ __align__(16) float sm[];
   const int D = a.D, NR2 = a.NR2, P = a.P, R = a.R, b = blockIdx.x;
-  float* Hs = sm;                   // NR2 x D
-  float* ys = Hs + NR2 * D;         // NR2
-  float* xs = ys + NR2;             // 8 warps x D candidate levels
-  float* bd = xs + 8 * D;           // 8
+  const int HS = NR2 + 1;
+  float* Hs = sm;                   // D x HS (transposed)
+  float* r0 = Hs + D * HS;          // NR2
+  float* bd = r0 + NR2;             // 8
   int* br = reinterpret_cast<int*>(bd + 8);
+  int8_t* xq8 = reinterpret_cast<int8_t*>(br + 8);  // D
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, W = kReadThreads / 32;
-  const float lo = a.M == 4 ? -1.0f : -3.0f, hi = -lo;
-  for (int x = tid; x < NR2 * D; x += kReadThreads) Hs[x] = a.H[(size_t)b * NR2 * D + x];
-  for (int x = tid; x < NR2; x += kReadThreads) ys[x] = a.y[(size_t)b * NR2 + x];
+  const int lo = a.M == 4 ? -1 : -3, hi = -lo;
+  const float* Hb = a.H + (size_t)b * NR2 * D;
+  for (int x = tid; x < NR2 * D; x += kReadThreads) {
+    const int i = x / D, j = x - i * D;
+    Hs[j * HS + i] = Hb[x];
+  }
+  for (int j = tid; j < D; j += kReadThreads) xq8[j] = a.xq[(size_t)b * D + j];
+  __syncthreads();
+  for (int i = tid; i < NR2; i += kReadThreads) {
+    float r = a.y[(size_t)b * NR2 + i];
+    for (int j = 0; j < D; ++j) r = __fmaf_rn(-Hs[j * HS + i], (float)xq8[j], r);
+    r0[i] = r;
+  }
   __syncthreads();
   float best = FLT_MAX;
   int bi = INT_MAX;
-  float* xw = xs + wid * D;
   for (int c = wid; c <= R; c += W) {
-    for (int j = lane; j < D; j += 32) {
-      float v = (float)a.xq[(size_t)b * D + j];
-      if (c < R) {
-        const int8_t* s = a.spins + ((size_t)b * R + c) * P * D;
-        int d = 0;
-        for (int p = 0; p < P; ++p) d += s[p * D + j];
-        v = fminf(fmaxf(v + (float)d, lo), hi);
-      }
-      xw[j] = v;
-    }
-    __syncwarp();
     float acc = 0.0f;
-    for (int i = lane; i < NR2; i += 32) {
-      float r = ys[i];
-      for (int j = 0; j < D; ++j) r = __fmaf_rn(-Hs[i * D + j], xw[j], r);
-      acc = __fmaf_rn(r, r, acc);
+    if (c == R) {
+      for (int i = lane; i < NR2; i += 32) acc = __fmaf_rn(r0[i], r0[i], acc);
+    } else {
+      const int8_t* s = a.spins + ((size_t)b * R + c) * P * D;
+      // e_j for the lanes' coordinates, then the warp walks the nonzero ones
+      int ej[4];
+      uint32_t nzm[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int j = t * 32 + lane;
+        int e = 0;
+        if (j < D) {
+          int d = 0;
+          for (int p = 0; p < P; ++p) d += s[p * D + j];
+          const int x = min(max((int)xq8[j] + d, lo), hi);
+          e = x - xq8[j];
+        }
+        ej[t] = e;
+        nzm[t] = __ballot_sync(ARP_FULL, e != 0);
+      }
+      float rr[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) rr[m] = (lane + 32 * m < NR2) ? r0[lane + 32 * m] : 0.0f;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        uint32_t mm = nzm[t];
+        while (mm) {
+          const int l = __ffs(mm) - 1;
+          mm &= mm - 1u;
+          const int j = t * 32 + l;
+          const float e = (float)__shfl_sync(ARP_FULL, ej[t], l);
+#pragma unroll
+          for (int m = 0; m < 8; ++m)
+            if (lane + 32 * m < NR2) rr[m] = __fmaf_rn(-Hs[j * HS + lane + 32 * m], e, rr[m]);
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 8; ++m) acc = __fmaf_rn(rr[m], rr[m], acc);
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(ARP_FULL, acc, o);
@@ -221,7 +328,6 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
       best = acc;
       bi = c;
     }
-    __syncwarp();
   }
   if (lane == 0) {
     bd[wid] = best;
@@ -237,12 +343,12 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
     }
   const int nb = a.M == 4 ? 1 : 2;
   for (int j = tid; j < D; j += kReadThreads) {
-    int v = a.xq[(size_t)b * D + j];
+    int v = xq8[j];
     if (gi < R) {
       const int8_t* s = a.spins + ((size_t)b * R + gi) * P * D;
       int d = 0;
       for (int p = 0; p < P; ++p) d += s[p * D + j];
-      v = min(max(v + d, (int)lo), (int)hi);
+      v = min(max(v + d, lo), hi);
     }
     a.levels[(size_t)b * D + j] = (int8_t)v;
     if (nb == 1) {
@@ -268,21 +374,20 @@ extern "C" int arp_map_dd(const float* H, const float* y, const float* sigma2, i
   if (B == 0) return ARP_OK;
   if (!H || !y || !sigma2 || !G || !h || !xq || !scale) return ARP_ERR_ARG;
   MapParams a{H, y, sigma2, B, NR2, D, M, quantize ? 4096.0f : 0.0f, G, h, xq, scale, status};
-  const size_t smem = sizeof(float) * ((size_t)kChunk * D + 2 * (size_t)D * (D + 1) + 4 * (size_t)D + 32);
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(k_map_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return ARP_ERR_LAUNCH;
-  k_map_dd<<<B, kMapThreads, smem, (cudaStream_t)stream>>>(a);
-  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = D <= 16 ? launch_map<1>(a, st) : D <= 32 ? launch_map<2>(a, st) : D <= 64 ? launch_map<4>(a, st)
+                                                                                   : launch_map<8>(a, st);
+  return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2,
                               int D, int P, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick,
                               void* stream) {
-  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || P < 1 || P > 6 || R < 0 || !(M == 4 || M == 16)) return ARP_ERR_SHAPE;
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || P < 1 || P > 6 || R < 0 || !(M == 4 || M == 16))
+    return ARP_ERR_SHAPE;
   if (B == 0) return ARP_OK;
   if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist) return ARP_ERR_ARG;
-  const size_t smem = sizeof(float) * ((size_t)NR2 * D + NR2 + 8 * (size_t)D + 8) + 8 * sizeof(int);
+  const size_t smem = sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + ((D + 15) & ~15);
   if (smem > 227 * 1024) return ARP_ERR_SHAPE;
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

@@ -86,7 +86,7 @@ def test_chord_full_bit_exact_vs_chord_fx(golden, name, mode):
     assert int(k.last_status.item()) == 0
     assert np.array_equal(s.cpu().numpy(), z['%s/%s_s' % (name, mode)])
     assert np.array_equal(e.cpu().numpy(), z['%s/%s_e' % (name, mode)])
-    assert int(stats[3].item()) == S * R
+    assert int(stats[3].item()) == S * R * F["h"].shape[0]
 
 
 def _random_dd(B, D, K, snr, seed):

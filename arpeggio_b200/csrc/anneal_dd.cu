@@ -340,10 +340,235 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
   }
 }
 
+// Integer fields, margin form.  For the pass's copy p each lane keeps its margin mu = theta - s w (accept iff
+// mu > 0, one compare) instead of w; a flip of lane j (old spin so) moves every margin by -4 so s_i G_ij with s_i
+// the lane's spin at the start of the pass, and the flipped lane's own term so w_j = theta_j - mu_j gives the
+// energy change 4 so w_j + 8 G_jj = 4 (kappa_j - mu_j), kappa = theta + 2 G_jj.  At the end of the pass the
+// fields come back exactly as w = s (theta - mu).  Spins are per-thread bits (bit p*NS + t = coordinate
+// t*32 + lane of copy p is +1).  First accept: a ballot over the remaining lanes (index > last commit) finds
+// the first accepted lane; the number of ballots a pass takes is the reference's `tests` for that pass
+// (one, plus one after every flip that is not on the last lane).
+template <int NS, int P, bool CHORD, bool CACHE>
+__global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
+  constexpr int DP = NS * 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  int32_t* Gs = reinterpret_cast<int32_t*>(smem);
+  __shared__ int s_bad;
+  const int D = a.D, L = a.L, R = a.R;
+  const int b = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  const int32_t* hg = reinterpret_cast<const int32_t*>(a.h) + (size_t)b * D;
+  const int32_t* Tg = reinterpret_cast<const int32_t*>(a.T);
+  const int32_t* cg = reinterpret_cast<const int32_t*>(a.c);
+  {
+    const int32_t* Gg = reinterpret_cast<const int32_t*>(a.Gt) + (size_t)b * D * D;
+    bool bad = false;
+    for (int x = threadIdx.x; x < D * DP; x += blockDim.x) {
+      const int j = x / DP, i = x - j * DP;
+      const int32_t v = i < D ? Gg[(size_t)j * D + i] : 0;
+      bad |= (v > kMaxG || v < -kMaxG);
+      Gs[x] = v;
+    }
+    for (int x = threadIdx.x; x < D; x += blockDim.x) bad |= (hg[x] > kMaxH || hg[x] < -kMaxH);
+    for (int x = threadIdx.x; x < L; x += blockDim.x) {
+      bad |= (Tg[x] > kMaxT || Tg[x] < -kMaxT);
+      if (cg) bad |= (cg[x] > kMaxT || cg[x] < -kMaxT);
+    }
+    bad |= (a.qi > kMaxT || a.qi < -kMaxT);
+    if (bad) s_bad = 1;
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (threadIdx.x == 0) set_status(a.status, ARP_ERR_RANGE);
+    return;
+  }
+  const uint32_t inst = a.inst[b];
+  int32_t dg2[NS];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) {
+    const int j = t * 32 + lane;
+    dg2[t] = j < D ? 2 * Gs[j * DP + j] : 0;
+  }
+
+  for (int r = wid; r < R; r += W) {
+    // ---- start state (arpeggio_fx.cu:48-57), packed per thread
+    uint32_t sp = 0;
+    if (a.start == 0) {
+#pragma unroll
+      for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+          uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+          philox10(c0, c1, c2, c3, a.k0, a.k1);
+          if (c0 >= 0x80000000u) sp |= 1u << (p * NS + t);
+        }
+    } else {
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)(t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+        philox10(c0, c1, c2, c3, a.k0, a.k1);
+        const int pat = bal_pattern(P, (uint32_t)(((uint64_t)c0 * (uint64_t)bal_choose(P)) >> 32));
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+          if ((pat >> p) & 1) sp |= 1u << (p * NS + t);
+      }
+    }
+    // ---- fields w = h - 2 G m (arpeggio_fx.cu:58-66); m of coordinate j is broadcast from its owner lane
+    int32_t w[NS], mloc[NS];
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+      const int j = t * 32 + lane;
+      int m = 0;
+#pragma unroll
+      for (int p = 0; p < P; ++p) m += ((sp >> (p * NS + t)) & 1u) ? 1 : -1;
+      mloc[t] = j < D ? m : 0;
+      w[t] = j < D ? hg[j] : 0;
+    }
+#pragma unroll
+    for (int tj = 0; tj < NS; ++tj) {
+      const uint32_t nz = __ballot_sync(ARP_FULL, mloc[tj] != 0);
+      uint32_t mm = nz;
+      while (mm) {
+        const int l = __ffs(mm) - 1;
+        mm &= mm - 1u;
+        const int m2 = 2 * __shfl_sync(ARP_FULL, mloc[tj], l);
+        const int32_t* gr = Gs + (tj * 32 + l) * DP + lane;
+#pragma unroll
+        for (int t = 0; t < NS; ++t) w[t] -= m2 * gr[t * 32];
+      }
+    }
+    long long de = 0, best = 1LL << 62;
+    uint32_t bsp = sp;
+    int32_t flips = 0, tests = 0;
+    const int nquad = (L + 4 * P - 1) / (4 * P);
+    for (int q4 = 0; q4 < nquad; ++q4) {
+      uint32_t cw[CACHE ? P : 1][CACHE ? NS : 1][4];
+      if constexpr (CACHE) {
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int t = 0; t < NS; ++t) {
+            uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+            philox10(c0, c1, c2, c3, a.k0, a.k1);
+            cw[p][t][0] = c0;
+            cw[p][t][1] = c1;
+            cw[p][t][2] = c2;
+            cw[p][t][3] = c3;
+          }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const int k = (q4 * 4 + i) * P + p;
+          if (k >= L) break;
+          const int32_t Tk = Tg[k];
+          const long long A = 4LL * Tk;
+          const int32_t Bk = a.qi + 2 * Tk - ((CHORD && cg) ? cg[k] : 0);
+          int32_t mu[NS], kap[NS], cpos[NS];
+#pragma unroll
+          for (int t = 0; t < NS; ++t) {
+            uint32_t u;
+            if constexpr (CACHE) {
+              u = cw[p][t][i];
+            } else {
+              uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
+              philox10(c0, c1, c2, c3, a.k0, a.k1);
+              u = i == 0 ? c0 : (i == 1 ? c1 : (i == 2 ? c2 : c3));
+            }
+            const bool valid = t * 32 + lane < D;
+            const int32_t th = valid ? (int32_t)ceil_shift32(u, A) - dg2[t] - Bk : -(1 << 30);
+            const bool up = (sp >> (p * NS + t)) & 1u;
+            mu[t] = th - (up ? w[t] : -w[t]);
+            kap[t] = th + dg2[t];
+            cpos[t] = up ? -4 : 4;
+          }
+          // commit the flip of lane l of slot ts: energy, margins, spin bit
+          auto commit = [&](int ts, int l, int32_t vsel) {
+            const int32_t v = __shfl_sync(ARP_FULL, vsel, l);
+            const uint32_t spo = __shfl_sync(ARP_FULL, sp, l);
+            const bool so_up = (spo >> (p * NS + ts)) & 1u;
+            de += 4LL * v;
+            const int32_t* gr = Gs + (ts * 32 + l) * DP + lane;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) mu[t] += (so_up ? cpos[t] : -cpos[t]) * gr[t * 32];
+            if (lane == l) sp ^= 1u << (p * NS + ts);
+            ++flips;
+          };
+          if constexpr (!CHORD) {
+            int jl = -1;
+            for (;;) {
+              uint32_t am[NS];
+#pragma unroll
+              for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, mu[t] > 0 && t * 32 + lane > jl);
+              ++tests;
+              int ts = NS;
+              uint32_t m = 0;
+              int32_t vsel = 0;
+#pragma unroll
+              for (int t = NS - 1; t >= 0; --t)
+                if (am[t]) {
+                  ts = t;
+                  m = am[t];
+                  vsel = kap[t] - mu[t];
+                }
+              if (ts == NS) break;
+              const int l = __ffs(m) - 1;
+              commit(ts, l, vsel);
+              jl = ts * 32 + l;
+              if (jl == D - 1) break;
+            }
+          } else {
+            uint32_t am[NS];
+#pragma unroll
+            for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, mu[t] > 0);
+            ++tests;
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+              uint32_t m = am[t];
+              while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1u;
+                commit(t, l, kap[t] - mu[t]);
+              }
+            }
+          }
+          // fields back from the margins: s w = theta - mu with the pass-start spin
+#pragma unroll
+          for (int t = 0; t < NS; ++t) {
+            const int32_t swv = kap[t] - dg2[t] - mu[t];
+            w[t] = cpos[t] < 0 ? swv : -swv;
+          }
+          if (de < best) {  // best state after each pass (arpeggio_fx.cu:90-93)
+            best = de;
+            bsp = sp;
+          }
+        }
+      }
+    }
+    const size_t ar = (size_t)b * R + r;
+    int8_t* os = a.out_s + ar * P * D;
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        const int j = t * 32 + lane;
+        if (j < D) os[p * D + j] = ((bsp >> (p * NS + t)) & 1u) ? 1 : -1;
+      }
+    if (lane == 0) {
+      reinterpret_cast<long long*>(a.out_de)[ar] = best;
+      a.out_st[2 * ar] = flips;
+      a.out_st[2 * ar + 1] = tests;
+    }
+  }
+}
+
 template <int NS, int P, bool CHORD, bool FLT>
 static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   constexpr bool CACHE = P * NS <= 8;
-  auto kern = k_anneal_dd<NS, P, CHORD, FLT, CACHE>;
+  auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE>;
   const size_t smem = (size_t)a.D * NS * 32 * 4;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -19,7 +19,9 @@
 namespace arp {
 
 constexpr int kMapThreads = 256;
-constexpr int kChunk = 32;
+// Rows of H staged per chunk: all of a 64 x 64 problem at once; 32-row chunks for the 128-wide tiles.
+template <int TB>
+__host__ __device__ constexpr int kChunkRows() { return TB <= 4 ? 64 : 32; }
 
 struct MapParams {
   const float* H;       // (B, NR2, D)
@@ -63,8 +65,8 @@ template <int TB>
 __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
   constexpr int Dp = 16 * TB, QP = Dp + 4;
   extern __shared__ __align__(16) float sm[];
-  float* Hc = sm;                 // kChunk x Dp
-  float* Qs = Hc + kChunk * Dp;   // Dp x QP
+  float* Hc = sm;                            // kChunkRows x Dp
+  float* Qs = Hc + kChunkRows<TB>() * Dp;    // Dp x QP
   float* rk = Qs + Dp * QP;       // 2 x Dp (double-buffered row k)
   float* ck = rk + 2 * Dp;        // 2 x Dp (double-buffered column k)
   float* gv = ck + 2 * Dp;        // Dp
@@ -80,13 +82,20 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
 #pragma unroll
     for (int j = 0; j < TB; ++j) A[i][j] = 0.0f;
   float gacc = 0.0f;
-  // ---- Q = H^T H and g = H^T y over 32-row chunks (every Q_ij, Q_ji is the same ordered fma chain)
-  for (int r0 = 0; r0 < NR2; r0 += kChunk) {
-    const int nr = min(kChunk, NR2 - r0);
+  // ---- Q = H^T H and g = H^T y over row chunks (every Q_ij, Q_ji is the same ordered fma chain)
+  constexpr int CH = kChunkRows<TB>();
+  for (int r0 = 0; r0 < NR2; r0 += CH) {
+    const int nr = min(CH, NR2 - r0);
     __syncthreads();
-    for (int x = tid; x < kChunk * Dp; x += kMapThreads) {
-      const int r = x / Dp, j = x - r * Dp;
-      Hc[x] = (r < nr && j < D) ? Hb[(size_t)(r0 + r) * D + j] : 0.0f;
+    if (D == Dp && (D & 3) == 0) {
+      const float4* src = reinterpret_cast<const float4*>(Hb + (size_t)r0 * D);
+      float4* dst = reinterpret_cast<float4*>(Hc);
+      for (int x = tid; x < nr * Dp / 4; x += kMapThreads) dst[x] = src[x];
+    } else {
+      for (int x = tid; x < nr * Dp; x += kMapThreads) {
+        const int r = x / Dp, j = x - r * Dp;
+        Hc[x] = j < D ? Hb[(size_t)(r0 + r) * D + j] : 0.0f;
+      }
     }
     __syncthreads();
     for (int r = 0; r < nr; ++r) {
@@ -116,39 +125,42 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
       if (gi == gj) A[i][j] = gi < D ? __fadd_rn(A[i][j], s2) : 1.0f;
     }
   if (tid < Dp) gv[tid] = gacc;
-  // ---- in-place Gauss-Jordan inverse of A = Q + sigma2 I (SPD, no pivoting), one barrier per step
-  for (int k = 0; k < Dp; ++k) {
-    const int kt = k / TB, kr = k - kt * TB, buf = (k & 1) * Dp;
-    if (ty == kt) {
+  // ---- in-place Gauss-Jordan inverse of A = Q + sigma2 I (SPD, no pivoting), one barrier per step;
+  //      k = kt*TB + kr with kr unrolled so the register tile is always indexed at compile time
+  for (int kt = 0; kt < 16; ++kt) {
 #pragma unroll
-      for (int j = 0; j < TB; ++j)
-        rk[buf + tx * TB + j] = A[kr][j];
+    for (int kr = 0; kr < TB; ++kr) {
+      const int k = kt * TB + kr, buf = (k & 1) * Dp;
+      if (ty == kt) {
+#pragma unroll
+        for (int j = 0; j < TB; ++j) rk[buf + tx * TB + j] = A[kr][j];
+      }
+      if (tx == kt) {
+#pragma unroll
+        for (int i = 0; i < TB; ++i) ck[buf + ty * TB + i] = A[i][kr];
+      }
+      __syncthreads();
+      const float inv = __frcp_rn(rk[buf + k]);
+      float f[TB], rj[TB];
+#pragma unroll
+      for (int i = 0; i < TB; ++i) {
+        f[i] = __fmul_rn(ck[buf + ty * TB + i], inv);
+        rj[i] = rk[buf + tx * TB + i];
+      }
+#pragma unroll
+      for (int i = 0; i < TB; ++i)
+#pragma unroll
+        for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(-f[i], rj[j], A[i][j]);
+      if (ty == kt) {
+#pragma unroll
+        for (int j = 0; j < TB; ++j) A[kr][j] = __fmul_rn(rj[j], inv);
+      }
+      if (tx == kt) {
+#pragma unroll
+        for (int i = 0; i < TB; ++i) A[i][kr] = -f[i];
+        if (ty == kt) A[kr][kr] = inv;
+      }
     }
-    if (tx == kt) {
-#pragma unroll
-      for (int i = 0; i < TB; ++i) ck[buf + ty * TB + i] = A[i][kr];
-    }
-    __syncthreads();
-    const float inv = __frcp_rn(rk[buf + k]);
-    float f[TB], rj[TB];
-#pragma unroll
-    for (int i = 0; i < TB; ++i) {
-      f[i] = __fmul_rn(ck[buf + ty * TB + i], inv);
-      rj[i] = rk[buf + tx * TB + i];
-    }
-#pragma unroll
-    for (int i = 0; i < TB; ++i)
-#pragma unroll
-      for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(-f[i], rj[j], A[i][j]);
-    if (ty == kt) {
-#pragma unroll
-      for (int j = 0; j < TB; ++j) A[kr][j] = __fmul_rn(rj[j], inv);
-    }
-    if (tx == kt) {
-#pragma unroll
-      for (int i = 0; i < TB; ++i) A[i][kr] = -f[i];
-    }
-    if (ty == kt && tx == kt) A[kr][kr] = inv;
   }
   // ---- z = A^-1 g, mu = diag(A^-1 Q) (Q symmetric: sum_j Ainv_ij Q_ij), x_q
   float zp[TB], mp[TB];
@@ -223,7 +235,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
 template <int TB>
 static size_t map_smem() {
   constexpr int Dp = 16 * TB;
-  return sizeof(float) * ((size_t)kChunk * Dp + (size_t)Dp * (Dp + 4) + 6 * (size_t)Dp + 8);
+  return sizeof(float) * ((size_t)kChunkRows<TB>() * Dp + (size_t)Dp * (Dp + 4) + 6 * (size_t)Dp + 8);
 }
 
 template <int TB>

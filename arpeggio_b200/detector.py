@@ -121,45 +121,87 @@ class Detector:
         s2 = (N0 / 2) / el2(self.M)
         self.sigma2[:n].copy_(s2.float().expand(n) if s2.numel() == 1 else s2.float(), non_blocking=True)
 
-    def run(self, H, y, seed, n=None, inst0=0, stream=None, events=None):
-        """Stream-ordered detection of the first n uses; H (n, NR2, D) and y (n, NR2) float32 on the device.
-        Returns views of the device outputs (bits, levels, dist); nothing is synchronised.  events: optional
-        four CUDA events recorded before map, anneal, readout and after readout (per-stage timing)."""
+    def run(self, H, y, seed, n=None, inst0=0, stream=None, events=None, off=0):
+        """Stream-ordered detection of n uses; H (n, NR2, D) and y (n, NR2) float32 on the device, written to
+        slots off .. off+n-1 of the detector's buffers with instance numbers inst0 + off + i.  Returns views of
+        the device outputs (bits, levels, dist); nothing is synchronised.  events: optional four CUDA events
+        recorded before map, anneal, readout and after readout (per-stage timing)."""
         ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
-        n = self.B if n is None else n
-        if self._inst_base != (inst0, n):
-            iv = (np.arange(inst0, inst0 + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
-            self.inst[:n].copy_(torch.from_numpy(iv))
-            self._inst_base = (inst0, n)
+        n = self.B - off if n is None else n
+        if off < 0 or n < 0 or off + n > self.B:
+            raise ValueError('slots %d..%d outside the detector batch %d' % (off, off + n, self.B))
+        key = (inst0, off, n)
+        if self._inst_base != key:
+            iv = (np.arange(inst0 + off, inst0 + off + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
+            self.inst[off:off + n].copy_(torch.from_numpy(iv))
+            self._inst_base = key
         L = _lib.lib()
         sp = _lib.stream_ptr(stream)
         D, NR2, P, R = self.D, self.NR2, self.P, self.R
         f32 = self.precision == 'f32'
+        sl = slice(off, off + n)
+        G, h, xq, sc, s2, inst = self.G[sl], self.h[sl], self.xq[sl], self.scale[sl], self.sigma2[sl], self.inst[sl]
+        spins, de, st = self.spins[sl], self.de[sl], self.st[sl]
         ev(0)
-        _lib.check(L.arp_map_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.sigma2), n, NR2, D, self.M, 0 if f32 else 1,
-                                _lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.xq), _lib.ptr(self.scale),
-                                _lib.ptr(self.status), sp), 'map')
+        _lib.check(L.arp_map_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(s2), n, NR2, D, self.M, 0 if f32 else 1,
+                                _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), _lib.ptr(sc), _lib.ptr(self.status), sp), 'map')
         k0, k1, sv = seed & M32, (seed >> 32) & M32, 0 if self.start == 'rand' else 1
         ev(1)
-        outs = (_lib.ptr(self.spins), _lib.ptr(self.de), _lib.ptr(self.st), _lib.ptr(self.status), sp)
+        outs = (_lib.ptr(spins), _lib.ptr(de), _lib.ptr(st), _lib.ptr(self.status), sp)
         Lt = int(self.T.shape[0])
         if f32:
-            rc = L.arp_anneal_dd_f32(0 if self.policy == 'arpeggio' else 1, _lib.ptr(self.G), _lib.ptr(self.h),
+            rc = L.arp_anneal_dd_f32(0 if self.policy == 'arpeggio' else 1, _lib.ptr(G), _lib.ptr(h),
                                      _lib.ptr(self.T), _lib.ptr(self.c), Lt, float(self.q), P, R, D, n,
-                                     _lib.ptr(self.inst), k0, k1, sv, *outs)
+                                     _lib.ptr(inst), k0, k1, sv, *outs)
         elif self.policy == 'arpeggio':
-            rc = L.arp_anneal_first_accept(_lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.T), Lt, int(self.q), P,
-                                           R, D, n, _lib.ptr(self.inst), k0, k1, sv, *outs)
+            rc = L.arp_anneal_first_accept(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P,
+                                           R, D, n, _lib.ptr(inst), k0, k1, sv, *outs)
         else:
-            rc = L.arp_anneal_chord_dd(_lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.T), _lib.ptr(self.c), Lt,
-                                       int(self.q), P, R, D, n, _lib.ptr(self.inst), k0, k1, sv, *outs)
+            rc = L.arp_anneal_chord_dd(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), _lib.ptr(self.c), Lt,
+                                       int(self.q), P, R, D, n, _lib.ptr(inst), k0, k1, sv, *outs)
         _lib.check(rc, 'anneal')
         ev(2)
-        _lib.check(L.arp_readout_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.xq), _lib.ptr(self.spins), n, NR2, D, P,
-                                    R, self.M, _lib.ptr(self.levels), _lib.ptr(self.bits), _lib.ptr(self.dist),
-                                    _lib.ptr(self.pick), sp), 'readout')
+        levels, bits, dist, pick = self.levels[sl], self.bits[sl], self.dist[sl], self.pick[sl]
+        _lib.check(L.arp_readout_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(xq), _lib.ptr(spins), n, NR2, D, P,
+                                    R, self.M, _lib.ptr(levels), _lib.ptr(bits), _lib.ptr(dist),
+                                    _lib.ptr(pick), sp), 'readout')
         ev(3)
-        return self.bits[:n], self.levels[:n], self.dist[:n]
+        return bits, levels, dist
+
+    def run_host(self, Hh, yh, seed, bits_out, dist_out, Hd, yd, chunks=8, inst0=0, stream=None):
+        """End-to-end detection from pinned host buffers: the batch is cut into `chunks` pieces; the host to
+        device copy of piece c+1 (on a copy stream) overlaps the detection of piece c (on `stream`), and each
+        piece's bits and distances go back to the pinned outputs as soon as it is done.  Hd, yd: device
+        staging buffers of the batch's size.  Results equal one run() over the whole batch.  Stream-ordered:
+        synchronise `stream` before reading bits_out / dist_out."""
+        import torch
+        cs = stream if stream is not None else torch.cuda.current_stream()
+        if not hasattr(self, '_copy_stream'):
+            self._copy_stream = torch.cuda.Stream(device=self.device)
+            self._copy_events = []
+        xs = self._copy_stream
+        B = Hh.shape[0]
+        edges = [B * c // chunks for c in range(chunks + 1)]
+        while len(self._copy_events) < chunks + 1:
+            self._copy_events.append(torch.cuda.Event())
+        go = self._copy_events[chunks]
+        go.record(cs)
+        xs.wait_event(go)
+        for c in range(chunks):
+            a, b = edges[c], edges[c + 1]
+            with torch.cuda.stream(xs):
+                Hd[a:b].copy_(Hh[a:b], non_blocking=True)
+                yd[a:b].copy_(yh[a:b], non_blocking=True)
+                self._copy_events[c].record(xs)
+        for c in range(chunks):
+            a, b = edges[c], edges[c + 1]
+            if b == a:
+                continue
+            cs.wait_event(self._copy_events[c])
+            bits, _, dist = self.run(Hd[a:b], yd[a:b], seed, n=b - a, inst0=inst0, stream=cs, off=a)
+            with torch.cuda.stream(cs):
+                bits_out[a:b].copy_(bits, non_blocking=True)
+                dist_out[a:b].copy_(dist, non_blocking=True)
 
     def check(self):
         _lib.check(int(self.status.item()), 'device check')

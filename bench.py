@@ -180,11 +180,7 @@ def run_ours(args):
     Hd, yd = torch.empty_like(H), torch.empty_like(y)
 
     def e2e_step(seed):
-        Hd.copy_(Hh, non_blocking=True)
-        yd.copy_(yh, non_blocking=True)
-        bits, _, dd = det.run(Hd, yd, seed)
-        bits_h.copy_(bits, non_blocking=True)
-        dist_h.copy_(dd, non_blocking=True)
+        det.run_host(Hh, yh, seed, bits_h, dist_h, Hd, yd, chunks=args.chunks, stream=stream)
 
     for i in range(max(1, args.warmup // 2)):
         e2e_step(3000 + i)
@@ -245,7 +241,9 @@ def run_ours(args):
         'config': config(args),
         'e2e': {'value': world * B / (ms_e2e / 1e3), 'unit': 'detections/s',
                 'h2d_bytes_per_step': int(H.numel() * 4 + y.numel() * 4),
-                'd2h_bytes_per_step': int(det.bits.numel() + B * 4), 'ms_per_step': ms_e2e, 'steps': Ke},
+                'd2h_bytes_per_step': int(det.bits.numel() + B * 4), 'ms_per_step': ms_e2e, 'steps': Ke,
+                'path': 'Detector.run_host: pinned host H, y in; bits, distances out; %d pipelined pieces'
+                        % args.chunks},
         'stages_ms': {'map': stage[0], 'anneal': stage[1], 'readout': stage[2]},
         'roofline': {'bound': 'int_issue', 'achieved': ops / t_anneal / 1e9, 'peak': peak_ops / 1e9,
                      'unit': 'Gop/s', 'frac': ops / t_anneal / peak_ops, 'traffic': traffic,
@@ -306,6 +304,7 @@ def main():
     ap.add_argument('--batch', type=int, default=WORKLOAD['batch'])
     ap.add_argument('--anneals', type=int, default=WORKLOAD['anneals'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    ap.add_argument('--chunks', type=int, default=8, help='pipelined pieces of the end-to-end step')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.rank = int(os.environ.get('RANK', 0))

@@ -290,3 +290,21 @@ def test_side_stream_and_repeatability():
     det.check()
     for a_, b_ in zip(o1, o2):
         assert torch.equal(a_, b_)
+
+
+def test_pipelined_host_path_equals_one_run():
+    """Detector.run_host (pinned host buffers, pieces overlapped with copies) gives exactly the one-run outputs."""
+    from arpeggio_b200 import channel, detector
+    B = 1000
+    d = channel.draw_device(11, 12.0, B, 32, 16)
+    det = detector.Detector(B, 32, anneals=8)
+    det.set_noise(12.0)
+    bits, levels, dist = [x.clone() for x in det.run(d['H'], d['y'], seed=5)]
+    Hh, yh = d['H'].cpu().pin_memory(), d['y'].cpu().pin_memory()
+    bo = torch.empty(bits.shape, dtype=torch.int8).pin_memory()
+    do = torch.empty(B, dtype=torch.float32).pin_memory()
+    det.run_host(Hh, yh, 5, bo, do, torch.empty_like(d['H']), torch.empty_like(d['y']), chunks=7)
+    torch.cuda.synchronize()
+    det.check()
+    assert torch.equal(bo, bits.cpu())
+    assert torch.equal(do, dist.cpu())

@@ -24,6 +24,9 @@ SIGNATURES = {
     'arp_anneal_chord': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _U, _U, _U, _I, _I, _P, _P, _P, _P, _P],
     'arp_map_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P],
     'arp_readout_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P],
+    'arp_detect_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U, _I, _P,
+                      ctypes.c_size_t, _P, _P, _P, _P, _P, _P],
+    'arp_detect_dd_workspace': [_I, _I, _I, _I, _I, _P],
 }
 
 _lib = None
@@ -46,7 +49,8 @@ def lib():
         for name, argt in SIGNATURES.items():
             f = getattr(L, name)
             f.argtypes = argt
-            f.restype = ctypes.c_char_p if name in ('arp_version', 'arp_status_string') else ctypes.c_int
+            f.restype = (ctypes.c_char_p if name in ('arp_version', 'arp_status_string') else
+                         ctypes.c_size_t if name.endswith('_workspace') else ctypes.c_int)
         _lib = L
     return _lib
 

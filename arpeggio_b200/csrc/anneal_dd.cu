@@ -27,26 +27,10 @@
 #include <type_traits>
 
 #include "arp_common.cuh"
+#include "arp_internal.h"
 
 namespace arp {
 
-struct DDParams {
-  const void* Gt;  // (B, D, D) int32 or float, Gt[b][j][i] = G[b][i][j]
-  const void* h;   // (B, D)
-  const void* T;   // (L)
-  const void* c;   // (L) Onsager terms or null
-  int L;
-  int32_t qi;
-  float qf;
-  int R, D, B;
-  const uint32_t* inst;
-  uint32_t k0, k1;
-  int start;
-  int8_t* out_s;
-  void* out_de;
-  int64_t* out_st;
-  int32_t* status;
-};
 
 constexpr int32_t kMaxG = 1 << 18, kMaxH = 1 << 28, kMaxT = 1 << 26;
 
@@ -90,7 +74,7 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
     if (threadIdx.x == 0) set_status(a.status, ARP_ERR_RANGE);
     return;
   }
-  const uint32_t inst = a.inst[b];
+  const uint32_t inst = a.inst ? a.inst[b] : a.inst0 + (uint32_t)b;
   FT dg[NS], hv[NS];
   uint32_t vmask[NS];
 #pragma unroll
@@ -384,7 +368,7 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
     if (threadIdx.x == 0) set_status(a.status, ARP_ERR_RANGE);
     return;
   }
-  const uint32_t inst = a.inst[b];
+  const uint32_t inst = a.inst ? a.inst[b] : a.inst0 + (uint32_t)b;
   int32_t dg2[NS];
 #pragma unroll
   for (int t = 0; t < NS; ++t) {
@@ -599,7 +583,12 @@ static int check_dd(const void* Gt, const void* h, const void* T, int L, int P, 
   return ARP_OK;
 }
 
-static int default_warps(int R) { return R < 8 ? R : 8; }
+int default_warps(int R) { return R < 8 ? R : 8; }
+
+cudaError_t anneal_dispatch(int policy, bool flt, const DDParams& a, int P, int warps, cudaStream_t st) {
+  if (flt) return policy == 0 ? launch_dd<false, true>(a, P, warps, st) : launch_dd<true, true>(a, P, warps, st);
+  return policy == 0 ? launch_dd<false, false>(a, P, warps, st) : launch_dd<true, false>(a, P, warps, st);
+}
 
 }  // namespace arp
 
@@ -611,7 +600,7 @@ extern "C" int arp_anneal_first_accept(const int32_t* Gt, const int32_t* h, cons
                                        int32_t* status, void* stream) {
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
-  DDParams a{Gt, h, T, nullptr, L, q, 0.0f, R, D, B, inst, k0, k1, start, out_s, out_de, out_st, status};
+  DDParams a{Gt, h, T, nullptr, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
   return launch_dd<false, false>(a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
                                                                                               : ARP_ERR_LAUNCH;
 }
@@ -622,7 +611,7 @@ extern "C" int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const in
                                    void* stream) {
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
-  DDParams a{Gt, h, T, c, L, q, 0.0f, R, D, B, inst, k0, k1, start, out_s, out_de, out_st, status};
+  DDParams a{Gt, h, T, c, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
   return launch_dd<true, false>(a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
                                                                                              : ARP_ERR_LAUNCH;
 }
@@ -634,7 +623,7 @@ extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, co
   if (policy != 0 && policy != 1) return ARP_ERR_ARG;
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
-  DDParams a{Gt, h, T, c, L, 0, q, R, D, B, inst, k0, k1, start, out_s, out_de, out_st, status};
+  DDParams a{Gt, h, T, c, L, 0, q, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
   cudaError_t e = policy == 0 ? launch_dd<false, true>(a, P, default_warps(R), (cudaStream_t)stream)
                               : launch_dd<true, true>(a, P, default_warps(R), (cudaStream_t)stream);
   return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;

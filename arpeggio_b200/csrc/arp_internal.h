@@ -1,0 +1,58 @@
+// Internal declarations shared by the kernel files (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace arp {
+
+struct DDParams {
+  const void* Gt;  // (B, D, D) int32 or float, Gt[b][j][i] = G[b][i][j]
+  const void* h;   // (B, D)
+  const void* T;   // (L)
+  const void* c;   // (L) Onsager terms or null
+  int L;
+  int32_t qi;
+  float qf;
+  int R, D, B;
+  const uint32_t* inst;  // (B) instance numbers, or null: inst0 + b
+  uint32_t inst0;
+  uint32_t k0, k1;
+  int start;
+  int8_t* out_s;
+  void* out_de;
+  int64_t* out_st;
+  int32_t* status;
+};
+
+struct MapParams {
+  const float* H;       // (B, NR2, D)
+  const float* y;       // (B, NR2)
+  const float* sigma2;  // (B) regulariser (N0/2)/E[l^2]
+  int B, NR2, D, M;     // M: 4 (QPSK) or 16 (16-QAM)
+  float qscale;         // 4096 for the integer problem, 0 for the float problem
+  void* G;              // (B, D, D) int32 or float
+  void* h;              // (B, D) int32 or float
+  int8_t* xq;           // (B, D)
+  float* scale;         // (B)
+  int32_t* status;
+};
+
+struct ReadParams {
+  const float* H;       // (B, NR2, D)
+  const float* y;       // (B, NR2)
+  const int8_t* xq;     // (B, D)
+  const int8_t* spins;  // (B, R, P*D)
+  int B, NR2, D, P, R, M;
+  int8_t* levels;       // (B, D)
+  int8_t* bits;         // (B, D * nb)
+  float* dist;          // (B)
+  int32_t* pick;        // (B) winning candidate (R = the guess), may be null
+};
+
+// policy: 0 first accept, 1 Chord round; flt: FP32 fields.  Shapes already validated.
+cudaError_t anneal_dispatch(int policy, bool flt, const DDParams& a, int P, int warps, cudaStream_t st);
+cudaError_t map_dispatch(const MapParams& a, cudaStream_t st);
+cudaError_t readout_dispatch(const ReadParams& a, cudaStream_t st);
+int default_warps(int R);
+
+}  // namespace arp

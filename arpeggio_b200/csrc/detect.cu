@@ -15,6 +15,7 @@
 #include <cfloat>
 
 #include "arp_common.cuh"
+#include "arp_internal.h"
 
 namespace arp {
 
@@ -23,18 +24,6 @@ constexpr int kMapThreads = 256;
 template <int TB>
 __host__ __device__ constexpr int kChunkRows() { return TB <= 4 ? 64 : 32; }
 
-struct MapParams {
-  const float* H;       // (B, NR2, D)
-  const float* y;       // (B, NR2)
-  const float* sigma2;  // (B) regulariser (N0/2)/E[l^2]
-  int B, NR2, D, M;     // M: 4 (QPSK) or 16 (16-QAM)
-  float qscale;         // 4096 for the integer problem, 0 for the float problem
-  void* G;              // (B, D, D) int32 or float
-  void* h;              // (B, D) int32 or float
-  int8_t* xq;           // (B, D)
-  float* scale;         // (B)
-  int32_t* status;
-};
 
 __device__ __forceinline__ float nearest_level(float v, int M) {
   if (M == 4) return fabsf(v - 1.0f) < fabsf(v + 1.0f) ? 1.0f : -1.0f;  // ties -> the first level, -1
@@ -249,17 +238,6 @@ static cudaError_t launch_map(const MapParams& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-struct ReadParams {
-  const float* H;       // (B, NR2, D)
-  const float* y;       // (B, NR2)
-  const int8_t* xq;     // (B, D)
-  const int8_t* spins;  // (B, R, P*D)
-  int B, NR2, D, P, R, M;
-  int8_t* levels;       // (B, D)
-  int8_t* bits;         // (B, D * nb)
-  float* dist;          // (B)
-  int32_t* pick;        // (B) winning candidate (R = the guess), may be null
-};
 
 constexpr int kReadThreads = 256;
 
@@ -376,9 +354,78 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   }
 }
 
+cudaError_t map_dispatch(const MapParams& a, cudaStream_t st) {
+  const int D = a.D;
+  return D <= 16 ? launch_map<1>(a, st) : D <= 32 ? launch_map<2>(a, st) : D <= 64 ? launch_map<4>(a, st)
+                                                                          : launch_map<8>(a, st);
+}
+
+static size_t readout_smem(int D, int NR2) {
+  return sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + ((D + 15) & ~15);
+}
+
+cudaError_t readout_dispatch(const ReadParams& a, cudaStream_t st) {
+  const size_t smem = readout_smem(a.D, a.NR2);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_readout_dd<<<a.B, kReadThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Workspace of the fused detector call: G, h, x_q, scale, spins, de, (flips, tests), 256-byte aligned.
+static size_t det_layout(int B, int D, int P, int R, int flt, size_t* off) {
+  const size_t sz[7] = {(size_t)B * D * D * 4, (size_t)B * D * 4, (size_t)B * D, (size_t)B * 4,
+                        (size_t)B * R * P * D, (size_t)B * R * (flt ? 4 : 8), (size_t)B * R * 16};
+  size_t o = 0;
+  for (int i = 0; i < 7; ++i) {
+    if (off) off[i] = o;
+    o = (o + sz[i] + 255) & ~(size_t)255;
+  }
+  return o;
+}
+
 }  // namespace arp
 
 using namespace arp;
+
+extern "C" size_t arp_detect_dd_workspace(int B, int D, int P, int R, int precision, size_t* offsets) {
+  if (B < 0 || D < 1 || P < 1 || R < 1) return 0;
+  return det_layout(B, D, P, R, precision == 1, offsets);
+}
+
+extern "C" int arp_detect_dd(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M,
+                             int policy, int precision, int P, int R, const void* T, const void* c, int L, double q,
+                             uint32_t inst0, uint32_t k0, uint32_t k1, int start, void* workspace,
+                             size_t workspace_bytes, int8_t* bits, int8_t* levels, float* dist, int32_t* pick,
+                             int32_t* status, void* stream) {
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || !(P == 2 || P == 4 || P == 6) || R < 1 || L < 1 ||
+      !(M == 4 || M == 16))
+    return ARP_ERR_SHAPE;
+  if ((policy != 0 && policy != 1) || (precision != 0 && precision != 1) || (start != 0 && start != 1))
+    return ARP_ERR_ARG;
+  if (B == 0) return ARP_OK;
+  if (!H || !y || !sigma2 || !T || !workspace || !bits || !levels || !dist) return ARP_ERR_ARG;
+  const bool flt = precision == 1;
+  size_t off[7];
+  if (workspace_bytes < det_layout(B, D, P, R, flt, off)) return ARP_ERR_WORKSPACE;
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  void* G = w + off[0];
+  void* h = w + off[1];
+  int8_t* xq = reinterpret_cast<int8_t*>(w + off[2]);
+  float* scale = reinterpret_cast<float*>(w + off[3]);
+  int8_t* spins = reinterpret_cast<int8_t*>(w + off[4]);
+  cudaStream_t st = (cudaStream_t)stream;
+  MapParams m{H, y, sigma2, B, NR2, D, M, flt ? 0.0f : 4096.0f, G, h, xq, scale, status};
+  if (map_dispatch(m, st) != cudaSuccess) return ARP_ERR_LAUNCH;
+  DDParams a{G, h, T, c, L, flt ? 0 : (int32_t)q, (float)q, R, D, B, nullptr, inst0, k0, k1, start, spins,
+             w + off[5], reinterpret_cast<int64_t*>(w + off[6]), status};
+  if (anneal_dispatch(policy, flt, a, P, default_warps(R), st) != cudaSuccess) return ARP_ERR_LAUNCH;
+  ReadParams rp{H, y, xq, spins, B, NR2, D, P, R, M, levels, bits, dist, pick};
+  if (readout_dispatch(rp, st) != cudaSuccess) return ARP_ERR_LAUNCH;
+  return ARP_OK;
+}
 
 extern "C" int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M,
                           int quantize, void* G, void* h, int8_t* xq, float* scale, int32_t* status, void* stream) {
@@ -386,10 +433,7 @@ extern "C" int arp_map_dd(const float* H, const float* y, const float* sigma2, i
   if (B == 0) return ARP_OK;
   if (!H || !y || !sigma2 || !G || !h || !xq || !scale) return ARP_ERR_ARG;
   MapParams a{H, y, sigma2, B, NR2, D, M, quantize ? 4096.0f : 0.0f, G, h, xq, scale, status};
-  cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = D <= 16 ? launch_map<1>(a, st) : D <= 32 ? launch_map<2>(a, st) : D <= 64 ? launch_map<4>(a, st)
-                                                                                   : launch_map<8>(a, st);
-  return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+  return map_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2,
@@ -399,12 +443,7 @@ extern "C" int arp_readout_dd(const float* H, const float* y, const int8_t* xq, 
     return ARP_ERR_SHAPE;
   if (B == 0) return ARP_OK;
   if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist) return ARP_ERR_ARG;
-  const size_t smem = sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + ((D + 15) & ~15);
-  if (smem > 227 * 1024) return ARP_ERR_SHAPE;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return ARP_ERR_LAUNCH;
+  if (readout_smem(D, NR2) > 227 * 1024) return ARP_ERR_SHAPE;
   ReadParams a{H, y, xq, spins, B, NR2, D, P, R, M, levels, bits, dist, pick};
-  k_readout_dd<<<B, kReadThreads, smem, (cudaStream_t)stream>>>(a);
-  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+  return readout_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

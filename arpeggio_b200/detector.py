@@ -95,15 +95,24 @@ class Detector:
         self.c = None if c is None else torch.tensor(c, dtype=tdt, device=dev)
         self.q = qq
         D, R, P, NR2 = self.D, self.R, self.P, self.NR2
-        self.G = torch.empty(B, D, D, dtype=tdt, device=dev)
-        self.h = torch.empty(B, D, dtype=tdt, device=dev)
-        self.xq = torch.empty(B, D, dtype=torch.int8, device=dev)
-        self.scale = torch.empty(B, dtype=torch.float32, device=dev)
+        # one workspace in the layout of arp_detect_dd; the intermediates are views into it
+        import ctypes
+        offs = (ctypes.c_size_t * 7)()
+        nbytes = _lib.lib().arp_detect_dd_workspace(B, D, P, R, 1 if f32 else 0, offs)
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+
+        def view(i, dtype, shape):
+            n = int(np.prod(shape)) * torch.tensor([], dtype=dtype).element_size()
+            return self.workspace[offs[i]:offs[i] + n].view(dtype).view(*shape)
+        self.G = view(0, tdt, (B, D, D))
+        self.h = view(1, tdt, (B, D))
+        self.xq = view(2, torch.int8, (B, D))
+        self.scale = view(3, torch.float32, (B,))
+        self.spins = view(4, torch.int8, (B, R, P * D))
+        self.de = view(5, torch.float32 if f32 else torch.int64, (B, R))
+        self.st = view(6, torch.int64, (B, R, 2))
         self.sigma2 = torch.empty(B, dtype=torch.float32, device=dev)
         self.inst = torch.empty(B, dtype=torch.int32, device=dev)
-        self.spins = torch.empty(B, R, P * D, dtype=torch.int8, device=dev)
-        self.de = torch.empty(B, R, dtype=torch.float32 if f32 else torch.int64, device=dev)
-        self.st = torch.empty(B, R, 2, dtype=torch.int64, device=dev)
         self.levels = torch.empty(B, D, dtype=torch.int8, device=dev)
         self.bits = torch.empty(B, D * PAM[M]['bits'], dtype=torch.int8, device=dev)
         self.dist = torch.empty(B, dtype=torch.float32, device=dev)
@@ -124,12 +133,15 @@ class Detector:
     def run(self, H, y, seed, n=None, inst0=0, stream=None, events=None, off=0):
         """Stream-ordered detection of n uses; H (n, NR2, D) and y (n, NR2) float32 on the device, written to
         slots off .. off+n-1 of the detector's buffers with instance numbers inst0 + off + i.  Returns views of
-        the device outputs (bits, levels, dist); nothing is synchronised.  events: optional four CUDA events
-        recorded before map, anneal, readout and after readout (per-stage timing)."""
-        ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
+        the device outputs (bits, levels, dist); nothing is synchronised.  The whole batch goes through the
+        single C entry arp_detect_dd; pieces (off, n) and per-stage timing (events: four CUDA events recorded
+        before map, anneal, readout and after readout) go through the three stage entries, same kernels."""
         n = self.B - off if n is None else n
         if off < 0 or n < 0 or off + n > self.B:
             raise ValueError('slots %d..%d outside the detector batch %d' % (off, off + n, self.B))
+        if off == 0 and n == self.B and events is None:
+            return self._run_fused(H, y, seed, inst0, stream)
+        ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
         key = (inst0, off, n)
         if self._inst_base != key:
             iv = (np.arange(inst0 + off, inst0 + off + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
@@ -167,6 +179,19 @@ class Detector:
                                     _lib.ptr(pick), sp), 'readout')
         ev(3)
         return bits, levels, dist
+
+    def _run_fused(self, H, y, seed, inst0, stream):
+        L = _lib.lib()
+        f32 = self.precision == 'f32'
+        rc = L.arp_detect_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.sigma2), self.B, self.NR2, self.D, self.M,
+                             0 if self.policy == 'arpeggio' else 1, 1 if f32 else 0, self.P, self.R,
+                             _lib.ptr(self.T), _lib.ptr(self.c), int(self.T.shape[0]), float(self.q),
+                             inst0 & M32, seed & M32, (seed >> 32) & M32, 0 if self.start == 'rand' else 1,
+                             _lib.ptr(self.workspace), self.workspace.numel(), _lib.ptr(self.bits),
+                             _lib.ptr(self.levels), _lib.ptr(self.dist), _lib.ptr(self.pick), _lib.ptr(self.status),
+                             _lib.stream_ptr(stream))
+        _lib.check(rc, 'detect')
+        return self.bits, self.levels, self.dist
 
     def run_host(self, Hh, yh, seed, bits_out, dist_out, Hd, yd, chunks=8, inst0=0, stream=None):
         """End-to-end detection from pinned host buffers: the batch is cut into `chunks` pieces; the host to

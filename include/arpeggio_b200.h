@@ -13,6 +13,7 @@
 #ifndef ARPEGGIO_B200_H
 #define ARPEGGIO_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -102,6 +103,22 @@ int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int N
  * mimo.select and mimo.levels_to_bits (arpeggio/mimo/mimo.py:185-190, 416-425, 45-51). */
 int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D,
                    int P, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick, void* stream);
+
+/* The detector call in one entry point: map (arp_map_dd) -> anneal (policy 0 = first accept, 1 = Chord round;
+ * precision 0 = int32 fixed point with T, c int32 and q rounded to an integer, 1 = FP32 fields with T, c, q
+ * float) -> readout (arp_readout_dd), stream-ordered, with the intermediates in the caller's workspace of at
+ * least arp_detect_dd_workspace() bytes.  Instance numbers inst0 + b, Philox key (k0, k1), start 0 = 'rand',
+ * 1 = 'bal', P = 2K copies, R anneals.  Outputs as arp_readout_dd.  This is the one-stage dDI detection of
+ * arpeggio/mimo/fxdetect.py:24-43 (candidates of every anneal plus the MMSE guess, lowest ||y - Hx||^2) with
+ * the sub-problem solve of arpeggio/sim/local_code_a513/run_a513.py:107-128. */
+int arp_detect_dd(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M, int policy,
+                  int precision, int P, int R, const void* T, const void* c, int L, double q, uint32_t inst0,
+                  uint32_t k0, uint32_t k1, int start, void* workspace, size_t workspace_bytes, int8_t* bits,
+                  int8_t* levels, float* dist, int32_t* pick, int32_t* status, void* stream);
+
+/* Workspace bytes arp_detect_dd needs; if offsets is not NULL it receives the 7 byte offsets of G, h, x_q,
+ * scale, spins, best energy changes and (flips, tests) inside it (for inspection after a call). */
+size_t arp_detect_dd_workspace(int B, int D, int P, int R, int precision, size_t* offsets);
 
 #ifdef __cplusplus
 }

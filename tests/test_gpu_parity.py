@@ -308,3 +308,20 @@ def test_pipelined_host_path_equals_one_run():
     det.check()
     assert torch.equal(bo, bits.cpu())
     assert torch.equal(do, dist.cpu())
+
+
+def test_fused_c_entry_equals_staged_calls():
+    """arp_detect_dd (one C call, caller workspace) == the three stage entries with per-stage events."""
+    from arpeggio_b200 import channel, detector
+    for policy, precision in (('arpeggio', 'int'), ('chord', 'int'), ('arpeggio', 'f32')):
+        B = 700
+        d = channel.draw_device(21, 10.0, B, 16, 16)
+        det = detector.Detector(B, 16, anneals=6, policy=policy, precision=precision)
+        det.set_noise(10.0)
+        fused = [x.clone() for x in det.run(d['H'], d['y'], seed=9)] + [det.spins.clone()]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        staged = [x.clone() for x in det.run(d['H'], d['y'], seed=9, events=ev)] + [det.spins.clone()]
+        torch.cuda.synchronize()
+        det.check()
+        for a_, b_ in zip(fused, staged):
+            assert torch.equal(a_, b_), (policy, precision)

@@ -120,3 +120,21 @@ def test_oracle_f32_rule_is_deterministic():
     b = O.anneal_dd_f32(G, hh, P, R, T, 0.1, np.arange(B), 77, 'rand', nthreads=4)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+def test_detect_entry_checks_workspace_before_launch():
+    """A workspace smaller than arp_detect_dd_workspace() is refused on the host (ARP_ERR_WORKSPACE)."""
+    import ctypes
+    from arpeggio_b200 import _lib
+    L = _lib.lib()
+    offs = (ctypes.c_size_t * 7)()
+    need = L.arp_detect_dd_workspace(100, 64, 2, 32, 0, offs)
+    assert need >= 100 * 64 * 64 * 4 + 100 * 32 * 128 and all(o % 256 == 0 for o in offs)
+    assert list(offs) == sorted(offs)
+    fake = ctypes.c_void_p(256)  # never dereferenced: the size check comes first
+    rc = L.arp_detect_dd(fake, fake, fake, 100, 64, 64, 16, 0, 0, 2, 32, fake, None, 64, 0.0, 0, 1, 2, 0, fake,
+                         need - 1, fake, fake, fake, None, None, None)
+    assert rc == 6
+    rc = L.arp_detect_dd(fake, fake, fake, 100, 64, 64, 16, 2, 0, 2, 32, fake, None, 64, 0.0, 0, 1, 2, 0, fake,
+                         need, fake, fake, fake, None, None, None)
+    assert rc == 3  # bad policy

@@ -120,6 +120,21 @@ int arp_detect_dd(const float* H, const float* y, const float* sigma2, int B, in
  * scale, spins, best energy changes and (flips, tests) inside it (for inspection after a call). */
 size_t arp_detect_dd_workspace(int B, int D, int P, int R, int precision, size_t* offsets);
 
+/* arp_detect_dd without a workspace argument, for callers that cannot allocate device memory: a receive
+ * chain with a hard per-frame latency budget cannot call cudaMalloc on the frame path (it synchronises the
+ * device and takes unbounded time), and a plugin inside a host program that owns all device memory may not
+ * allocate at all.  Same arguments and outputs as arp_detect_dd minus (workspace, workspace_bytes); the
+ * intermediates live in one 32 MiB array compiled into the library, which every GPU that loads the library
+ * holds until the process exits.  A batch whose arp_detect_dd_workspace() exceeds 32 MiB is refused with
+ * ARP_ERR_WORKSPACE before any launch.  All calls on a device share the array (it keeps the last call's
+ * contents, and nothing in it needs to start at zero); calls whose work overlaps on the GPU race on it.  The
+ * first call on each device looks up the array's address and should come before any stream capture.
+ * No counterpart in the reference: it exists only for callers that cannot allocate. */
+int arp_detect_dd_static(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M,
+                         int policy, int precision, int P, int R, const void* T, const void* c, int L, double q,
+                         uint32_t inst0, uint32_t k0, uint32_t k1, int start, int8_t* bits, int8_t* levels,
+                         float* dist, int32_t* pick, int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

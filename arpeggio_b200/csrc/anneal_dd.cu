@@ -324,16 +324,22 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
   }
 }
 
-// Integer fields, margin form.  For the pass's copy p each lane keeps its margin mu = theta - s w (accept iff
-// mu > 0, one compare) instead of w; a flip of lane j (old spin so) moves every margin by -4 so s_i G_ij with s_i
-// the lane's spin at the start of the pass, and the flipped lane's own term so w_j = theta_j - mu_j gives the
-// energy change 4 so w_j + 8 G_jj = 4 (kappa_j - mu_j), kappa = theta + 2 G_jj.  At the end of the pass the
-// fields come back exactly as w = s (theta - mu).  Spins are per-thread bits (bit p*NS + t = coordinate
-// t*32 + lane of copy p is +1).  First accept: a ballot over the remaining lanes (index > last commit) finds
-// the first accepted lane; the number of ballots a pass takes is the reference's `tests` for that pass
-// (one, plus one after every flip that is not on the last lane).
+// Integer fields, margin form.  For the pass's copy p each lane keeps psi = s w + 2 G_jj, with s the lane's
+// spin at the start of the pass, packed as psi2 = 2 psi + (s == +1).  Lane j accepts iff
+// s w < theta = ceil(u 4T / 2^32) - 2 G_jj - q - 2T (the reference's decision as a 32-bit compare), i.e. iff
+// psi < kappa = theta + 2 G_jj, i.e. iff psi2 < 2 kappa.  A flip of lane j (old spin so) adds 4 so G_ij to w_i,
+// so psi2_i moves by 8 so s_i G_ij (one IMAD; bit 0 stays), and the energy moves by 4 so w_j + 8 G_jj = 4 psi_j:
+// one shuffle of the owner's psi2 gives both the energy change and so.  Fields come back at the end of the pass
+// as w = s (psi - 2 G_jj).  Spins are per-thread bits (bit p*NS + t = coordinate t*32 + lane of copy p is +1).
+// First accept: a ballot over the lanes after the last commit finds the first acceptance; the pass ends on an
+// empty ballot.  The reference's counters follow from the ballots: a pass with f flips takes 1 + f ballots here
+// and reports tests = 1 + f - [its last flip was on lane D-1], flips = f.
+#ifndef ARP_ANNEAL_MINB
+#define ARP_ANNEAL_MINB 1
+#endif
+
 template <int NS, int P, bool CHORD, bool CACHE>
-__global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
+__global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
   constexpr int DP = NS * 32;
   extern __shared__ __align__(16) unsigned char smem[];
   int32_t* Gs = reinterpret_cast<int32_t*>(smem);
@@ -369,6 +375,7 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
     return;
   }
   const uint32_t inst = a.inst ? a.inst[b] : a.inst0 + (uint32_t)b;
+  const PhiloxKeys& K = *reinterpret_cast<const PhiloxKeys*>(a.rk0);
   int32_t dg2[NS];
 #pragma unroll
   for (int t = 0; t < NS; ++t) {
@@ -385,14 +392,14 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
 #pragma unroll
         for (int t = 0; t < NS; ++t) {
           uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
-          philox10(c0, c1, c2, c3, a.k0, a.k1);
+          philox10(c0, c1, c2, c3, K);
           if (c0 >= 0x80000000u) sp |= 1u << (p * NS + t);
         }
     } else {
 #pragma unroll
       for (int t = 0; t < NS; ++t) {
         uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)(t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
-        philox10(c0, c1, c2, c3, a.k0, a.k1);
+        philox10(c0, c1, c2, c3, K);
         const int pat = bal_pattern(P, (uint32_t)(((uint64_t)c0 * (uint64_t)bal_choose(P)) >> 32));
 #pragma unroll
         for (int p = 0; p < P; ++p)
@@ -412,8 +419,7 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
     }
 #pragma unroll
     for (int tj = 0; tj < NS; ++tj) {
-      const uint32_t nz = __ballot_sync(ARP_FULL, mloc[tj] != 0);
-      uint32_t mm = nz;
+      uint32_t mm = __ballot_sync(ARP_FULL, mloc[tj] != 0);
       while (mm) {
         const int l = __ffs(mm) - 1;
         mm &= mm - 1u;
@@ -425,7 +431,7 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
     }
     long long de = 0, best = 1LL << 62;
     uint32_t bsp = sp;
-    int32_t flips = 0, tests = 0;
+    int32_t ballots = 0, lastflips = 0, passes = 0;
     const int nquad = (L + 4 * P - 1) / (4 * P);
     for (int q4 = 0; q4 < nquad; ++q4) {
       uint32_t cw[CACHE ? P : 1][CACHE ? NS : 1][4];
@@ -435,7 +441,7 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
 #pragma unroll
           for (int t = 0; t < NS; ++t) {
             uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
-            philox10(c0, c1, c2, c3, a.k0, a.k1);
+            philox10(c0, c1, c2, c3, K);
             cw[p][t][0] = c0;
             cw[p][t][1] = c1;
             cw[p][t][2] = c2;
@@ -448,10 +454,11 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
         for (int p = 0; p < P; ++p) {
           const int k = (q4 * 4 + i) * P + p;
           if (k >= L) break;
+          ++passes;
           const int32_t Tk = Tg[k];
           const long long A = 4LL * Tk;
           const int32_t Bk = a.qi + 2 * Tk - ((CHORD && cg) ? cg[k] : 0);
-          int32_t mu[NS], kap[NS], cpos[NS];
+          int32_t psi2[NS], kap2[NS], cp[NS];
 #pragma unroll
           for (int t = 0; t < NS; ++t) {
             uint32_t u;
@@ -459,71 +466,69 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
               u = cw[p][t][i];
             } else {
               uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
-              philox10(c0, c1, c2, c3, a.k0, a.k1);
+              philox10(c0, c1, c2, c3, K);
               u = i == 0 ? c0 : (i == 1 ? c1 : (i == 2 ? c2 : c3));
             }
             const bool valid = t * 32 + lane < D;
-            const int32_t th = valid ? (int32_t)ceil_shift32(u, A) - dg2[t] - Bk : -(1 << 30);
             const bool up = (sp >> (p * NS + t)) & 1u;
-            mu[t] = th - (up ? w[t] : -w[t]);
-            kap[t] = th + dg2[t];
-            cpos[t] = up ? -4 : 4;
+            const int32_t psi = (up ? w[t] : -w[t]) + dg2[t];
+            psi2[t] = 2 * psi + (up ? 1 : 0);
+            kap2[t] = valid ? 2 * ((int32_t)ceil_shift32(u, A) - Bk) : -(1 << 30);
+            cp[t] = up ? 8 : -8;
           }
+          int jl = -1;
           // commit the flip of lane l of slot ts: energy, margins, spin bit
           auto commit = [&](int ts, int l, int32_t vsel) {
-            const int32_t v = __shfl_sync(ARP_FULL, vsel, l);
-            const uint32_t spo = __shfl_sync(ARP_FULL, sp, l);
-            const bool so_up = (spo >> (p * NS + ts)) & 1u;
-            de += 4LL * v;
+            const int32_t packed = __shfl_sync(ARP_FULL, vsel, l);
+            de += 4LL * (packed >> 1);
+            const bool so_up = packed & 1;
             const int32_t* gr = Gs + (ts * 32 + l) * DP + lane;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) mu[t] += (so_up ? cpos[t] : -cpos[t]) * gr[t * 32];
+            for (int t = 0; t < NS; ++t) psi2[t] += (so_up ? cp[t] : -cp[t]) * gr[t * 32];
             if (lane == l) sp ^= 1u << (p * NS + ts);
-            ++flips;
+            jl = ts * 32 + l;
           };
           if constexpr (!CHORD) {
-            int jl = -1;
             for (;;) {
               uint32_t am[NS];
 #pragma unroll
-              for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, mu[t] > 0 && t * 32 + lane > jl);
-              ++tests;
-              int ts = NS;
-              uint32_t m = 0;
-              int32_t vsel = 0;
+              for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, psi2[t] < kap2[t] && t * 32 + lane > jl);
+              ++ballots;
+              int ts = NS - 1;
+              uint32_t m = am[NS - 1];
+              int32_t vsel = psi2[NS - 1];
 #pragma unroll
-              for (int t = NS - 1; t >= 0; --t)
+              for (int t = NS - 2; t >= 0; --t)
                 if (am[t]) {
                   ts = t;
                   m = am[t];
-                  vsel = kap[t] - mu[t];
+                  vsel = psi2[t];
                 }
-              if (ts == NS) break;
-              const int l = __ffs(m) - 1;
-              commit(ts, l, vsel);
-              jl = ts * 32 + l;
-              if (jl == D - 1) break;
+              if (m == 0) break;
+              commit(ts, __ffs(m) - 1, vsel);
             }
           } else {
             uint32_t am[NS];
 #pragma unroll
-            for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, mu[t] > 0);
-            ++tests;
+            for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, psi2[t] < kap2[t]);
+            ++ballots;
 #pragma unroll
             for (int t = 0; t < NS; ++t) {
               uint32_t m = am[t];
               while (m) {
                 const int l = __ffs(m) - 1;
                 m &= m - 1u;
-                commit(t, l, kap[t] - mu[t]);
+                commit(t, l, psi2[t]);
+                ++ballots;
               }
             }
           }
-          // fields back from the margins: s w = theta - mu with the pass-start spin
+          if (jl == D - 1) ++lastflips;
+          // fields back: w = s (psi - 2 G_jj) with the pass-start spin
 #pragma unroll
           for (int t = 0; t < NS; ++t) {
-            const int32_t swv = kap[t] - dg2[t] - mu[t];
-            w[t] = cpos[t] < 0 ? swv : -swv;
+            const int32_t v = (psi2[t] >> 1) - dg2[t];
+            w[t] = cp[t] > 0 ? v : -v;
           }
           if (de < best) {  // best state after each pass (arpeggio_fx.cu:90-93)
             best = de;
@@ -542,11 +547,32 @@ __global__ void __launch_bounds__(256) k_anneal_int(const DDParams a) {
         if (j < D) os[p * D + j] = ((bsp >> (p * NS + t)) & 1u) ? 1 : -1;
       }
     if (lane == 0) {
+      // first accept: ballots = passes + flips; Chord: ballots = passes + flips (one per commit + one per pass)
+      const int32_t flips = ballots - passes;
       reinterpret_cast<long long*>(a.out_de)[ar] = best;
       a.out_st[2 * ar] = flips;
-      a.out_st[2 * ar + 1] = tests;
+      a.out_st[2 * ar + 1] = CHORD ? passes : ballots - lastflips;
     }
   }
+}
+
+// Warps per block: a block holds one problem and its warps share the anneals, so fewer warps per block let
+// more blocks (problems) share an SM.  Pick the width with the most resident warps per SM for this kernel's
+// registers and shared memory (ties go to the wider block, which loads G fewer times per anneal).
+template <typename K>
+static int pick_warps(K kern, size_t smem, int R) {
+  int best_w = 1, best_res = -1;
+  for (int w = 1; w <= 8; w *= 2) {
+    if (w > R && w > 1) break;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * w, smem) != cudaSuccess) return R < 8 ? R : 8;
+    const int res = nb * w;
+    if (res >= best_res) {
+      best_res = res;
+      best_w = w;
+    }
+  }
+  return best_w;
 }
 
 template <int NS, int P, bool CHORD, bool FLT>
@@ -554,9 +580,21 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   constexpr bool CACHE = P * NS <= 8;
   auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE>;
   const size_t smem = (size_t)a.D * NS * 32 * 4;
-  if (smem > 48 * 1024) {
+  static size_t attr_smem = 48 * 1024;
+  if (smem > attr_smem) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    attr_smem = smem;
+  }
+  static size_t cached_smem = 0;
+  static int cached_w = 0;
+  if (warps <= 0) {
+    if (cached_w == 0 || cached_smem != smem) {
+      cached_w = pick_warps(kern, smem, 8);
+      cached_smem = smem;
+    }
+    warps = cached_w;
+    while (warps > 1 && warps > a.R) warps >>= 1;
   }
   kern<<<a.B, warps * 32, smem, st>>>(a);
   return cudaGetLastError();
@@ -583,9 +621,15 @@ static int check_dd(const void* Gt, const void* h, const void* T, int L, int P, 
   return ARP_OK;
 }
 
-int default_warps(int R) { return R < 8 ? R : 8; }
+int default_warps(int R) { return 0; }  // 0: chosen per kernel by occupancy (pick_warps)
 
-cudaError_t anneal_dispatch(int policy, bool flt, const DDParams& a, int P, int warps, cudaStream_t st) {
+cudaError_t anneal_dispatch(int policy, bool flt, const DDParams& a0, int P, int warps, cudaStream_t st) {
+  DDParams a = a0;
+  const PhiloxKeys K = philox_keys(a.k0, a.k1);
+  for (int i = 0; i < 10; ++i) {
+    a.rk0[i] = K.k0[i];
+    a.rk1[i] = K.k1[i];
+  }
   if (flt) return policy == 0 ? launch_dd<false, true>(a, P, warps, st) : launch_dd<true, true>(a, P, warps, st);
   return policy == 0 ? launch_dd<false, false>(a, P, warps, st) : launch_dd<true, false>(a, P, warps, st);
 }
@@ -601,8 +645,8 @@ extern "C" int arp_anneal_first_accept(const int32_t* Gt, const int32_t* h, cons
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
   DDParams a{Gt, h, T, nullptr, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
-  return launch_dd<false, false>(a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
-                                                                                              : ARP_ERR_LAUNCH;
+  return anneal_dispatch(0, false, a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
+                                                                                                : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L,
@@ -612,8 +656,8 @@ extern "C" int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const in
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
   DDParams a{Gt, h, T, c, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
-  return launch_dd<true, false>(a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
-                                                                                             : ARP_ERR_LAUNCH;
+  return anneal_dispatch(1, false, a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
+                                                                                                : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, const float* T, const float* c, int L,
@@ -624,7 +668,6 @@ extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, co
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
   DDParams a{Gt, h, T, c, L, 0, q, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
-  cudaError_t e = policy == 0 ? launch_dd<false, true>(a, P, default_warps(R), (cudaStream_t)stream)
-                              : launch_dd<true, true>(a, P, default_warps(R), (cudaStream_t)stream);
+  cudaError_t e = anneal_dispatch(policy, true, a, P, default_warps(R), (cudaStream_t)stream);
   return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

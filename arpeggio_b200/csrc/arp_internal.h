@@ -22,6 +22,7 @@ struct DDParams {
   void* out_de;
   int64_t* out_st;
   int32_t* status;
+  uint32_t rk0[10], rk1[10];  // Philox round keys of (k0, k1), filled by anneal_dispatch
 };
 
 struct MapParams {

@@ -15,12 +15,13 @@ __global__ void k_philox_kat(const uint32_t* __restrict__ in, uint32_t* __restri
   out[4 * t + 3] = c3;
 }
 
-// Calibration: `iters` chained Philox4x32-10 blocks per thread (the anneal's dominant integer work), for the
-// measured integer-issue peak the benchmark divides by.
-__global__ void k_philox_rate(uint32_t* out, int iters, uint32_t k0, uint32_t k1) {
+// Calibration: `iters` chained Philox4x32-10 blocks per thread (the anneal's dominant integer work, with the
+// round keys in the parameter block exactly as the anneal kernels take them), for the measured integer-issue
+// peak the benchmark divides by.
+__global__ void k_philox_rate(uint32_t* out, int iters, const PhiloxKeys K) {
   uint32_t c0 = blockIdx.x, c1 = threadIdx.x, c2 = 0, c3 = 0;
   for (int i = 0; i < iters; ++i) {
-    philox10(c0, c1, c2, c3, k0, k1);
+    philox10(c0, c1, c2, c3, K);
     c2 += (uint32_t)i;
   }
   if ((c0 ^ c1 ^ c2 ^ c3) == 0x9E3779B9u) out[0] = c0;  // keeps the work live; almost never stores
@@ -31,7 +32,7 @@ __global__ void k_philox_rate(uint32_t* out, int iters, uint32_t k0, uint32_t k1
 extern "C" int arp_philox_rate(uint32_t* out, int blocks, int threads, int iters, void* stream) {
   if (blocks < 1 || threads < 32 || threads > 1024 || iters < 1) return ARP_ERR_SHAPE;
   if (!out) return ARP_ERR_ARG;
-  arp::k_philox_rate<<<blocks, threads, 0, (cudaStream_t)stream>>>(out, iters, 0x12345678u, 0x9abcdef0u);
+  arp::k_philox_rate<<<blocks, threads, 0, (cudaStream_t)stream>>>(out, iters, arp::philox_keys(0x12345678u, 0x9abcdef0u));
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 

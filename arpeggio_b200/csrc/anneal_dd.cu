@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
   FT* Gs = reinterpret_cast<FT*>(smem);
   __shared__ int s_bad;
   const int D = a.D, L = a.L, R = a.R;
-  const int b = blockIdx.x;
+  const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
   const FT* Tg = reinterpret_cast<const FT*>(a.T);
   const FT* cg = reinterpret_cast<const FT*>(a.c);
 
-  for (int r = wid; r < R; r += W) {
+  for (int r = bs + split * wid; r < R; r += split * W) {
     uint32_t Sm[P][NS], Bm[P][NS];
     // ---- start state (arpeggio_fx.cu:48-57)
     if (a.start == 0) {
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
   int32_t* Gs = reinterpret_cast<int32_t*>(smem);
   __shared__ int s_bad;
   const int D = a.D, L = a.L, R = a.R;
-  const int b = blockIdx.x;
+  const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
     dg2[t] = j < D ? 2 * Gs[j * DP + j] : 0;
   }
 
-  for (int r = wid; r < R; r += W) {
+  for (int r = bs + split * wid; r < R; r += split * W) {
     // ---- start state (arpeggio_fx.cu:48-57), packed per thread
     uint32_t sp = 0;
     if (a.start == 0) {
@@ -588,15 +588,31 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   }
   static size_t cached_smem = 0;
   static int cached_w = 0;
+  static int cached_nb = 0, sms = 0;
   if (warps <= 0) {
     if (cached_w == 0 || cached_smem != smem) {
       cached_w = pick_warps(kern, smem, 8);
       cached_smem = smem;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_nb, kern, 32 * cached_w, smem) != cudaSuccess)
+        cached_nb = 1;
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
     warps = cached_w;
     while (warps > 1 && warps > a.R) warps >>= 1;
   }
-  kern<<<a.B, warps * 32, smem, st>>>(a);
+  // Small batches: split each problem's anneals over several blocks so the batch still fills the GPU.
+  DDParams b = a;
+  b.split = 1;
+  const long long slots = (long long)(cached_nb > 0 ? cached_nb : 1) * (sms > 0 ? sms : 148);
+  if ((long long)a.B < slots) {
+    const int most = (a.R + warps - 1) / warps;
+    long long sp = (slots + a.B - 1) / a.B;
+    b.split = (int)(sp < most ? sp : most);
+    if (b.split < 1) b.split = 1;
+  }
+  kern<<<(unsigned)((long long)a.B * b.split), warps * 32, smem, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -23,6 +23,7 @@ struct DDParams {
   int64_t* out_st;
   int32_t* status;
   uint32_t rk0[10], rk1[10];  // Philox round keys of (k0, k1), filled by anneal_dispatch
+  int split;                  // blocks per problem (anneals r = s, s + split, ... in block s), set at launch
 };
 
 struct MapParams {

@@ -228,6 +228,30 @@ class Detector:
                 bits_out[a:b].copy_(bits, non_blocking=True)
                 dist_out[a:b].copy_(dist, non_blocking=True)
 
+    def capture(self, Hh, yh, seed, bits_out, dist_out, Hd, yd):
+        """A CUDA graph of one whole-batch detection from pinned host buffers: copy H, y in, detect, copy bits
+        and distances out.  Replaying it re-runs the same seed on whatever the pinned inputs hold, with no host
+        work per frame beyond the launch of the graph (the serving path for small frames).  Warms the launch
+        configuration up first, outside the capture."""
+        import torch
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(2):
+                Hd.copy_(Hh, non_blocking=True)
+                yd.copy_(yh, non_blocking=True)
+                self.run(Hd, yd, seed)
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            Hd.copy_(Hh, non_blocking=True)
+            yd.copy_(yh, non_blocking=True)
+            bits, _, dist = self.run(Hd, yd, seed)
+            bits_out.copy_(bits, non_blocking=True)
+            dist_out.copy_(dist, non_blocking=True)
+        return g
+
     def check(self):
         _lib.check(int(self.status.item()), 'device check')
 

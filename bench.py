@@ -196,6 +196,35 @@ def run_ours(args):
     det.check()
     ms_e2e = e0.elapsed_time(e1) / Ke
 
+    # ---- per-frame latency: one 32-user channel use, host buffers in and out, replayed CUDA graph
+    lat = None
+    if args.latency_frames > 0:
+        f = channel.draw_device(77 + rank, float(w['snrs'][len(w['snrs']) // 2]), 1, w['nt'], w['M'], dev=dev)
+        det1 = detector.Detector(1, w['nt'], w['nr'], w['M'], w['policy'], args.anneals, w['K'], sweeps=w['sweeps'],
+                                 T0=w['T0'], T1=w['T1'], q=w['q'], start=w['start'], precision=w['precision'],
+                                 device=dev)
+        det1.set_noise(N0=f['N0'])
+        Hh1, yh1 = f['H'].cpu().pin_memory(), f['y'].cpu().pin_memory()
+        bo1 = torch.empty(det1.bits.shape, dtype=torch.int8).pin_memory()
+        do1 = torch.empty(1, dtype=torch.float32).pin_memory()
+        g = det1.capture(Hh1, yh1, 5, bo1, do1, torch.empty_like(f['H']), torch.empty_like(f['y']))
+        for _ in range(50):
+            g.replay()
+        torch.cuda.synchronize()
+        n = args.latency_frames
+        le = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for i in range(n):
+            le[i][0].record(stream)
+            g.replay()
+            le[i][1].record(stream)
+        torch.cuda.synchronize()
+        det1.check()
+        us = sorted(1e3 * a_.elapsed_time(b_) for a_, b_ in le)
+        lat = {'frame': 'one %d-user x %d-antenna 16-QAM channel use, %d anneals, H/y from pinned host memory, bits '
+                        'and distance back to pinned host memory, one replayed CUDA graph (copy in, map, anneal, '
+                        'readout, copy out); device time per replay' % (w['nt'], w['nr'], args.anneals),
+               'frames': n, 'p50_us': us[n // 2], 'p99_us': us[min(n - 1, int(0.99 * n))], 'max_us': us[-1]}
+
     # ---- integer-issue peak (calibration kernel) and the anneal kernel's algorithmic work
     L = _lib.lib()
     buf = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -255,6 +284,7 @@ def run_ours(args):
                          'frac': alg_bytes / t_anneal / 1e9 / hbm_peak,
                          'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if peaks else 'fallback'},
         'anneal_counters': {'flips': int(st[0]), 'tests': int(st[1]), 'anneals': B * R, 'philox_blocks': blocks},
+        'latency': lat,
         'gpu_launches': 3 * K,
         'clocks': ck,
     }
@@ -305,6 +335,7 @@ def main():
     ap.add_argument('--anneals', type=int, default=WORKLOAD['anneals'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--chunks', type=int, default=8, help='pipelined pieces of the end-to-end step')
+    ap.add_argument('--latency-frames', type=int, default=2000, help='single-frame replays for p50/p99 latency')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.rank = int(os.environ.get('RANK', 0))

@@ -325,3 +325,29 @@ def test_fused_c_entry_equals_staged_calls():
         det.check()
         for a_, b_ in zip(fused, staged):
             assert torch.equal(a_, b_), (policy, precision)
+
+
+def test_small_batch_split_and_graph_replay():
+    """A batch smaller than the GPU splits each problem's anneals over blocks; results equal the oracle's, and a
+    captured single-frame graph gives the same outputs as a direct run."""
+    from arpeggio_b200 import channel, detector
+    B, R = 3, 32
+    b = channel.draw(55, 12.0, 0, B, 32, 16)
+    det = detector.Detector(B, 32, anneals=R)
+    det.set_noise(12.0)
+    bits, levels, dist = [x.clone() for x in det.run(b['H'].cuda(), b['y'].cuda(), seed=77)]
+    torch.cuda.synchronize()
+    det.check()
+    T, q = det.schedule['T'], det.schedule['q']
+    ws, wde, wst = O.anneal_dd(det.G.cpu().numpy(), det.h.cpu().numpy(), 2, R, T, q, np.arange(B), 77, 'rand',
+                               nthreads=NTH)
+    assert np.array_equal(det.spins.cpu().numpy(), ws)
+    assert np.array_equal(det.de.cpu().numpy(), wde)
+    assert np.array_equal(det.st.cpu().numpy(), wst)
+    Hh, yh = b['H'].pin_memory(), b['y'].pin_memory()
+    bo = torch.empty(bits.shape, dtype=torch.int8).pin_memory()
+    do = torch.empty(B, dtype=torch.float32).pin_memory()
+    g = det.capture(Hh, yh, 77, bo, do, torch.empty_like(b['H'].cuda()), torch.empty_like(b['y'].cuda()))
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(bo, bits.cpu()) and torch.equal(do, dist.cpu())

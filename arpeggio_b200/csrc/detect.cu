@@ -252,8 +252,8 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   float* Hs = sm;                   // D x HS (transposed)
   float* r0 = Hs + D * HS;          // NR2
   float* bd = r0 + NR2;             // 8
-  int* br = reinterpret_cast<int*>(bd + 8);
-  int8_t* xq8 = reinterpret_cast<int8_t*>(br + 8);  // D
+  int* br = reinterpret_cast<int*>(bd + 8);  // 8
+  int8_t* ek = reinterpret_cast<int8_t*>(br + 8);  // (R + 1) x D: candidate level minus guess; row R = x_q
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, W = kReadThreads / 32;
   const int lo = a.M == 4 ? -1 : -3, hi = -lo;
   const float* Hb = a.H + (size_t)b * NR2 * D;
@@ -261,8 +261,18 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
     const int i = x / D, j = x - i * D;
     Hs[j * HS + i] = Hb[x];
   }
+  int8_t* xq8 = ek + R * D;
   for (int j = tid; j < D; j += kReadThreads) xq8[j] = a.xq[(size_t)b * D + j];
   __syncthreads();
+  // every candidate's clipped delta from the guess, from one coalesced pass over its spins
+  const int8_t* sb = a.spins + (size_t)b * R * P * D;
+  for (int x = tid; x < R * D; x += kReadThreads) {
+    const int c = x / D, j = x - c * D;
+    int d = 0;
+    for (int p = 0; p < P; ++p) d += sb[(size_t)c * P * D + p * D + j];
+    const int xv = min(max((int)xq8[j] + d, lo), hi);
+    ek[x] = (int8_t)(xv - xq8[j]);
+  }
   for (int i = tid; i < NR2; i += kReadThreads) {
     float r = a.y[(size_t)b * NR2 + i];
     for (int j = 0; j < D; ++j) r = __fmaf_rn(-Hs[j * HS + i], (float)xq8[j], r);
@@ -276,22 +286,12 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
     if (c == R) {
       for (int i = lane; i < NR2; i += 32) acc = __fmaf_rn(r0[i], r0[i], acc);
     } else {
-      const int8_t* s = a.spins + ((size_t)b * R + c) * P * D;
-      // e_j for the lanes' coordinates, then the warp walks the nonzero ones
-      int ej[4];
+      const int8_t* e = ek + c * D;
       uint32_t nzm[4];
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int j = t * 32 + lane;
-        int e = 0;
-        if (j < D) {
-          int d = 0;
-          for (int p = 0; p < P; ++p) d += s[p * D + j];
-          const int x = min(max((int)xq8[j] + d, lo), hi);
-          e = x - xq8[j];
-        }
-        ej[t] = e;
-        nzm[t] = __ballot_sync(ARP_FULL, e != 0);
+        nzm[t] = __ballot_sync(ARP_FULL, j < D && e[j] != 0);
       }
       float rr[8];
 #pragma unroll
@@ -303,10 +303,10 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
           const int l = __ffs(mm) - 1;
           mm &= mm - 1u;
           const int j = t * 32 + l;
-          const float e = (float)__shfl_sync(ARP_FULL, ej[t], l);
+          const float ev = (float)e[j];
 #pragma unroll
           for (int m = 0; m < 8; ++m)
-            if (lane + 32 * m < NR2) rr[m] = __fmaf_rn(-Hs[j * HS + lane + 32 * m], e, rr[m]);
+            if (lane + 32 * m < NR2) rr[m] = __fmaf_rn(-Hs[j * HS + lane + 32 * m], ev, rr[m]);
         }
       }
 #pragma unroll
@@ -333,13 +333,7 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
     }
   const int nb = a.M == 4 ? 1 : 2;
   for (int j = tid; j < D; j += kReadThreads) {
-    int v = xq8[j];
-    if (gi < R) {
-      const int8_t* s = a.spins + ((size_t)b * R + gi) * P * D;
-      int d = 0;
-      for (int p = 0; p < P; ++p) d += s[p * D + j];
-      v = min(max(v + d, lo), hi);
-    }
+    const int v = xq8[j] + (gi < R ? ek[gi * D + j] : 0);
     a.levels[(size_t)b * D + j] = (int8_t)v;
     if (nb == 1) {
       a.bits[(size_t)b * D + j] = v > 0;
@@ -354,18 +348,22 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   }
 }
 
+}  // namespace arp
+
+namespace arp {
+
 cudaError_t map_dispatch(const MapParams& a, cudaStream_t st) {
   const int D = a.D;
   return D <= 16 ? launch_map<1>(a, st) : D <= 32 ? launch_map<2>(a, st) : D <= 64 ? launch_map<4>(a, st)
                                                                           : launch_map<8>(a, st);
 }
 
-static size_t readout_smem(int D, int NR2) {
-  return sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + ((D + 15) & ~15);
+static size_t readout_smem(int D, int NR2, int R) {
+  return sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + (size_t)(R + 1) * D + 16;
 }
 
 cudaError_t readout_dispatch(const ReadParams& a, cudaStream_t st) {
-  const size_t smem = readout_smem(a.D, a.NR2);
+  const size_t smem = readout_smem(a.D, a.NR2, a.R);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -443,7 +441,7 @@ extern "C" int arp_readout_dd(const float* H, const float* y, const int8_t* xq, 
     return ARP_ERR_SHAPE;
   if (B == 0) return ARP_OK;
   if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist) return ARP_ERR_ARG;
-  if (readout_smem(D, NR2) > 227 * 1024) return ARP_ERR_SHAPE;
+  if (readout_smem(D, NR2, R) > 227 * 1024) return ARP_ERR_SHAPE;
   ReadParams a{H, y, xq, spins, B, NR2, D, P, R, M, levels, bits, dist, pick};
   return readout_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

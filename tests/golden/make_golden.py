@@ -15,6 +15,8 @@ Fixtures (all small, numpy .npz):
                       (CPU generator, fewer instances), modes 'chains' and 'best'.
   golden_mapping.npz  the float chain: draws, MMSE guess, ising_delta_at scale, to_fixed/compress
                       integers, spins_to_levels_delta, dist and select on fixed spin sets.
+  golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
+                      (sim/a56an.py:74-108) on seeded per-use error vectors (`... /root/reference stats`).
 """
 import math
 import os
@@ -190,7 +192,33 @@ def mapping_fixture():
     np.savez_compressed(os.path.join(OUT, 'golden_mapping.npz'), **out)
 
 
+def stats_fixture():
+    """stats_chord.boot_ber, a56an.boot_ratio and a56an.mcnemar on seeded per-use error vectors."""
+    import importlib.util
+    import stats_chord
+
+    spec = importlib.util.spec_from_file_location('a56an_ref', os.path.join(REF, 'arpeggio/sim/a56an.py'))
+    a56 = importlib.util.module_from_spec(spec)
+    try:
+        spec.loader.exec_module(a56)
+    except SystemExit:
+        pass
+    rng = np.random.default_rng(99)
+    a = (rng.random(3000) < 0.02) * rng.integers(1, 4, 3000)
+    b = (rng.random(3000) < 0.03) * rng.integers(1, 4, 3000)
+    lo, hi, _ = stats_chord.boot_ber(a, 64, B=500)
+    r0, rlo, rhi = a56.boot_ratio(a, b, B=800)
+    p, x, y = a56.mcnemar(a, b)
+    np.savez_compressed(os.path.join(OUT, 'golden_stats.npz'), a=a, b=b,
+                        boot_ber=np.array([lo, hi]), boot_ratio=np.array([r0, rlo, rhi]), mcnemar=np.array([p, x, y]))
+    print('stats', lo, hi, r0, rlo, rhi, p)
+
+
 if __name__ == '__main__':
+    if len(sys.argv) > 2 and sys.argv[2] == 'stats':
+        stats_fixture()
+        sys.exit(0)
+    stats_fixture()
     philox_fixture()
     arpeggio_fixture()
     chord_fixture()

@@ -27,6 +27,11 @@ SIGNATURES = {
     'arp_detect_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U, _I, _P,
                       ctypes.c_size_t, _P, _P, _P, _P, _P, _P],
     'arp_detect_dd_workspace': [_I, _I, _I, _I, _I, _P],
+    'arp_mdi_guesses': [_P, _P, _P, _I, _I, _I, _I, _P, _P, _P],
+    'arp_mdi_radius': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P],
+    'arp_mdi_map': [_P, _P, _P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P],
+    'arp_mdi_update': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P],
+    'arp_mdi_select': [_P, _P, _I, _I, _I, _I, _P, _P, _P],
     'arp_detect_dd_static': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U,
                              _I, _P, _P, _P, _P, _P, _P],
 }

@@ -37,6 +37,9 @@ struct MapParams {
   int8_t* xq;           // (B, D)
   float* scale;         // (B)
   int32_t* status;
+  const int32_t* idx = nullptr;  // (B) rows of H, y (and of xg) for each problem, or null: b
+  const int8_t* xg = nullptr;    // guesses to map around (row idx[b] with stride xg_stride), or null: MMSE guess
+  int xg_stride = 0;
 };
 
 struct ReadParams {
@@ -49,6 +52,16 @@ struct ReadParams {
   int8_t* bits;         // (B, D * nb)
   float* dist;          // (B)
   int32_t* pick;        // (B) winning candidate (R = the guess), may be null
+  // MDI update mode (mdi != 0): problem b is use idx[b]; candidates are taken around xg[idx[b] * xg_stride];
+  // the first best candidate replaces the use's current best bl[idx[b] * bl_stride * D] and
+  // bd[idx[b] * bl_stride] only if it is strictly closer (mimo.py:590-593); levels/bits/dist/pick unused.
+  const int32_t* idx = nullptr;
+  const int8_t* xg = nullptr;
+  int xg_stride = 0;
+  int8_t* bl = nullptr;
+  float* bd = nullptr;
+  int bl_stride = 0;
+  int mdi = 0;
 };
 
 // policy: 0 first accept, 1 Chord round; flt: FP32 fields.  Shapes already validated.

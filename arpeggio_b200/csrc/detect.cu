@@ -63,8 +63,9 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
   float* red = xv + Dp;           // 8
   const int D = a.D, NR2 = a.NR2, b = blockIdx.x;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4, lane = tid & 31;
-  const float* Hb = a.H + (size_t)b * NR2 * D;
-  const float* yb = a.y + (size_t)b * NR2;
+  const int u = a.idx ? a.idx[b] : b;
+  const float* Hb = a.H + (size_t)u * NR2 * D;
+  const float* yb = a.y + (size_t)u * NR2;
   float A[TB][TB];
 #pragma unroll
   for (int i = 0; i < TB; ++i)
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
       for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * Dp + tid], yb[r0 + r], gacc);
   }
   float qmax = 0.0f;
-  const float s2 = a.sigma2[b];
+  const float s2 = a.xg ? 0.0f : a.sigma2[b];  // only the MMSE solve reads sigma2 (null for a given guess)
 #pragma unroll
   for (int i = 0; i < TB; ++i)
 #pragma unroll
@@ -114,67 +115,77 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
       if (gi == gj) A[i][j] = gi < D ? __fadd_rn(A[i][j], s2) : 1.0f;
     }
   if (tid < Dp) gv[tid] = gacc;
-  // ---- in-place Gauss-Jordan inverse of A = Q + sigma2 I (SPD, no pivoting), one barrier per step;
-  //      k = kt*TB + kr with kr unrolled so the register tile is always indexed at compile time
-  for (int kt = 0; kt < 16; ++kt) {
+  if (a.xg) {
+    // the guess is given (MDI stages): map around it, no MMSE solve
+    if (tid < Dp) {
+      const float lv = tid < D ? (float)a.xg[(size_t)u * a.xg_stride + tid] : 0.0f;
+      xv[tid] = lv;
+      if (tid < D) a.xq[(size_t)b * D + tid] = (int8_t)lv;
+    }
+    __syncthreads();
+  } else {
+    // ---- in-place Gauss-Jordan inverse of A = Q + sigma2 I (SPD, no pivoting), one barrier per step;
+    //      k = kt*TB + kr with kr unrolled so the register tile is always indexed at compile time
+    for (int kt = 0; kt < 16; ++kt) {
 #pragma unroll
-    for (int kr = 0; kr < TB; ++kr) {
-      const int k = kt * TB + kr, buf = (k & 1) * Dp;
-      if (ty == kt) {
+      for (int kr = 0; kr < TB; ++kr) {
+        const int k = kt * TB + kr, buf = (k & 1) * Dp;
+        if (ty == kt) {
 #pragma unroll
-        for (int j = 0; j < TB; ++j) rk[buf + tx * TB + j] = A[kr][j];
-      }
-      if (tx == kt) {
+          for (int j = 0; j < TB; ++j) rk[buf + tx * TB + j] = A[kr][j];
+        }
+        if (tx == kt) {
 #pragma unroll
-        for (int i = 0; i < TB; ++i) ck[buf + ty * TB + i] = A[i][kr];
-      }
-      __syncthreads();
-      const float inv = __frcp_rn(rk[buf + k]);
-      float f[TB], rj[TB];
+          for (int i = 0; i < TB; ++i) ck[buf + ty * TB + i] = A[i][kr];
+        }
+        __syncthreads();
+        const float inv = __frcp_rn(rk[buf + k]);
+        float f[TB], rj[TB];
 #pragma unroll
-      for (int i = 0; i < TB; ++i) {
-        f[i] = __fmul_rn(ck[buf + ty * TB + i], inv);
-        rj[i] = rk[buf + tx * TB + i];
-      }
+        for (int i = 0; i < TB; ++i) {
+          f[i] = __fmul_rn(ck[buf + ty * TB + i], inv);
+          rj[i] = rk[buf + tx * TB + i];
+        }
 #pragma unroll
-      for (int i = 0; i < TB; ++i)
+        for (int i = 0; i < TB; ++i)
 #pragma unroll
-        for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(-f[i], rj[j], A[i][j]);
-      if (ty == kt) {
+          for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(-f[i], rj[j], A[i][j]);
+        if (ty == kt) {
 #pragma unroll
-        for (int j = 0; j < TB; ++j) A[kr][j] = __fmul_rn(rj[j], inv);
-      }
-      if (tx == kt) {
+          for (int j = 0; j < TB; ++j) A[kr][j] = __fmul_rn(rj[j], inv);
+        }
+        if (tx == kt) {
 #pragma unroll
-        for (int i = 0; i < TB; ++i) A[i][kr] = -f[i];
-        if (ty == kt) A[kr][kr] = inv;
+          for (int i = 0; i < TB; ++i) A[i][kr] = -f[i];
+          if (ty == kt) A[kr][kr] = inv;
+        }
       }
     }
-  }
-  // ---- z = A^-1 g, mu = diag(A^-1 Q) (Q symmetric: sum_j Ainv_ij Q_ij), x_q
-  float zp[TB], mp[TB];
-#pragma unroll
-  for (int i = 0; i < TB; ++i) {
-    zp[i] = 0.0f;
-    mp[i] = 0.0f;
-#pragma unroll
-    for (int j = 0; j < TB; ++j) {
-      zp[i] = __fmaf_rn(A[i][j], gv[tx * TB + j], zp[i]);
-      mp[i] = __fmaf_rn(A[i][j], Qs[(ty * TB + i) * QP + tx * TB + j], mp[i]);
-    }
-    zp[i] = hsum16(zp[i]);
-    mp[i] = hsum16(mp[i]);
-  }
-  if (tx == 0) {
+    // ---- z = A^-1 g, mu = diag(A^-1 Q) (Q symmetric: sum_j Ainv_ij Q_ij), x_q
+    float zp[TB], mp[TB];
 #pragma unroll
     for (int i = 0; i < TB; ++i) {
-      const int gi = ty * TB + i;
-      const float lv = gi < D ? nearest_level(__fdiv_rn(zp[i], mp[i]), a.M) : 0.0f;
-      xv[gi] = lv;
-      if (gi < D) a.xq[(size_t)b * D + gi] = (int8_t)lv;
+      zp[i] = 0.0f;
+      mp[i] = 0.0f;
+#pragma unroll
+      for (int j = 0; j < TB; ++j) {
+        zp[i] = __fmaf_rn(A[i][j], gv[tx * TB + j], zp[i]);
+        mp[i] = __fmaf_rn(A[i][j], Qs[(ty * TB + i) * QP + tx * TB + j], mp[i]);
+      }
+      zp[i] = hsum16(zp[i]);
+      mp[i] = hsum16(mp[i]);
     }
+    if (tx == 0) {
+#pragma unroll
+      for (int i = 0; i < TB; ++i) {
+        const int gi = ty * TB + i;
+        const float lv = gi < D ? nearest_level(__fdiv_rn(zp[i], mp[i]), a.M) : 0.0f;
+        xv[gi] = lv;
+        if (gi < D) a.xq[(size_t)b * D + gi] = (int8_t)lv;
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
   // ---- h = 2 (g - Q x_q), scale = max(|h|, |Q|)
   float hp[TB];
 #pragma unroll
@@ -256,16 +267,18 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   int8_t* ek = reinterpret_cast<int8_t*>(br + 8);  // (R + 1) x D: candidate level minus guess; row R = x_q
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, W = kReadThreads / 32;
   const int lo = a.M == 4 ? -1 : -3, hi = -lo;
-  const float* Hb = a.H + (size_t)b * NR2 * D;
+  const int u = a.idx ? a.idx[b] : b;
+  const float* Hb = a.H + (size_t)u * NR2 * D;
   for (int x = tid; x < NR2 * D; x += kReadThreads) {
     const int i = x / D, j = x - i * D;
     Hs[j * HS + i] = Hb[x];
   }
   int8_t* xq8 = ek + R * D;
-  for (int j = tid; j < D; j += kReadThreads) xq8[j] = a.xq[(size_t)b * D + j];
+  for (int j = tid; j < D; j += kReadThreads)
+    xq8[j] = a.mdi ? a.xg[(size_t)u * a.xg_stride + j] : a.xq[(size_t)b * D + j];
   __syncthreads();
   // every candidate's clipped delta from the guess, from one coalesced pass over its spins
-  const int8_t* sb = a.spins + (size_t)b * R * P * D;
+  const int8_t* sb = a.spins + (size_t)b * R * P * D;  // spins are per problem b (group-local)
   for (int x = tid; x < R * D; x += kReadThreads) {
     const int c = x / D, j = x - c * D;
     int d = 0;
@@ -274,14 +287,15 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
     ek[x] = (int8_t)(xv - xq8[j]);
   }
   for (int i = tid; i < NR2; i += kReadThreads) {
-    float r = a.y[(size_t)b * NR2 + i];
+    float r = a.y[(size_t)u * NR2 + i];
     for (int j = 0; j < D; ++j) r = __fmaf_rn(-Hs[j * HS + i], (float)xq8[j], r);
     r0[i] = r;
   }
   __syncthreads();
   float best = FLT_MAX;
   int bi = INT_MAX;
-  for (int c = wid; c <= R; c += W) {
+  const int last = a.mdi ? R - 1 : R;  // MDI stages compare the candidates with the use's current best instead
+  for (int c = wid; c <= last; c += W) {
     float acc = 0.0f;
     if (c == R) {
       for (int i = lane; i < NR2; i += 32) acc = __fmaf_rn(r0[i], r0[i], acc);
@@ -331,6 +345,15 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
       gb = bd[w];
       gi = br[w];
     }
+  if (a.mdi) {
+    const float cur = a.bd[(size_t)u * a.bl_stride];
+    __syncthreads();
+    if (gb < cur) {
+      for (int j = tid; j < D; j += kReadThreads) a.bl[(size_t)u * a.bl_stride * D + j] = (int8_t)(xq8[j] + ek[gi * D + j]);
+      if (tid == 0) a.bd[(size_t)u * a.bl_stride] = gb;
+    }
+    return;
+  }
   const int nb = a.M == 4 ? 1 : 2;
   for (int j = tid; j < D; j += kReadThreads) {
     const int v = xq8[j] + (gi < R ? ek[gi * D + j] : 0);

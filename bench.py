@@ -225,6 +225,29 @@ def run_ours(args):
                         'readout, copy out); device time per replay' % (w['nt'], w['nr'], args.anneals),
                'frames': n, 'p50_us': us[n // 2], 'p99_us': us[min(n - 1, int(0.99 * n))], 'max_us': us[-1]}
 
+    # ---- the reference's full chain: multi-stage MDI at its recorded x16 point (16 x 16, 20 dB, Ns 32,
+    #      abl_far_64_0.1_0.1_0_rand_32; 267.9 detections/s recorded on a B200 with a 4-thread CPU wrapper)
+    mdi_line = None
+    if args.mdi_batch > 0:
+        from arpeggio_b200 import mdi
+        bm = channel.draw_device(4242 + rank, 20.0, args.mdi_batch, 16, 16, dev=dev)
+        mdi.detect(bm['H'][:256], bm['y'][:256], 16 / 100.0, 16, 1, 'abl_far_64_0.1_0.1_0_rand_32')
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        lv_m, ann_m, cnt_m, _ = mdi.detect(bm['H'], bm['y'], 16 / 100.0, 16, 2, 'abl_far_64_0.1_0.1_0_rand_32')
+        m1.record(stream)
+        torch.cuda.synchronize()
+        ms_m = m0.elapsed_time(m1)
+        mdi_line = {'value': args.mdi_batch / (ms_m / 1e3), 'unit': 'detections/s', 'uses': args.mdi_batch,
+                    'ms': ms_m, 'anneals_per_use': float(ann_m.mean()),
+                    'config': 'MDI-MIMO (MMSE + SIC guesses, radius rule, K=1..3, up to 8 stages), 16 x 16 16-QAM, '
+                              '20 dB, Ns 32, Arpeggio fixed point S=64 T=0.1 q=0 rand; device time incl. the host '
+                              'walk over groups',
+                    'reference_recorded': 267.9,
+                    'reference_recorded_source': 'data/results/a513_fixed/x16/arpeggiofx_64_0.1_0.1_0_rand_32/'
+                                                 'snr_20.00 (B200 anneal + 4 CPU threads)'}
+
     # ---- integer-issue peak (calibration kernel) and the anneal kernel's algorithmic work
     L = _lib.lib()
     buf = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -285,6 +308,7 @@ def run_ours(args):
                          'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if peaks else 'fallback'},
         'anneal_counters': {'flips': int(st[0]), 'tests': int(st[1]), 'anneals': B * R, 'philox_blocks': blocks},
         'latency': lat,
+        'mdi_x16': mdi_line,
         'gpu_launches': 3 * K,
         'clocks': ck,
     }
@@ -336,6 +360,7 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--chunks', type=int, default=8, help='pipelined pieces of the end-to-end step')
     ap.add_argument('--latency-frames', type=int, default=2000, help='single-frame replays for p50/p99 latency')
+    ap.add_argument('--mdi-batch', type=int, default=16384, help='uses of the multi-stage (MDI) line; 0 skips it')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.rank = int(os.environ.get('RANK', 0))

@@ -120,6 +120,31 @@ int arp_detect_dd(const float* H, const float* y, const float* sigma2, int B, in
  * scale, spins, best energy changes and (flips, tests) inside it (for inspection after a call). */
 size_t arp_detect_dd_workspace(int B, int D, int P, int R, int precision, size_t* offsets);
 
+/* Multi-stage delta-Ising detection (MDI-MIMO, arpeggio/mimo/mimo.py:553-602 and run_a513.mdi_logged,
+ * arpeggio/sim/local_code_a513/run_a513.py:42-80): the host walks stages, guesses, K and groups exactly as the
+ * reference does and calls these per group; the anneal is arp_anneal_first_accept / arp_anneal_chord_dd with
+ * inst = the group's use indices.
+ * arp_mdi_guesses: per use the hard MMSE guess (mimo.py:98-109, 176-182) and the ordered MMSE-SIC guess
+ *   (mimo.py:466-503, per='real'), int8 levels (B, D) each.
+ * arp_mdi_radius: per use and guess in cur (B, G, D): the search radius R (B, G) of mimo.mdi_radius
+ *   (mimo.py:526-543, heuristic 'mean', capped at Rmax) and ||y - H x_g||^2 (B, G).
+ * arp_mdi_map: the compressed dDI problem around guess gi of cur for the uses idx (n), as arp_map_dd
+ *   (mimo.ising_delta_at + to_fixed + compress, mimo.py:506-523).
+ * arp_mdi_update: the group's candidates (spins (n, R, P*D)) around guess gi; for each use the first closest
+ *   candidate replaces next[idx, gi] and best_dist[idx, gi] if strictly closer (mimo.py:588-593).
+ * arp_mdi_select: the first guess with the lowest distance (mimo.py:600-602), levels (B, D) and Gray bits. */
+int arp_mdi_guesses(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M, int8_t* xmmse,
+                    int8_t* xsic, void* stream);
+int arp_mdi_radius(const float* H, const float* y, const int8_t* cur, int B, int NR2, int D, int G, int M, int Rmax,
+                   int32_t* R, float* dist, void* stream);
+int arp_mdi_map(const float* H, const float* y, const int32_t* idx, int n, int NR2, int D, int M, const int8_t* cur,
+                int G, int gi, int quantize, void* Gout, void* hout, int8_t* xq, float* scale, int32_t* status,
+                void* stream);
+int arp_mdi_update(const float* H, const float* y, const int32_t* idx, int n, int NR2, int D, int P, int R, int M,
+                   const int8_t* cur, int G, int gi, const int8_t* spins, int8_t* next, float* best_dist, void* stream);
+int arp_mdi_select(const int8_t* cur, const float* dist, int B, int D, int G, int M, int8_t* levels, int8_t* bits,
+                   void* stream);
+
 /* arp_detect_dd without a workspace argument, for callers that cannot allocate device memory: a receive
  * chain with a hard per-frame latency budget cannot call cudaMalloc on the frame path (it synchronises the
  * device and takes unbounded time), and a plugin inside a host program that owns all device memory may not

@@ -15,6 +15,8 @@ Fixtures (all small, numpy .npz):
                       (CPU generator, fewer instances), modes 'chains' and 'best'.
   golden_mapping.npz  the float chain: draws, MMSE guess, ising_delta_at scale, to_fixed/compress
                       integers, spins_to_levels_delta, dist and select on fixed spin sets.
+  golden_a513_b0.npz  batch 0 of the recorded B200 runs data/results/a513_fixed/{x16,x32}: per-use bit
+                      errors, anneals per use, per-K [flips, tests, anneals] (`... /root/reference a513`).
   golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
                       (sim/a56an.py:74-108) on seeded per-use error vectors (`... /root/reference stats`).
 """
@@ -192,6 +194,25 @@ def mapping_fixture():
     np.savez_compressed(os.path.join(OUT, 'golden_mapping.npz'), **out)
 
 
+def a513_fixture():
+    """Batch 0 of the recorded B200 runs (data/results/a513_fixed): per-use bit errors, anneals per use and the
+    per-K counters [flips, tests, anneals] of info.cnt, for the on-device MDI parity test."""
+    import json
+    pts = {'x16': ('x16/arpeggiofx_64_0.1_0.1_0_rand_32/snr_20.00', 16, 20.0, 102, 'abl_far_64_0.1_0.1_0_rand_32'),
+           'x32': ('x32/arpeggiofx_32_0.1_0.1_0_rand_8/snr_22.00', 32, 22.0, 102, 'abl_far_32_0.1_0.1_0_rand_8')}
+    out = {}
+    for tag, (rel, nt, snr, seed, pick) in pts.items():
+        z = np.load(os.path.join(REF, 'data/results/a513_fixed', rel, 'b00000.npz'))
+        info = json.loads(str(z['info']))
+        out[tag + '/biterr'] = z['biterr']
+        out[tag + '/anneals'] = z['anneals']
+        out[tag + '/cnt'] = np.array([info['cnt'][str(K)] for K in (1, 2, 3)], dtype=np.int64)
+        out[tag + '/meta'] = np.array([nt, snr, seed, info['m']], dtype=np.float64)
+        out[tag + '/pick'] = np.array(pick)
+        print('a513', tag, int(z['biterr'].sum()), 'bit errors over', info['m'], 'uses')
+    np.savez_compressed(os.path.join(OUT, 'golden_a513_b0.npz'), **out)
+
+
 def stats_fixture():
     """stats_chord.boot_ber, a56an.boot_ratio and a56an.mcnemar on seeded per-use error vectors."""
     import importlib.util
@@ -215,9 +236,10 @@ def stats_fixture():
 
 
 if __name__ == '__main__':
-    if len(sys.argv) > 2 and sys.argv[2] == 'stats':
-        stats_fixture()
+    if len(sys.argv) > 2:
+        {'stats': stats_fixture, 'a513': a513_fixture}[sys.argv[2]]()
         sys.exit(0)
+    a513_fixture()
     stats_fixture()
     philox_fixture()
     arpeggio_fixture()

@@ -62,6 +62,10 @@ struct ReadParams {
   float* bd = nullptr;
   int bl_stride = 0;
   int mdi = 0;
+  // soft output (llr != null): max-log LLRs over the list and the single-bit-flip neighbours of the decision
+  const float* N0 = nullptr;  // (B) noise density of each use
+  float clip = 0.0f;
+  float* llr = nullptr;       // (B, D * nb), positive = bit 1
 };
 
 // policy: 0 first accept, 1 Chord round; flt: FP32 fields.  Shapes already validated.

@@ -295,6 +295,11 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   float best = FLT_MAX;
   int bi = INT_MAX;
   const int last = a.mdi ? R - 1 : R;  // MDI stages compare the candidates with the use's current best instead
+  const int nbl = a.M == 4 ? 1 : 2, nbits = D * nbl;
+  const bool soft = a.llr != nullptr;
+  float mb0[8], mb1[8];  // per-warp minima of the distance over list entries with bit k = 0 / 1, k = lane + 32 m
+#pragma unroll
+  for (int m = 0; m < 8; ++m) mb0[m] = mb1[m] = FLT_MAX;
   for (int c = wid; c <= last; c += W) {
     float acc = 0.0f;
     if (c == R) {
@@ -332,6 +337,21 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
       best = acc;
       bi = c;
     }
+    if (soft) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int k = lane + 32 * m;
+        if (k < nbits) {
+          const int j = k / nbl;
+          const int v = xq8[j] + (c < R ? ek[c * D + j] : 0);
+          const bool bit = (k - j * nbl) == 0 ? v > 0 : (v == 1 || v == -1);
+          if (bit)
+            mb1[m] = fminf(mb1[m], acc);
+          else
+            mb0[m] = fminf(mb0[m], acc);
+        }
+      }
+    }
   }
   if (lane == 0) {
     bd[wid] = best;
@@ -345,6 +365,116 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
       gb = bd[w];
       gi = br[w];
     }
+  if (soft) {
+    // ---- max-log LLRs over the list and the single-bit-flip neighbours of the decision (mimo.py:434-462)
+    unsigned char* base = reinterpret_cast<unsigned char*>(ek) + (size_t)(R + 1) * D;
+    base += (16 - (reinterpret_cast<uintptr_t>(base) & 15)) & 15;
+    int* s0 = reinterpret_cast<int*>(base);  // list minima, bit 0 (non-negative floats order as their patterns)
+    int* s1 = s0 + nbits;                    // list minima, bit 1
+    float* rh = reinterpret_cast<float*>(s1 + nbits);  // residual of the decision, NR2
+    float* cj = rh + NR2;                    // H_j^T rh
+    float* nj = cj + D;                      // ||H_j||^2
+    float* dn = nj + D;                      // neighbour distances, nbits
+    float* rv = dn + nbits;                  // 8 warps x (min1, min2)
+    int* ri = reinterpret_cast<int*>(rv + 16);
+    for (int k = tid; k < nbits; k += kReadThreads) s0[k] = s1[k] = __float_as_int(FLT_MAX);
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int k = lane + 32 * m;
+      if (k < nbits) {
+        atomicMin(&s0[k], __float_as_int(mb0[m]));
+        atomicMin(&s1[k], __float_as_int(mb1[m]));
+      }
+    }
+    for (int i = tid; i < NR2; i += kReadThreads) {
+      float r = r0[i];
+      if (gi < R)
+        for (int j = 0; j < D; ++j)
+          if (ek[gi * D + j]) r = __fmaf_rn(-Hs[j * HS + i], (float)ek[gi * D + j], r);
+      rh[i] = r;
+    }
+    __syncthreads();
+    for (int j = tid; j < D; j += kReadThreads) {
+      float c = 0.0f, n = 0.0f;
+      for (int i = 0; i < NR2; ++i) {
+        const float hv = Hs[j * HS + i];
+        c = __fmaf_rn(hv, rh[i], c);
+        n = __fmaf_rn(hv, hv, n);
+      }
+      cj[j] = c;
+      nj[j] = n;
+    }
+    __syncthreads();
+    float n1 = FLT_MAX, n2 = FLT_MAX;
+    int i1 = INT_MAX;
+    for (int k = tid; k < nbits; k += kReadThreads) {
+      const int j = k / nbl;
+      const int lv = xq8[j] + (gi < R ? ek[gi * D + j] : 0);
+      // Gray neighbour: the MSB flips the sign; the LSB swaps +-1 and +-3 (16-QAM)
+      const int nl = (k - j * nbl) == 0 ? -lv : (lv > 0 ? 4 - lv : -4 - lv);
+      const float del = (float)(nl - lv);
+      const float d = __fmaf_rn(del * del, nj[j], __fmaf_rn(-2.0f * del, cj[j], gb));
+      dn[k] = d;
+      if (d < n1) {
+        n2 = n1;
+        n1 = d;
+        i1 = k;
+      } else if (d < n2) {
+        n2 = d;
+      }
+    }
+    // block-wide smallest and second smallest neighbour distance
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const float o1 = __shfl_xor_sync(ARP_FULL, n1, o), o2 = __shfl_xor_sync(ARP_FULL, n2, o);
+      const int oi = __shfl_xor_sync(ARP_FULL, i1, o);
+      if (o1 < n1 || (o1 == n1 && oi < i1)) {
+        n2 = fminf(n1, o2);
+        n1 = o1;
+        i1 = oi;
+      } else {
+        n2 = fminf(n2, o1);
+      }
+    }
+    if (lane == 0) {
+      rv[2 * wid] = n1;
+      rv[2 * wid + 1] = n2;
+      ri[wid] = i1;
+    }
+    __syncthreads();
+    n1 = FLT_MAX;
+    n2 = FLT_MAX;
+    i1 = INT_MAX;
+    for (int w = 0; w < W; ++w) {
+      const float o1 = rv[2 * w], o2 = rv[2 * w + 1];
+      const int oi = ri[w];
+      if (o1 < n1 || (o1 == n1 && oi < i1)) {
+        n2 = fminf(n1, o2);
+        n1 = o1;
+        i1 = oi;
+      } else {
+        n2 = fminf(n2, o1);
+      }
+    }
+    const float inv_n0 = 1.0f / a.N0[u];
+    for (int k = tid; k < nbits; k += kReadThreads) {
+      const int j = k / nbl;
+      const int lv = xq8[j] + (gi < R ? ek[gi * D + j] : 0);
+      const bool bh = (k - j * nbl) == 0 ? lv > 0 : (lv == 1 || lv == -1);
+      const float same = k == i1 ? n2 : n1;  // nearest neighbour that keeps bit k
+      float m0 = __int_as_float(s0[k]), m1 = __int_as_float(s1[k]);
+      if (bh) {
+        m1 = fminf(m1, same);
+        m0 = fminf(m0, dn[k]);
+      } else {
+        m0 = fminf(m0, same);
+        m1 = fminf(m1, dn[k]);
+      }
+      const float l = (m0 - m1) * inv_n0;
+      a.llr[(size_t)b * nbits + k] = fminf(fmaxf(l, -a.clip), a.clip);
+    }
+  }
   if (a.mdi) {
     const float cur = a.bd[(size_t)u * a.bl_stride];
     __syncthreads();
@@ -381,12 +511,14 @@ cudaError_t map_dispatch(const MapParams& a, cudaStream_t st) {
                                                                           : launch_map<8>(a, st);
 }
 
-static size_t readout_smem(int D, int NR2, int R) {
-  return sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + (size_t)(R + 1) * D + 16;
+static size_t readout_smem(int D, int NR2, int R, bool soft = false) {
+  size_t s = sizeof(float) * ((size_t)D * (NR2 + 1) + NR2 + 8) + 8 * sizeof(int) + (size_t)(R + 1) * D + 16;
+  if (soft) s += 16 + sizeof(float) * (3 * (size_t)D * 2 + NR2 + 2 * (size_t)D + 24);  // s0, s1, dn, rh, cj, nj, rv, ri
+  return s;
 }
 
 cudaError_t readout_dispatch(const ReadParams& a, cudaStream_t st) {
-  const size_t smem = readout_smem(a.D, a.NR2, a.R);
+  const size_t smem = readout_smem(a.D, a.NR2, a.R, a.llr != nullptr);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -466,5 +598,20 @@ extern "C" int arp_readout_dd(const float* H, const float* y, const int8_t* xq, 
   if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist) return ARP_ERR_ARG;
   if (readout_smem(D, NR2, R) > 227 * 1024) return ARP_ERR_SHAPE;
   ReadParams a{H, y, xq, spins, B, NR2, D, P, R, M, levels, bits, dist, pick};
+  return readout_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_readout_llr_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2,
+                                  int D, int P, int R, int M, const float* N0, float clip, int8_t* levels,
+                                  int8_t* bits, float* dist, int32_t* pick, float* llr, void* stream) {
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || P < 1 || P > 6 || R < 0 || !(M == 4 || M == 16))
+    return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist || !N0 || !llr) return ARP_ERR_ARG;
+  if (readout_smem(D, NR2, R, true) > 227 * 1024) return ARP_ERR_SHAPE;
+  ReadParams a{H, y, xq, spins, B, NR2, D, P, R, M, levels, bits, dist, pick};
+  a.N0 = N0;
+  a.clip = clip;
+  a.llr = llr;
   return readout_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

@@ -180,6 +180,25 @@ class Detector:
         ev(3)
         return bits, levels, dist
 
+    def run_soft(self, H, y, seed, N0, clip=1e4, inst0=0, stream=None):
+        """Detection with soft output (the reference's dDI soft detector, softlib.detect_llr 'aned'): the same
+        map and anneal, then arp_readout_llr_dd.  N0: scalar or (B,) noise density.  Returns (bits, levels, dist,
+        llr (B, D * log2(M)/2) float32, positive = bit 1), stream-ordered."""
+        import torch
+        ev = [torch.cuda.Event() for _ in range(4)]
+        self.run(H, y, seed, inst0=inst0, stream=stream, events=ev)  # map + anneal (+ a plain readout)
+        n0 = torch.as_tensor(N0, dtype=torch.float32).reshape(-1).to(self.device)
+        n0 = n0.expand(self.B).contiguous() if n0.numel() == 1 else n0.contiguous()
+        if getattr(self, 'llr', None) is None:
+            self.llr = torch.empty(self.bits.shape, dtype=torch.float32, device=self.device)
+        L = _lib.lib()
+        _lib.check(L.arp_readout_llr_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.xq), _lib.ptr(self.spins), self.B,
+                                        self.NR2, self.D, self.P, self.R, self.M, _lib.ptr(n0), float(clip),
+                                        _lib.ptr(self.levels), _lib.ptr(self.bits), _lib.ptr(self.dist),
+                                        _lib.ptr(self.pick), _lib.ptr(self.llr), _lib.stream_ptr(stream)), 'readout_llr')
+        self._n0_keep = n0
+        return self.bits, self.levels, self.dist, self.llr
+
     def _run_fused(self, H, y, seed, inst0, stream):
         L = _lib.lib()
         f32 = self.precision == 'f32'

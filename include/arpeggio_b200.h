@@ -104,6 +104,14 @@ int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int N
 int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D,
                    int P, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick, void* stream);
 
+/* Soft output: arp_readout_dd plus max-log LLRs (B, D * log2(M)/2) float32, positive = bit 1, over the candidate
+ * list (the R candidates and the guess) and the single-bit-flip neighbours of the decision, divided by N0 (B)
+ * and clipped to +-clip.  Replaces mimo.list_llr (arpeggio/mimo/mimo.py:434-462) as the reference's dDI soft
+ * detector calls it (arpeggio/mimo/softlib.py:37-46, method 'aned'). */
+int arp_readout_llr_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D,
+                       int P, int R, int M, const float* N0, float clip, int8_t* levels, int8_t* bits, float* dist,
+                       int32_t* pick, float* llr, void* stream);
+
 /* The detector call in one entry point: map (arp_map_dd) -> anneal (policy 0 = first accept, 1 = Chord round;
  * precision 0 = int32 fixed point with T, c int32 and q rounded to an integer, 1 = FP32 fields with T, c, q
  * float) -> readout (arp_readout_dd), stream-ordered, with the intermediates in the caller's workspace of at

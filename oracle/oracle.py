@@ -252,3 +252,29 @@ def energy_dd(G, h, S, K):
     m = np.asarray(S, dtype=np.float64).reshape(S.shape[0], S.shape[1], P, D).sum(2)
     tr = np.trace(G, axis1=1, axis2=2)
     return -(m * h[:, None]).sum(-1) + np.einsum('brj,bjk,brk->br', m, G, m) - P * tr[:, None]
+
+
+def gray_neighbours(l, M):
+    """Single-bit-flip neighbours of levels l (B, D): (B, D*nb, D), bit order dim-major, MSB first
+    (the construction of mimo.list_llr, mimo.py:441-455)."""
+    l = np.asarray(l)
+    B, D = l.shape
+    nb = PAM[M]['bits']
+    out = np.repeat(l[:, None, :], D * nb, axis=1).copy()
+    for j in range(D):
+        for k in range(nb):
+            v = l[:, j]
+            out[:, j * nb + k, j] = -v if k == 0 else np.sign(v) * (4 - np.abs(v))
+    return out
+
+
+def list_llr(H, y, N0, allc, d, best, M, clip=50.0):
+    """mimo.list_llr (mimo.py:434-462): max-log LLRs (positive = bit 1) over the list (allc, d) and the
+    single-bit-flip neighbours of `best`, clipped to +-clip.  float64."""
+    nbr = gray_neighbours(best, M)
+    allc2 = np.concatenate([allc, nbr], 1)
+    d2 = np.concatenate([d, dist(H, y, nbr)], 1)
+    bits = levels_to_bits(allc2, M).astype(bool)
+    m1 = np.where(bits, d2[..., None], np.inf).min(1)
+    m0 = np.where(~bits, d2[..., None], np.inf).min(1)
+    return np.clip((m0 - m1) / N0, -clip, clip)

@@ -14,7 +14,8 @@ Fixtures (all small, numpy .npz):
   golden_chord.npz    chordfx.chord_fx (chordfx.py:80-118) on the cases of arpeggio/mimo/test_kernel.py:213-221
                       (CPU generator, fewer instances), modes 'chains' and 'best'.
   golden_mapping.npz  the float chain: draws, MMSE guess, ising_delta_at scale, to_fixed/compress
-                      integers, spins_to_levels_delta, dist and select on fixed spin sets.
+                      integers, spins_to_levels_delta, dist, select and list_llr (mimo.py:434-462, clip 1e4,
+                      as softlib.detect_llr) on fixed spin sets.
   golden_a513_b0.npz  batch 0 of the recorded B200 runs data/results/a513_fixed/{x16,x32}: per-use bit
                       errors, anneals per use, per-K [flips, tests, anneals] (`... /root/reference a513`).
   golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
@@ -184,7 +185,8 @@ def mapping_fixture():
             S = torch.from_numpy(rng.choice([-1.0, 1.0], size=(B, 5, 2 * K * 2 * nt)).astype(np.float32))
             Lc = mimo.spins_to_levels_delta(S, I, 16)
             dd = mimo.dist(b, Lc)
-            lh, _, _ = mimo.select(b, Lc, lm)
+            lh, allc, dsel = mimo.select(b, Lc, lm)
+            out['%s/K%d/llr' % (tag, K)] = mimo.list_llr(b, allc, dsel, lh, clip=1e4).numpy()
             out['%s/K%d/S' % (tag, K)] = S.numpy().astype(np.int8)
             out['%s/K%d/Lc' % (tag, K)] = Lc.numpy().astype(np.int8)
             out['%s/K%d/dist' % (tag, K)] = dd.numpy()
@@ -237,7 +239,7 @@ def stats_fixture():
 
 if __name__ == '__main__':
     if len(sys.argv) > 2:
-        {'stats': stats_fixture, 'a513': a513_fixture}[sys.argv[2]]()
+        {'stats': stats_fixture, 'a513': a513_fixture, 'mapping': mapping_fixture}[sys.argv[2]]()
         sys.exit(0)
     a513_fixture()
     stats_fixture()

@@ -351,3 +351,54 @@ def test_small_batch_split_and_graph_replay():
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(bo, bits.cpu()) and torch.equal(do, dist.cpu())
+
+
+def test_soft_output_llr_vs_reference(golden):
+    """arp_readout_llr_dd == mimo.list_llr (the reference's dDI soft detector, softlib.detect_llr 'aned') on the
+    golden candidate lists: the same decision and LLRs within the float32 tolerance of differences of distances."""
+    from arpeggio_b200 import _lib
+    z = golden('golden_mapping.npz')
+    L = _lib.lib()
+    for tag in ('x16', 'x32', 'x64'):
+        for K in (1, 2):
+            H = torch.from_numpy(z[tag + '/H']).cuda().contiguous()
+            y = torch.from_numpy(z[tag + '/y']).cuda().contiguous()
+            B, NR2, D = H.shape
+            S = torch.from_numpy(z['%s/K%d/S' % (tag, K)]).cuda().contiguous()
+            R = S.shape[1]
+            xq = torch.from_numpy(z[tag + '/xq'].astype(np.int8)).cuda()
+            N0 = torch.full((B,), float(z[tag + '/N0'][0]), dtype=torch.float32, device='cuda')
+            lv = torch.empty(B, D, dtype=torch.int8, device='cuda')
+            bits = torch.empty(B, 2 * D, dtype=torch.int8, device='cuda')
+            dist = torch.empty(B, dtype=torch.float32, device='cuda')
+            llr = torch.empty(B, 2 * D, dtype=torch.float32, device='cuda')
+            _lib.check(L.arp_readout_llr_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(xq), _lib.ptr(S), B, NR2, D, 2 * K, R,
+                                            16, _lib.ptr(N0), 1e4, _lib.ptr(lv), _lib.ptr(bits), _lib.ptr(dist), None,
+                                            _lib.ptr(llr), _lib.stream_ptr()), 'readout_llr')
+            torch.cuda.synchronize()
+            assert np.array_equal(lv.cpu().numpy(), z['%s/K%d/sel' % (tag, K)]), (tag, K)
+            np.testing.assert_allclose(llr.cpu().numpy(), z['%s/K%d/llr' % (tag, K)], rtol=1e-3, atol=5e-2)
+
+
+def test_detector_soft_output_vs_oracle():
+    """Detector.run_soft: LLRs of the GPU's own candidate list equal the numpy list_llr over the same list."""
+    from arpeggio_b200 import channel, detector
+    B, nt, snr = 200, 16, 10.0
+    b = channel.draw(808, snr, 0, B, nt, 16)
+    det = detector.Detector(B, nt, anneals=8)
+    det.set_noise(snr)
+    bits, levels, dist, llr = det.run_soft(b['H'].cuda(), b['y'].cuda(), 4, b['N0'])
+    torch.cuda.synchronize()
+    det.check()
+    H, y = b['H'].numpy(), b['y'].numpy()
+    xq = det.xq.cpu().numpy().astype(np.int64)
+    cand = O.spins_to_levels_delta(det.spins.cpu().numpy(), xq, 1, 16)
+    allc = np.concatenate([cand, xq[:, None, :]], 1)
+    d = O.dist(H, y, allc)
+    best = allc[np.arange(B), d.argmin(1)]
+    assert (best == levels.cpu().numpy()).all(-1).mean() >= 0.99
+    ref = O.list_llr(H, y, b['N0'], allc, d, levels.cpu().numpy().astype(np.int64), 16, clip=1e4)
+    np.testing.assert_allclose(llr.cpu().numpy(), ref, rtol=1e-3, atol=5e-2)
+    # the decision's own bits sit on the positive side of every LLR
+    lv = llr.cpu().numpy()
+    assert ((lv > 0) == bits.cpu().numpy().astype(bool)).mean() >= 0.999

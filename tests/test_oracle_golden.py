@@ -95,3 +95,17 @@ def test_readout_matches_reference(golden):
             sel, _ = O.select(H, y, Lc, xq)
             assert np.array_equal(sel, z['%s/K%d/sel' % (tag, K)])
             assert np.array_equal(O.levels_to_bits(sel, 16), z['%s/K%d/bits' % (tag, K)])
+
+
+def test_list_llr_restatement_matches_reference(golden):
+    """The numpy list_llr (float64) against mimo.list_llr (float32 torch) on the golden candidate lists."""
+    z = golden('golden_mapping.npz')
+    for tag in ('x16', 'x32', 'x64'):
+        H, y, xq, N0 = z[tag + '/H'], z[tag + '/y'], z[tag + '/xq'], float(z[tag + '/N0'][0])
+        for K in (1, 2):
+            Lc = O.spins_to_levels_delta(z['%s/K%d/S' % (tag, K)], xq, K, 16)
+            allc = np.concatenate([Lc, xq[:, None, :]], 1)
+            d = O.dist(H, y, allc)
+            best = allc[np.arange(allc.shape[0]), d.argmin(1)]
+            llr = O.list_llr(H, y, N0, allc, d, best, 16, clip=1e4)
+            np.testing.assert_allclose(llr, z['%s/K%d/llr' % (tag, K)], rtol=1e-3, atol=2e-2)

@@ -24,6 +24,9 @@ SIGNATURES = {
     'arp_anneal_chord': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _U, _U, _U, _I, _I, _P, _P, _P, _P, _P],
     'arp_map_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P],
     'arp_readout_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P],
+    'arp_map_ri': [_P, _P, _P, _I, _I, _I, _I, _F, _P, _P, _P, _P, _P, _P, _P],
+    'arp_anneal_full_f32': [_I, _P, _P, _P, _P, _P, _I, _F, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _P],
+    'arp_readout_ri': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P],
     'arp_readout_llr_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _F, _P, _P, _P, _P, _P, _P],
     'arp_detect_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U, _I, _P,
                       ctypes.c_size_t, _P, _P, _P, _P, _P, _P],

@@ -40,6 +40,15 @@ struct MapParams {
   const int32_t* idx = nullptr;  // (B) rows of H, y (and of xg) for each problem, or null: b
   const int8_t* xg = nullptr;    // guesses to map around (row idx[b] with stride xg_stride), or null: MMSE guess
   int xg_stride = 0;
+  // RI map (ri != 0; mimo.ising, mimo.py:132-149): N = D * log2(M)/2 spins, outputs J (B, N, N) float scaled,
+  // h0 (B, N), h = h0 + 2 r sP (B, N), sP (B, N) int8 spins of the hard MMSE z; xq gets the biased-corrected
+  // hard decision (mmse_hard) for the final selection; G/h above are not written.
+  int ri = 0;
+  float r_reg = 0.15f;
+  float* Jri = nullptr;
+  float* h0ri = nullptr;
+  float* hri = nullptr;
+  int8_t* sP = nullptr;
 };
 
 struct ReadParams {
@@ -62,6 +71,7 @@ struct ReadParams {
   float* bd = nullptr;
   int bl_stride = 0;
   int mdi = 0;
+  int ri = 0;  // candidates are RI spins (levels 2 s1 + s2, or s for QPSK) instead of dDI deltas
   // soft output (llr != null): max-log LLRs over the list and the single-bit-flip neighbours of the decision
   const float* N0 = nullptr;  // (B) noise density of each use
   float clip = 0.0f;

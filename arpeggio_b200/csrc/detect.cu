@@ -182,9 +182,71 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
         const float lv = gi < D ? nearest_level(__fdiv_rn(zp[i], mp[i]), a.M) : 0.0f;
         xv[gi] = lv;
         if (gi < D) a.xq[(size_t)b * D + gi] = (int8_t)lv;
+        ck[gi] = gi < D ? nearest_level(zp[i], a.M) : 0.0f;  // RI map: spins of the unbiased z (mimo.py:148)
       }
     }
     __syncthreads();
+  }
+  if (a.ri) {
+    // ---- RI map: T = [2I, I] (16-QAM) or I (QPSK); h = 2 (HT)^T y, J = -offdiag(T^T Q T), scale by max
+    const bool qam = a.M == 16;
+    const int N = qam ? 2 * D : D;
+    float off = 0.0f, dgm = 0.0f, gm = 0.0f;
+#pragma unroll
+    for (int i = 0; i < TB; ++i)
+#pragma unroll
+      for (int j = 0; j < TB; ++j) {
+        const int gi = ty * TB + i, gj = tx * TB + j;
+        if (gi < D && gj < D) {
+          const float v = fabsf(Qs[gi * QP + gj]);
+          if (gi == gj)
+            dgm = fmaxf(dgm, v);
+          else
+            off = fmaxf(off, v);
+        }
+      }
+    if (tid < D) gm = fabsf(gv[tid]);
+    float sc = qam ? fmaxf(fmaxf(4.0f * off, 2.0f * dgm), 4.0f * gm) : fmaxf(off, 2.0f * gm);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sc = fmaxf(sc, __shfl_xor_sync(ARP_FULL, sc, o));
+    if (lane == 0) red[tid >> 5] = sc;
+    __syncthreads();
+    sc = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kMapThreads / 32; ++w) sc = fmaxf(sc, red[w]);
+    sc = fmaxf(sc, 1e-12f);
+    if (tid == 0) a.scale[b] = sc;
+    float* Jo = a.Jri + (size_t)b * N * N;
+#pragma unroll
+    for (int i = 0; i < TB; ++i)
+#pragma unroll
+      for (int j = 0; j < TB; ++j) {
+        const int gi = ty * TB + i, gj = tx * TB + j;
+        if (gi >= D || gj >= D) continue;
+        const float q = Qs[gi * QP + gj];
+        if (qam) {
+          Jo[(size_t)gi * N + gj] = gi == gj ? 0.0f : __fdiv_rn(-4.0f * q, sc);
+          Jo[(size_t)gi * N + D + gj] = __fdiv_rn(-2.0f * q, sc);
+          Jo[(size_t)(D + gi) * N + gj] = __fdiv_rn(-2.0f * q, sc);
+          Jo[(size_t)(D + gi) * N + D + gj] = gi == gj ? 0.0f : __fdiv_rn(-q, sc);
+        } else {
+          Jo[(size_t)gi * N + gj] = gi == gj ? 0.0f : __fdiv_rn(-q, sc);
+        }
+      }
+    const float r2 = __fmul_rn(2.0f, a.r_reg);
+    for (int i = tid; i < D; i += kMapThreads) {
+      const float lv = ck[i];
+      const float hv[2] = {qam ? __fmul_rn(4.0f, gv[i]) : __fmul_rn(2.0f, gv[i]), __fmul_rn(2.0f, gv[i])};
+      const float sp[2] = {qam ? (lv > 0.0f ? 1.0f : -1.0f) : lv, (lv == 3.0f || lv == -1.0f) ? 1.0f : -1.0f};
+      for (int c = 0; c < (qam ? 2 : 1); ++c) {
+        const int k = c * D + i;
+        const float h0 = __fdiv_rn(hv[c], sc);
+        a.h0ri[(size_t)b * N + k] = h0;
+        a.hri[(size_t)b * N + k] = __fadd_rn(h0, __fmul_rn(r2, sp[c]));
+        a.sP[(size_t)b * N + k] = (int8_t)sp[c];
+      }
+    }
+    return;
   }
   // ---- h = 2 (g - Q x_q), scale = max(|h|, |Q|)
   float hp[TB];
@@ -281,9 +343,14 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   const int8_t* sb = a.spins + (size_t)b * R * P * D;  // spins are per problem b (group-local)
   for (int x = tid; x < R * D; x += kReadThreads) {
     const int c = x / D, j = x - c * D;
-    int d = 0;
-    for (int p = 0; p < P; ++p) d += sb[(size_t)c * P * D + p * D + j];
-    const int xv = min(max((int)xq8[j] + d, lo), hi);
+    int xv;
+    if (a.ri) {  // RI spins: l = 2 s1 + s2 (16-QAM) or s (QPSK), mimo.spins_to_levels (mimo.py:39-42)
+      xv = P == 1 ? sb[(size_t)c * D + j] : 2 * sb[(size_t)c * 2 * D + j] + sb[(size_t)c * 2 * D + D + j];
+    } else {
+      int d = 0;
+      for (int p = 0; p < P; ++p) d += sb[(size_t)c * P * D + p * D + j];
+      xv = min(max((int)xq8[j] + d, lo), hi);
+    }
     ek[x] = (int8_t)(xv - xq8[j]);
   }
   for (int i = tid; i < NR2; i += kReadThreads) {
@@ -613,5 +680,32 @@ extern "C" int arp_readout_llr_dd(const float* H, const float* y, const int8_t* 
   a.N0 = N0;
   a.clip = clip;
   a.llr = llr;
+  return readout_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_map_ri(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M, float r,
+                          float* J, float* h0, float* h, int8_t* sP, int8_t* xq, float* scale, void* stream) {
+  if (B < 0 || D < 1 || D > 64 || NR2 < 1 || NR2 > 1024 || !(M == 4 || M == 16)) return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!H || !y || !sigma2 || !J || !h0 || !h || !sP || !xq || !scale) return ARP_ERR_ARG;
+  MapParams a{H, y, sigma2, B, NR2, D, M, 0.0f, nullptr, nullptr, xq, scale, nullptr};
+  a.ri = 1;
+  a.r_reg = r;
+  a.Jri = J;
+  a.h0ri = h0;
+  a.hri = h;
+  a.sP = sP;
+  return map_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_readout_ri(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2,
+                              int D, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick,
+                              void* stream) {
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || R < 0 || !(M == 4 || M == 16)) return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist) return ARP_ERR_ARG;
+  if (readout_smem(D, NR2, R) > 227 * 1024) return ARP_ERR_SHAPE;
+  ReadParams a{H, y, xq, spins, B, NR2, D, M == 16 ? 2 : 1, R, M, levels, bits, dist, pick};
+  a.ri = 1;
   return readout_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

@@ -333,3 +333,56 @@ def solver_protocol(policy='arpeggio', precision='int', seed=0, key_step=0xD1B54
         check_status(status)
         return s_.float().to(I['h'].device)
     return solver
+
+
+def detect_ri(H, y, M=16, snr_db=None, N0=None, anneals=16, sweeps=64, T0=0.1, T1=0.1, q=0.0, seed=0,
+              start='mmse', policy='arpeggio', r=0.15, kappa=0.0, inst0=0):
+    """Detection on the RI map (mimo.ising: each PAM coordinate as 2 s1 + s2), FP32 fields on the full J, anneals
+    started at the MMSE spins ('mmse') or at random ('rand'); candidates of every anneal plus the hard MMSE
+    decision go to the distance selection (the reference's fxdetect.detect for kind 'ri', fxdetect.py:24-43).
+    Returns a dict of device tensors: bits, levels, dist, spins, de, st, J, h, h0, sP, xq, scale."""
+    L_ = _lib.lib()
+    H = torch.as_tensor(H, dtype=torch.float32).cuda().contiguous()
+    y = torch.as_tensor(y, dtype=torch.float32).cuda().contiguous()
+    B, NR2, D = H.shape
+    dev = H.device
+    if N0 is None:
+        N0 = (D // 2) / (10 ** (snr_db / 10))
+    n0 = torch.as_tensor(N0, dtype=torch.float64).reshape(-1)
+    s2 = ((n0 / 2) / el2(M)).float().to(dev)
+    sigma2 = s2.expand(B).contiguous() if s2.numel() == 1 else s2.contiguous()
+    N = 2 * D if M == 16 else D
+    P = 2 if M == 16 else 1
+    f = torch.float32
+    J = torch.empty(B, N, N, dtype=f, device=dev)
+    h0, h = torch.empty(B, N, dtype=f, device=dev), torch.empty(B, N, dtype=f, device=dev)
+    sP = torch.empty(B, N, dtype=torch.int8, device=dev)
+    xq = torch.empty(B, D, dtype=torch.int8, device=dev)
+    scale = torch.empty(B, dtype=f, device=dev)
+    sp = _lib.stream_ptr()
+    _lib.check(L_.arp_map_ri(_lib.ptr(H), _lib.ptr(y), _lib.ptr(sigma2), B, NR2, D, M, float(r), _lib.ptr(J),
+                             _lib.ptr(h0), _lib.ptr(h), _lib.ptr(sP), _lib.ptr(xq), _lib.ptr(scale), sp), 'map_ri')
+    if policy == 'arpeggio':
+        T, qq, c = arpeggio_schedule(sweeps, T0, T1, q, P // 2 if P > 1 else 1, 'f32')
+        if P == 1:
+            T = T[::2]
+    else:
+        T, qq, c = chord_schedule(sweeps * P, T0, T1, q, kappa, precision='f32')
+    Tt = torch.tensor(T, dtype=f, device=dev)
+    ct = None if c is None else torch.tensor(c, dtype=f, device=dev)
+    inst = torch.as_tensor((np.arange(inst0, inst0 + B, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)).to(dev)
+    spins = torch.empty(B, anneals, N, dtype=torch.int8, device=dev)
+    de = torch.empty(B, anneals, dtype=f, device=dev)
+    st = torch.empty(B, anneals, 2, dtype=torch.int64, device=dev)
+    _lib.check(L_.arp_anneal_full_f32(0 if policy == 'arpeggio' else 1, _lib.ptr(J), _lib.ptr(h),
+                                      _lib.ptr(sP) if start == 'mmse' else None, _lib.ptr(Tt), _lib.ptr(ct), len(T),
+                                      float(qq), P, anneals, N, B, _lib.ptr(inst), seed & M32, (seed >> 32) & M32,
+                                      _lib.ptr(spins), _lib.ptr(de), _lib.ptr(st), sp), 'anneal_full_f32')
+    levels = torch.empty(B, D, dtype=torch.int8, device=dev)
+    bits = torch.empty(B, D * PAM[M]['bits'], dtype=torch.int8, device=dev)
+    dist = torch.empty(B, dtype=f, device=dev)
+    pick = torch.empty(B, dtype=torch.int32, device=dev)
+    _lib.check(L_.arp_readout_ri(_lib.ptr(H), _lib.ptr(y), _lib.ptr(xq), _lib.ptr(spins), B, NR2, D, anneals, M,
+                                 _lib.ptr(levels), _lib.ptr(bits), _lib.ptr(dist), _lib.ptr(pick), sp), 'readout_ri')
+    return dict(bits=bits, levels=levels, dist=dist, pick=pick, spins=spins, de=de, st=st, J=J, h=h, h0=h0, sP=sP,
+                xq=xq, scale=scale, T=T, q=qq, P=P)

@@ -104,6 +104,27 @@ int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int N
 int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D,
                    int P, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick, void* stream);
 
+/* The RI map (mimo.ising, arpeggio/mimo/mimo.py:132-149): each PAM coordinate as 2 s1 + s2 (T = [2I, I];
+ * QPSK: s), N = 2D (16-QAM) or D spins: J (B, N, N) = -offdiag(T^T H^T H T) / scale, h0 (B, N) = 2 (HT)^T y / scale,
+ * h = h0 + 2 r sP (B, N) with sP (B, N) the spins of the hard MMSE z (the MMSE initialisation), xq (B, D) the
+ * bias-corrected hard MMSE decision (mimo.mmse_hard, mimo.py:91-95) for the selection, scale (B).  D <= 64. */
+int arp_map_ri(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M, float r, float* J,
+               float* h0, float* h, int8_t* sP, int8_t* xq, float* scale, void* stream);
+
+/* FP32-field anneal on a full symmetric J (B, N, N), N <= 128 spins in P banks of N/P lanes (a multiple of 32); pass
+ * k tests bank k % P.  policy 0 = first accept, 1 = Chord round (Onsager c may be NULL); s0 (B, N) start spins
+ * (the MMSE initialisation) or NULL for 'rand'.  Outputs spins (B, R, N), best energy change (B, R) (E0 units,
+ * flipping s_g moves E0 by 2 s_g u_g), (flips, tests).  The float rule of arpeggio/sim/arpx55.py:28-99 (rule (2))
+ * with Philox draws (counters as arp_anneal_first_accept's, spin index i = bank * N/P + lane). */
+int arp_anneal_full_f32(int policy, const float* J, const float* h, const int8_t* s0, const float* T, const float* c,
+                        int L, float q, int P, int R, int N, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                        int8_t* out_s, float* out_de, int64_t* out_st, void* stream);
+
+/* Readout of RI spins (B, R, 2D) or (B, R, D): candidate levels 2 s1 + s2 (mimo.spins_to_levels, mimo.py:39-42),
+ * then the selection with the guess xq (mmse_hard) as arp_readout_dd (fxdetect.py:41-42). */
+int arp_readout_ri(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D, int R,
+                   int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick, void* stream);
+
 /* Soft output: arp_readout_dd plus max-log LLRs (B, D * log2(M)/2) float32, positive = bit 1, over the candidate
  * list (the R candidates and the guess) and the single-bit-flip neighbours of the decision, divided by N0 (B)
  * and clipped to +-clip.  Replaces mimo.list_llr (arpeggio/mimo/mimo.py:434-462) as the reference's dDI soft

@@ -458,3 +458,119 @@ int orc_anneal_dd_f32(const float* G, const float* h, int B, int D, int P, int R
   orc_run(f32_job, &x, (long)B * R, nthreads);
   return 0;
 }
+
+/* ------------------------------------------------------------------ FP32 fields, full coupling J (N x N)
+ * The float first-accept / Chord rules of arpeggio/sim/arpx55.py:28-99 (arpeggio_seq, rule (2)) on a generic
+ * problem (the RI map of mimo.ising, mimo.py:132-149): N spins in P banks of D = N/P lanes, pass k tests bank
+ * k % P; fields u = h + 2 J s (J symmetric, zero diagonal), one IEEE rounding per operation:
+ *   u_i  = h_i + 2 (sum_j J_ij s_j)        sum in j order
+ *   rr   = (x >> 8) 2^-24, thr = (rr - 1/2) (4 T_k)
+ *   flip iff (s_i u_i + q) < thr           (Chord: q - c_k)
+ *   de  += 2 s_g u_g                       (exact product, one rounding)
+ *   u_i += (-4 s_g) J_ig                   (exact product, one rounding)
+ * Start: 'rand' (Philox word 0 of (2^32-1, i, r, inst) >= 2^31) or given spins s0 (B, N).  Best: lowest de after
+ * each pass. */
+typedef struct {
+  const float *J, *h, *T, *c;
+  const int8_t* s0;
+  int B, N, P, R, L;
+  float q;
+  const uint32_t* inst;
+  uint32_t k0, k1;
+  int policy;
+  int8_t* out_s;
+  float* out_de;
+  int64_t* out_st;
+} full_ctx;
+
+static void full_job(void* vctx, long t) {
+  const full_ctx* x = (const full_ctx*)vctx;
+  const int N = x->N, P = x->P, R = x->R, D = N / P;
+  const long b = t / R;
+  const uint32_t r = (uint32_t)(t % R), inst = x->inst[b];
+  const float* J = x->J + (size_t)b * N * N;
+  const float* h = x->h + (size_t)b * N;
+  int8_t s[256], bs[256];
+  uint8_t F[256];
+  float u[256];
+  for (int i = 0; i < N; i++)
+    s[i] = x->s0 ? x->s0[(size_t)b * N + i]
+                 : (philox_word(0xFFFFFFFFu, (uint32_t)i, r, inst, x->k0, x->k1, 0) >= 0x80000000u ? 1 : -1);
+  memcpy(bs, s, (size_t)N);
+  for (int i = 0; i < N; i++) {
+    volatile float acc = 0.0f;
+    for (int j = 0; j < N; j++) {
+      volatile float pj = J[i * N + j] * (float)s[j];
+      acc = acc + pj;
+    }
+    volatile float two = 2.0f * acc;
+    u[i] = h[i] + two;
+  }
+  volatile float de = 0.0f;
+  float best = INFINITY;
+  int64_t flips = 0, tests = 0;
+  for (int k = 0; k < x->L; k++) {
+    const int p = k % P;
+    const uint32_t n = (uint32_t)(k / P);
+    const float A = 4.0f * x->T[k];
+    const float qk = (x->policy == 1 && x->c) ? x->q - x->c[k] : x->q;
+    int64_t tt = 1;
+    if (x->policy == 1) memset(F, 0, sizeof F);
+    for (int jj = 0; jj < D; jj++) {
+      const int g = p * D + jj;
+      uint32_t w = philox_word(n >> 2, (uint32_t)g, r, inst, x->k0, x->k1, (int)(n & 3));
+      float thr = orc_thr(w, A);
+      volatile float su = (float)s[g] * u[g];
+      volatile float z = su + qk;
+      if (!(z < thr)) continue;
+      if (x->policy == 1) {
+        F[g] = 1;
+        continue;
+      }
+      int so = s[g];
+      volatile float e1 = (float)(2 * so) * u[g];
+      de = de + e1;
+      for (int i = 0; i < N; i++) {
+        volatile float inc = (float)(-4 * so) * J[i * N + g];
+        u[i] = u[i] + inc;
+      }
+      s[g] = (int8_t)(-so);
+      flips++;
+      if (jj < D - 1) tt++;
+    }
+    if (x->policy == 1) {
+      for (int jj = 0; jj < D; jj++) {
+        const int g = p * D + jj;
+        if (!F[g]) continue;
+        int so = s[g];
+        volatile float e1 = (float)(2 * so) * u[g];
+        de = de + e1;
+        for (int i = 0; i < N; i++) {
+          volatile float inc = (float)(-4 * so) * J[i * N + g];
+          u[i] = u[i] + inc;
+        }
+        s[g] = (int8_t)(-so);
+        flips++;
+      }
+      tt = 1;
+    }
+    tests += tt;
+    if (de < best) {
+      best = de;
+      memcpy(bs, s, (size_t)N);
+    }
+  }
+  memcpy(x->out_s + (size_t)t * N, bs, (size_t)N);
+  x->out_de[t] = best;
+  x->out_st[2 * t] = flips;
+  x->out_st[2 * t + 1] = tests;
+}
+
+int orc_anneal_full_f32(const float* J, const float* h, const int8_t* s0, int B, int N, int P, int R, const float* T,
+                        const float* c, int L, float q, const uint32_t* inst, uint32_t k0, uint32_t k1, int policy,
+                        int8_t* out_s, float* out_de, int64_t* out_st, int nthreads) {
+  if (N < 1 || N > 256 || P < 1 || N % P || L < 1 || R < 1 || B < 0) return 1;
+  full_ctx x = {J, h, T, c, s0, B, N, P, R, L, q, inst, k0, k1, policy, out_s, out_de, out_st};
+  orc_run(full_job, &x, (long)B * R, nthreads);
+  return 0;
+}

@@ -48,6 +48,9 @@ def lib():
         L.orc_anneal_dd_f32.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
                                         ctypes.c_int, ctypes.c_float, _P, ctypes.c_uint32, ctypes.c_uint32,
                                         ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_int]
+        L.orc_anneal_full_f32.argtypes = [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P,
+                                          _P, ctypes.c_int, ctypes.c_float, _P, ctypes.c_uint32, ctypes.c_uint32,
+                                          ctypes.c_int, _P, _P, _P, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -104,6 +107,56 @@ def anneal_dd_f32(G, h, P, R, T, q, inst, key, start, policy='arpeggio', c=None,
     if rc:
         raise ValueError('orc_anneal_dd_f32: unsupported shape')
     return out_s, out_de, out_st
+
+
+def anneal_full_f32(J, h, P, R, T, q, inst, key, s0=None, policy='arpeggio', c=None, nthreads=1):
+    """FP32-field anneal on a full symmetric J (B, N, N) with N/P lanes per bank (rule in arp_oracle.c, after
+    arpeggio/sim/arpx55.py:28-99); s0 (B, N) start spins or None for 'rand'.  Returns spins (B, R, N) int8,
+    best energy change (B, R) float32 (E0 units: flipping s_g changes E0 by 2 s_g u_g), (B, R, 2) [flips, tests]."""
+    J = np.ascontiguousarray(J, dtype=np.float32)
+    h = np.ascontiguousarray(h, dtype=np.float32)
+    B, N = h.shape
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    cc = None if c is None else np.ascontiguousarray(c, dtype=np.float32)
+    ss = None if s0 is None else np.ascontiguousarray(s0, dtype=np.int8)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    out_s = np.zeros((B, R, N), dtype=np.int8)
+    out_de = np.zeros((B, R), dtype=np.float32)
+    out_st = np.zeros((B, R, 2), dtype=np.int64)
+    rc = lib().orc_anneal_full_f32(_ptr(J), _ptr(h), _ptr(ss), B, N, P, R, _ptr(T), _ptr(cc), len(T), float(q),
+                                   _ptr(it), key & MASK, (key >> 32) & MASK, 0 if policy == 'arpeggio' else 1,
+                                   _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_full_f32: unsupported shape')
+    return out_s, out_de, out_st
+
+
+def ising_ri(H, y, z_mmse, M, r=0.15):
+    """mimo.ising (mimo.py:132-149), float64: T = [2I, I] (16-QAM) or I (QPSK), h = 2 (HT)^T y, J = -offdiag(T^T Q T),
+    scale = max(|h|, |J|); returns h_reg = h0 + 2 r sP, h0, J (scaled), sP (spins of the hard MMSE z), scale."""
+    H = np.asarray(H, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    D = H.shape[-1]
+    T = np.eye(D) if M == 4 else np.concatenate([2 * np.eye(D), np.eye(D)], 1)
+    HT = H @ T
+    h = 2 * np.einsum('bij,bi->bj', HT, y)
+    Q = np.einsum('bki,bkj->bij', HT, HT)
+    J = -(Q - np.einsum('bii->bi', Q)[:, :, None] * np.eye(Q.shape[-1]))
+    scale = np.maximum(np.abs(h).max(-1), np.abs(J).reshape(J.shape[0], -1).max(-1))
+    scale = np.maximum(scale, 1e-12)
+    h0 = h / scale[:, None]
+    J = J / scale[:, None, None]
+    l = quantize_levels(np.asarray(z_mmse, dtype=np.float64), M)
+    sP = l.copy() if M == 4 else np.concatenate([np.where(l > 0, 1.0, -1.0), np.where((l == 3) | (l == -1), 1.0, -1.0)], -1)
+    return h0 + 2 * r * sP, h0, J, sP, scale
+
+
+def energy_full(h, J, s):
+    """E0 = -h.s - s^T J s for s (B, R, N) (mimo.energy0, mimo.py:193-195), float64."""
+    h = np.asarray(h, dtype=np.float64)
+    J = np.asarray(J, dtype=np.float64)
+    s = np.asarray(s, dtype=np.float64)
+    return -(s * h[:, None, :]).sum(-1) - np.einsum('bri,bij,brj->br', s, J, s)
 
 
 def chord_fx(J, h, h0, T, c, q, S, P, R, seed, inst0=0, mode='chains', nthreads=1):

@@ -73,7 +73,7 @@ def detect(H, y, N0, M, seed, pick, Rmax=None, stages=None, policy='arpeggio', p
     for K in range(1, Rmax + 1):
         if policy == 'arpeggio':
             T, q, c = arpeggio_schedule(pk['S'], pk['T0'], pk['T1'], pk['q'], K, precision)
-        else:
+        else:  # Chord's MDI schedule: 128 steps per copy pair (mdi_solvers.py:18, MDICHORD)
             T, q, c = chord_schedule(pk.get('steps_per_copy_pair', 128) * 2 * K, pk['T0'], pk['T1'], pk['q'],
                                      pk.get('kappa', 0.0), precision=precision)
         sched[K] = (torch.tensor(T, dtype=tdt, device=dev), q,

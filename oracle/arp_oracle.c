@@ -18,6 +18,8 @@
  *  orc_anneal_dd_f32 the same two policies with FP32 fields (no reference kernel exists; the
  *                    rule is the integer rule of arpeggio_ref59.py:62 with the float decision
  *                    of arpeggio/sim/arpx55.py:65, written out operation by operation below).
+ *  orc_anneal_full_f32 both policies with FP32 fields on a full symmetric J (the RI map of
+ *                    arpeggio/mimo/mimo.py:132-149), the float rule of arpx55.py:28-99 with Philox draws.
  *
  * Parity pins: tests/golden (KATs of chordfx.py:53-56, outputs of arpeggio_ref59.anneal and
  * chordfx.chord_fx produced by importing the reference, generator committed beside them).

@@ -9,7 +9,8 @@ import math
 
 import torch
 
-PAM = {4: dict(levels=[-1, 1], a=1 / math.sqrt(2)), 16: dict(levels=[-3, -1, 1, 3], a=1 / math.sqrt(10))}
+PAM = {4: dict(levels=[-1, 1], a=1 / math.sqrt(2)), 16: dict(levels=[-3, -1, 1, 3], a=1 / math.sqrt(10)),
+       64: dict(levels=[-7, -5, -3, -1, 1, 3, 5, 7], a=1 / math.sqrt(42))}
 
 
 def draw_seed(seed, snr, bi):
@@ -57,9 +58,14 @@ def draw_device(seed, snr, B, nt, M, nr=None, dev='cuda'):
 
 
 def levels_to_bits(l, M):
-    """Gray bits per real dimension, MSB first (mimo.py:45-51)."""
+    """Gray bits per real dimension, MSB first (mimo.py:45-51; 64-QAM: the binary-reflected Gray code of the level
+    index, which is also what the QPSK and 16-QAM tables are)."""
     if M == 4:
         return (l > 0).to(torch.int8)
-    b1 = (l > 0).to(torch.int8)
-    b2 = (l.abs() == 1).to(torch.int8)
-    return torch.stack([b1, b2], dim=-1).flatten(-2)
+    if M == 16:
+        b1 = (l > 0).to(torch.int8)
+        b2 = (l.abs() == 1).to(torch.int8)
+        return torch.stack([b1, b2], dim=-1).flatten(-2)
+    i = ((l.to(torch.int64) + 7) // 2)
+    g = i ^ (i >> 1)
+    return torch.stack([(g >> (2 - k)) & 1 for k in range(3)], dim=-1).flatten(-2).to(torch.int8)

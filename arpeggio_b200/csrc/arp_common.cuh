@@ -85,4 +85,15 @@ __device__ __forceinline__ int bal_pattern(int P, uint32_t i) {
 
 __host__ __device__ __forceinline__ int bal_choose(int P) { return P == 2 ? 2 : (P == 4 ? 6 : 20); }
 
+// Square QAM per real dimension: L = sqrt(M) odd levels -(L-1) .. L-1, log2(L) Gray bits (binary-reflected code
+// of the level index, MSB first; for QPSK and 16-QAM this is the reference's table, mimo.py:21-22).
+__host__ __device__ __forceinline__ int pam_size(int M) { return M == 4 ? 2 : (M == 16 ? 4 : 8); }
+__host__ __device__ __forceinline__ int pam_bits(int M) { return M == 4 ? 1 : (M == 16 ? 2 : 3); }
+__device__ __forceinline__ int gray_bit(int l, int k, int M) {
+  const int L = pam_size(M), nb = pam_bits(M);
+  const int i = (l + L - 1) >> 1;
+  const int g = i ^ (i >> 1);
+  return (g >> (nb - 1 - k)) & 1;
+}
+
 }  // namespace arp

@@ -27,6 +27,10 @@ __host__ __device__ constexpr int kChunkRows() { return TB <= 4 ? 64 : 32; }
 
 __device__ __forceinline__ float nearest_level(float v, int M) {
   if (M == 4) return fabsf(v - 1.0f) < fabsf(v + 1.0f) ? 1.0f : -1.0f;  // ties -> the first level, -1
+  if (M == 64) {  // nearest odd level in [-7, 7], the lower one on ties
+    const float l = 2.0f * ceilf(0.5f * v) - 1.0f;
+    return fminf(fmaxf(l, -7.0f), 7.0f);
+  }
   float best = -3.0f, bd = fabsf(v + 3.0f);
 #pragma unroll
   for (int i = 1; i < 4; ++i) {
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   int* br = reinterpret_cast<int*>(bd + 8);  // 8
   int8_t* ek = reinterpret_cast<int8_t*>(br + 8);  // (R + 1) x D: candidate level minus guess; row R = x_q
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, W = kReadThreads / 32;
-  const int lo = a.M == 4 ? -1 : -3, hi = -lo;
+  const int lo = 1 - pam_size(a.M), hi = -lo;
   const int u = a.idx ? a.idx[b] : b;
   const float* Hb = a.H + (size_t)u * NR2 * D;
   for (int x = tid; x < NR2 * D; x += kReadThreads) {
@@ -551,15 +555,17 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
     }
     return;
   }
-  const int nb = a.M == 4 ? 1 : 2;
+  const int nb = pam_bits(a.M);
   for (int j = tid; j < D; j += kReadThreads) {
     const int v = xq8[j] + (gi < R ? ek[gi * D + j] : 0);
     a.levels[(size_t)b * D + j] = (int8_t)v;
     if (nb == 1) {
       a.bits[(size_t)b * D + j] = v > 0;
-    } else {
+    } else if (nb == 2) {
       a.bits[(size_t)b * D * 2 + 2 * j] = v > 0;
       a.bits[(size_t)b * D * 2 + 2 * j + 1] = (v == 1 || v == -1);
+    } else {
+      for (int k = 0; k < nb; ++k) a.bits[((size_t)b * D + j) * nb + k] = (int8_t)gray_bit(v, k, a.M);
     }
   }
   if (tid == 0) {
@@ -621,7 +627,7 @@ extern "C" int arp_detect_dd(const float* H, const float* y, const float* sigma2
                              size_t workspace_bytes, int8_t* bits, int8_t* levels, float* dist, int32_t* pick,
                              int32_t* status, void* stream) {
   if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || !(P == 2 || P == 4 || P == 6) || R < 1 || L < 1 ||
-      !(M == 4 || M == 16))
+      !(M == 4 || M == 16 || M == 64))
     return ARP_ERR_SHAPE;
   if ((policy != 0 && policy != 1) || (precision != 0 && precision != 1) || (start != 0 && start != 1))
     return ARP_ERR_ARG;
@@ -649,7 +655,7 @@ extern "C" int arp_detect_dd(const float* H, const float* y, const float* sigma2
 
 extern "C" int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M,
                           int quantize, void* G, void* h, int8_t* xq, float* scale, int32_t* status, void* stream) {
-  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 1024 || !(M == 4 || M == 16)) return ARP_ERR_SHAPE;
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 1024 || !(M == 4 || M == 16 || M == 64)) return ARP_ERR_SHAPE;
   if (B == 0) return ARP_OK;
   if (!H || !y || !sigma2 || !G || !h || !xq || !scale) return ARP_ERR_ARG;
   MapParams a{H, y, sigma2, B, NR2, D, M, quantize ? 4096.0f : 0.0f, G, h, xq, scale, status};
@@ -659,7 +665,7 @@ extern "C" int arp_map_dd(const float* H, const float* y, const float* sigma2, i
 extern "C" int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2,
                               int D, int P, int R, int M, int8_t* levels, int8_t* bits, float* dist, int32_t* pick,
                               void* stream) {
-  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || P < 1 || P > 6 || R < 0 || !(M == 4 || M == 16))
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 256 || P < 1 || P > 6 || R < 0 || !(M == 4 || M == 16 || M == 64))
     return ARP_ERR_SHAPE;
   if (B == 0) return ARP_OK;
   if (!H || !y || !xq || (R > 0 && !spins) || !levels || !bits || !dist) return ARP_ERR_ARG;

@@ -20,7 +20,8 @@ from . import _lib
 from .chordfx import QSCALE, geom
 
 PAM = {4: dict(levels=(-1, 1), a=1 / math.sqrt(2), bits=1),
-       16: dict(levels=(-3, -1, 1, 3), a=1 / math.sqrt(10), bits=2)}
+       16: dict(levels=(-3, -1, 1, 3), a=1 / math.sqrt(10), bits=2),
+       64: dict(levels=(-7, -5, -3, -1, 1, 3, 5, 7), a=1 / math.sqrt(42), bits=3)}
 # Budgets the reference runs: Arpeggio picks abl_far_<S>_<T0>_<T1>_<q>_<start>_<Ns> (run_a513.py:35-39,
 # data/results/a513_fixed) and Chord's MDI schedule MDICHORD (mdi_solvers.py:18: 128 steps per copy pair).
 ARPEGGIO_PICKS = {16: dict(sweeps=64, T0=0.1, T1=0.1, q=0.0, start='rand'),

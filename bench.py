@@ -241,6 +241,48 @@ def run_ours(args):
                         'readout, copy out); device time per replay' % (w['nt'], w['nr'], args.anneals),
                'frames': n, 'p50_us': us[n // 2], 'p99_us': us[min(n - 1, int(0.99 * n))], 'max_us': us[-1]}
 
+    # ---- BER of the last timed step per SNR point (the detection itself, and its MMSE guess for reference)
+    ber = None
+    if rank == 0:
+        bt = channel.levels_to_bits(data['l'], w['M'])
+        err = (det.bits != bt).float().mean(-1)
+        errq = (channel.levels_to_bits(det.xq.float(), w['M']) != bt).float().mean(-1)
+        ber = {'%d dB' % v: {'ber': float(err[snr == v].mean()), 'ber_mmse_guess': float(errq[snr == v].mean())}
+               for v in w['snrs']}
+
+    # ---- the other policy and the 64-user workload, same kernels (reported beside the headline)
+    extra = {}
+    if args.extras:
+        for name, kw, Bx, ntx, snrs in (
+                ('chord_x32', dict(policy='chord', sweeps=None, T0=0.3, T1=0.3, q=0.4, start='rand'), B, 32,
+                 w['snrs']),
+                ('arpeggio_x64', dict(policy='arpeggio', sweeps=64, T0=0.1, T1=0.1, q=0.0, start='bal'), 16384, 64,
+                 list(range(10, 25, 2)))):
+            sx = torch.tensor([snrs[i % len(snrs)] for i in range(Bx)], dtype=torch.float32)
+            dx = data if ntx == 32 else channel.draw_device(5678 + rank, sx, Bx, ntx, w['M'], dev=dev)
+            anx = args.anneals if ntx == 32 else 64
+            dtx = detector.Detector(Bx, ntx, ntx, w['M'], anneals=anx, K=1, precision='int', device=dev, **kw)
+            dtx.set_noise(N0=dx['N0'])
+            for i in range(2):
+                dtx.run(dx['H'], dx['y'], seed=i)
+            x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            x0.record(stream)
+            for i in range(3):
+                dtx.run(dx['H'], dx['y'], seed=10 + i)
+            x1.record(stream)
+            torch.cuda.synchronize()
+            dtx.check()
+            msx = x0.elapsed_time(x1) / 3
+            btx = channel.levels_to_bits(dx['l'], w['M'])
+            extra[name] = {'value': Bx / (msx / 1e3), 'unit': 'detections/s', 'ms_per_step': msx, 'uses': Bx,
+                           'users': ntx, 'anneals': anx, 'policy': kw['policy'],
+                           'budget': 'S=%s T0=%g T1=%g q=%g start=%s' % (kw['sweeps'] or '128 steps/copy pair',
+                                                                           kw['T0'], kw['T1'], kw['q'], kw['start']),
+                           'ber': float((dtx.bits != btx).float().mean()),
+                           'flips_per_anneal': float(dtx.st[..., 0].float().mean()),
+                           'tests_per_anneal': float(dtx.st[..., 1].float().mean())}
+            del dtx
+
     # ---- the reference's full chain: multi-stage MDI at its recorded x16 point (16 x 16, 20 dB, Ns 32,
     #      abl_far_64_0.1_0.1_0_rand_32; 267.9 detections/s recorded on a B200 with a 4-thread CPU wrapper)
     mdi_line = None
@@ -322,7 +364,9 @@ def run_ours(args):
                          'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if peaks else 'fallback'},
         'anneal_counters': {'flips': int(st[0]), 'tests': int(st[1]), 'anneals': B * R, 'philox_blocks': blocks},
         'latency': lat,
+        'ber': ber,
         'mdi_x16': mdi_line,
+        'extra': extra,
         'gpu_launches': 3 * K,
         'clocks': ck,
     }
@@ -375,6 +419,7 @@ def main():
     ap.add_argument('--chunks', type=int, default=8, help='pipelined pieces of the end-to-end step')
     ap.add_argument('--latency-frames', type=int, default=2000, help='single-frame replays for p50/p99 latency')
     ap.add_argument('--mdi-batch', type=int, default=16384, help='uses of the multi-stage (MDI) line; 0 skips it')
+    ap.add_argument('--no-extras', dest='extras', action='store_false', help='skip the Chord and 64-user lines')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.rank = int(os.environ.get('RANK', 0))

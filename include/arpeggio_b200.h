@@ -87,7 +87,8 @@ int arp_anneal_chord(const int16_t* J, const int32_t* h, const int32_t* h0, cons
 
 /* Gram / field formation with the MMSE guess, per channel use (one block each).  H (B, NR2, D) float32
  * real-lifted channels [[Re, -Im], [Im, Re]] scaled by the constellation factor, y (B, NR2), sigma2 (B)
- * the MMSE regulariser (N0/2)/E[l^2], M in {4, 16}.  Outputs: G (B, D, D) = H^T H / scale (symmetric, so
+ * the MMSE regulariser (N0/2)/E[l^2], M in {4, 16, 64} (64-QAM: levels -7..7, Gray-coded level index; no
+ * reference counterpart, the reference's table stops at 16-QAM).  Outputs: G (B, D, D) = H^T H / scale (symmetric, so
  * also its own transpose Gt), h (B, D) = 2 H^T (y - H x_q) / scale, x_q (B, D) int8 hard MMSE guess,
  * scale (B).  quantize != 0: G and h are int32 round(x * 4096) (the integer problem); else float32.
  * Replaces the host chain mimo.mmse / mimo._mu / quantize_levels (arpeggio/mimo/mimo.py:86-109, 176-182),
@@ -98,7 +99,7 @@ int arp_map_dd(const float* H, const float* y, const float* sigma2, int B, int N
 
 /* Readout: candidate levels clip(x_q + sum_p s_p) of each anneal's best spins (B, R, P*D), their distance
  * ||y - H x||^2, the first minimum over the R candidates and then the guess, Gray bits (MSB first per
- * dimension).  Outputs levels (B, D) int8, bits (B, D * log2(M)/2) int8, dist (B) float32, pick (B) int32
+ * dimension; M in {4, 16, 64}).  Outputs levels (B, D) int8, bits (B, D * log2(M)/2) int8, dist (B) float32, pick (B) int32
  * (index of the winner, R = the guess; may be NULL).  Replaces mimo.spins_to_levels_delta, mimo.dist,
  * mimo.select and mimo.levels_to_bits (arpeggio/mimo/mimo.py:185-190, 416-425, 45-51). */
 int arp_readout_dd(const float* H, const float* y, const int8_t* xq, const int8_t* spins, int B, int NR2, int D,

@@ -184,14 +184,20 @@ def chord_fx(J, h, h0, T, c, q, S, P, R, seed, inst0=0, mode='chains', nthreads=
 
 # ---------------------------------------------------------------- constellation (mimo.py:19-51)
 PAM = {4: dict(levels=[-1, 1], a=1 / math.sqrt(2), bits=1),
-       16: dict(levels=[-3, -1, 1, 3], a=1 / math.sqrt(10), bits=2)}
+       16: dict(levels=[-3, -1, 1, 3], a=1 / math.sqrt(10), bits=2),
+       64: dict(levels=[-7, -5, -3, -1, 1, 3, 5, 7], a=1 / math.sqrt(42), bits=3)}
 
 
 def levels_to_bits(l, M):
-    """mimo.levels_to_bits (mimo.py:45-51): per dimension MSB first."""
+    """mimo.levels_to_bits (mimo.py:45-51): per dimension MSB first (64-QAM, which the reference does not have:
+    the binary-reflected Gray code of the level index)."""
     l = np.asarray(l)
     if M == 4:
         return (l > 0).astype(np.int8)
+    if M == 64:
+        i = (l.astype(np.int64) + 7) // 2
+        g = i ^ (i >> 1)
+        return np.stack([(g >> (2 - k)) & 1 for k in range(3)], -1).reshape(*l.shape[:-1], -1).astype(np.int8)
     b1 = (l > 0).astype(np.int8)
     b2 = (np.abs(l) == 1).astype(np.int8)
     return np.stack([b1, b2], -1).reshape(*l.shape[:-1], -1)

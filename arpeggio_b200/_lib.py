@@ -36,6 +36,14 @@ SIGNATURES = {
     'arp_mdi_map': [_P, _P, _P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P],
     'arp_mdi_update': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P],
     'arp_mdi_select': [_P, _P, _I, _I, _I, _I, _P, _P, _P],
+    'arp_map_dd_soft': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
+    'arp_gemm_bf16': [_P, _I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P],
+    'arp_warm_features': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P],
+    'arp_warm_loss': [_P, _I, _P, _I, _I, _P, _I, _P, _P, _P],
+    'arp_colsum_bf16': [_P, _I, _I, _I, _P, _P],
+    'arp_adam': [_P, _P, _P, _P, _P, _I, _F, _F, _F, _F, _I, _F, _P],
+    'arp_warm_start': [_P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P],
+    'arp_anneal_first_accept_warm': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P],
     'arp_detect_dd_static': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U,
                              _I, _P, _P, _P, _P, _P, _P],
 }

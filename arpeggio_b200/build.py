@@ -19,7 +19,7 @@ def stale():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')]
+    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cuh', '.h'))]
     deps.append(os.path.join(HERE, '..', 'include', 'arpeggio_b200.h'))
     return any(os.path.getmtime(d) > t for d in deps)
 
@@ -30,13 +30,19 @@ def build(force=False, verbose=False):
     objs = []
     os.makedirs(os.path.join(HERE, '_build'), exist_ok=True)
     procs = []
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cuh', '.h'))]
+    headers.append(os.path.join(HERE, '..', 'include', 'arpeggio_b200.h'))
+    newest_header = max(os.path.getmtime(h) for h in headers)
     for src in sources():
         obj = os.path.join(HERE, '_build', os.path.basename(src)[:-3] + '.o')
+        objs.append(obj)
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
+                and os.path.getmtime(obj) > newest_header):
+            continue
         cmd = [NVCC] + [f for f in FLAGS if f != '-shared'] + ['-c', src, '-o', obj]
         if verbose:
             cmd += ['-Xptxas', '-v']
         procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))
-        objs.append(obj)
     for p, src in procs:
         out = p.communicate()[0].decode()
         if verbose or p.returncode:

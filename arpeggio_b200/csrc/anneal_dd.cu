@@ -338,12 +338,13 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
 #define ARP_ANNEAL_MINB 1
 #endif
 
-template <int NS, int P, bool CHORD, bool CACHE>
+template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false>
 __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
   constexpr int DP = NS * 32;
   extern __shared__ __align__(16) unsigned char smem[];
   int32_t* Gs = reinterpret_cast<int32_t*>(smem);
   __shared__ int s_bad;
+  __shared__ uint8_t s_perm[WARM ? 128 : 1];
   const int D = a.D, L = a.L, R = a.R;
   const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
@@ -352,12 +353,25 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
   const int32_t* hg = reinterpret_cast<const int32_t*>(a.h) + (size_t)b * D;
   const int32_t* Tg = reinterpret_cast<const int32_t*>(a.T);
   const int32_t* cg = reinterpret_cast<const int32_t*>(a.c);
+  if constexpr (WARM) {
+    // position j' of the scan holds coordinate perm[j']: G and h are gathered into that order
+    for (int x = threadIdx.x; x < D; x += blockDim.x) {
+      const uint8_t pv = a.perm[(size_t)b * D + x];
+      if (pv >= D) s_bad = 1;  // not an order of 0..D-1: reported as ARP_ERR_RANGE, never dereferenced
+      s_perm[x] = pv < D ? pv : 0;
+    }
+    __syncthreads();
+  }
   {
     const int32_t* Gg = reinterpret_cast<const int32_t*>(a.Gt) + (size_t)b * D * D;
     bool bad = false;
     for (int x = threadIdx.x; x < D * DP; x += blockDim.x) {
       const int j = x / DP, i = x - j * DP;
-      const int32_t v = i < D ? Gg[(size_t)j * D + i] : 0;
+      int32_t v;
+      if constexpr (WARM)
+        v = i < D ? Gg[(size_t)s_perm[j] * D + s_perm[i]] : 0;
+      else
+        v = i < D ? Gg[(size_t)j * D + i] : 0;
       bad |= (v > kMaxG || v < -kMaxG);
       Gs[x] = v;
     }
@@ -386,7 +400,22 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
   for (int r = bs + split * wid; r < R; r += split * W) {
     // ---- start state (arpeggio_fx.cu:48-57), packed per thread
     uint32_t sp = 0;
-    if (a.start == 0) {
+    if constexpr (WARM) {
+      // given spin sums: m = 0 takes the 'bal' pattern of the position's draw, m != 0 sets copies p < (m + P)/2
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        const int j = t * 32 + lane;
+        uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)j, c2 = (uint32_t)r, c3 = inst;
+        philox10(c0, c1, c2, c3, K);
+        int mv = j < D ? a.m0[(size_t)b * D + s_perm[j]] : 0;
+        mv = mv < -P ? -P : (mv > P ? P : mv);
+        const int pat = mv == 0 ? bal_pattern(P, (uint32_t)(((uint64_t)c0 * (uint64_t)bal_choose(P)) >> 32))
+                                : (1 << ((mv + P) >> 1)) - 1;
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+          if ((pat >> p) & 1) sp |= 1u << (p * NS + t);
+      }
+    } else if (a.start == 0) {
 #pragma unroll
       for (int p = 0; p < P; ++p)
 #pragma unroll
@@ -415,7 +444,10 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
 #pragma unroll
       for (int p = 0; p < P; ++p) m += ((sp >> (p * NS + t)) & 1u) ? 1 : -1;
       mloc[t] = j < D ? m : 0;
-      w[t] = j < D ? hg[j] : 0;
+      if constexpr (WARM)
+        w[t] = j < D ? hg[s_perm[j]] : 0;
+      else
+        w[t] = j < D ? hg[j] : 0;
     }
 #pragma unroll
     for (int tj = 0; tj < NS; ++tj) {
@@ -544,7 +576,7 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
 #pragma unroll
       for (int t = 0; t < NS; ++t) {
         const int j = t * 32 + lane;
-        if (j < D) os[p * D + j] = ((bsp >> (p * NS + t)) & 1u) ? 1 : -1;
+        if (j < D) os[p * D + (WARM ? (int)s_perm[j] : j)] = ((bsp >> (p * NS + t)) & 1u) ? 1 : -1;
       }
     if (lane == 0) {
       // first accept: ballots = passes + flips; Chord: ballots = passes + flips (one per commit + one per pass)
@@ -575,10 +607,10 @@ static int pick_warps(K kern, size_t smem, int R) {
   return best_w;
 }
 
-template <int NS, int P, bool CHORD, bool FLT>
+template <int NS, int P, bool CHORD, bool FLT, bool WARM = false>
 static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   constexpr bool CACHE = P * NS <= 8;
-  auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE>;
+  auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE, WARM>;
   const size_t smem = (size_t)a.D * NS * 32 * 4;
   static size_t attr_smem = 48 * 1024;
   if (smem > attr_smem) {
@@ -639,6 +671,23 @@ static int check_dd(const void* Gt, const void* h, const void* T, int L, int P, 
 
 int default_warps(int R) { return 0; }  // 0: chosen per kernel by occupancy (pick_warps)
 
+// Warm-started first accept (integer fields, P = 2).
+static cudaError_t launch_warm(const DDParams& a0, cudaStream_t st) {
+  DDParams a = a0;
+  const PhiloxKeys K = philox_keys(a.k0, a.k1);
+  for (int i = 0; i < 10; ++i) {
+    a.rk0[i] = K.k0[i];
+    a.rk1[i] = K.k1[i];
+  }
+  switch ((a.D + 31) / 32) {
+    case 1: return launch_ns_p<1, 2, false, false, true>(a, 0, st);
+    case 2: return launch_ns_p<2, 2, false, false, true>(a, 0, st);
+    case 3: return launch_ns_p<3, 2, false, false, true>(a, 0, st);
+    case 4: return launch_ns_p<4, 2, false, false, true>(a, 0, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t anneal_dispatch(int policy, bool flt, const DDParams& a0, int P, int warps, cudaStream_t st) {
   DDParams a = a0;
   const PhiloxKeys K = philox_keys(a.k0, a.k1);
@@ -686,4 +735,18 @@ extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, co
   DDParams a{Gt, h, T, c, L, 0, q, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
   cudaError_t e = anneal_dispatch(policy, true, a, P, default_warps(R), (cudaStream_t)stream);
   return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_anneal_first_accept_warm(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P,
+                                            int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                                            const int8_t* m0, const uint8_t* perm, int8_t* out_s, int64_t* out_de,
+                                            int64_t* out_st, int32_t* status, void* stream) {
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, 1, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  if (P != 2) return ARP_ERR_SHAPE;
+  if (!m0 || !perm) return ARP_ERR_ARG;
+  DDParams a{Gt, h, T, nullptr, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, 1, out_s, out_de, out_st, status};
+  a.m0 = m0;
+  a.perm = perm;
+  return launch_warm(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

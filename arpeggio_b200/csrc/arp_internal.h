@@ -24,6 +24,10 @@ struct DDParams {
   int32_t* status;
   uint32_t rk0[10], rk1[10];  // Philox round keys of (k0, k1), filled by anneal_dispatch
   int split;                  // blocks per problem (anneals r = s, s + split, ... in block s), set at launch
+  // warm start (first accept, integer fields): start spin sums m0 (B, D) and the flip-test order perm (B, D)
+  // (position j' of the scan tests coordinate perm[j']); null for the reference's starts and index order
+  const int8_t* m0 = nullptr;
+  const uint8_t* perm = nullptr;
 };
 
 struct MapParams {
@@ -49,6 +53,7 @@ struct MapParams {
   float* h0ri = nullptr;
   float* hri = nullptr;
   int8_t* sP = nullptr;
+  float* zs = nullptr;  // (B, D) MMSE soft estimate z / mu (bias-corrected), or null
 };
 
 struct ReadParams {

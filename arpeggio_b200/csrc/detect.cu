@@ -183,9 +183,11 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
 #pragma unroll
       for (int i = 0; i < TB; ++i) {
         const int gi = ty * TB + i;
-        const float lv = gi < D ? nearest_level(__fdiv_rn(zp[i], mp[i]), a.M) : 0.0f;
+        const float zu = gi < D ? __fdiv_rn(zp[i], mp[i]) : 0.0f;
+        const float lv = gi < D ? nearest_level(zu, a.M) : 0.0f;
         xv[gi] = lv;
         if (gi < D) a.xq[(size_t)b * D + gi] = (int8_t)lv;
+        if (a.zs && gi < D) a.zs[(size_t)b * D + gi] = zu;
         ck[gi] = gi < D ? nearest_level(zp[i], a.M) : 0.0f;  // RI map: spins of the unbiased z (mimo.py:148)
       }
     }
@@ -659,6 +661,17 @@ extern "C" int arp_map_dd(const float* H, const float* y, const float* sigma2, i
   if (B == 0) return ARP_OK;
   if (!H || !y || !sigma2 || !G || !h || !xq || !scale) return ARP_ERR_ARG;
   MapParams a{H, y, sigma2, B, NR2, D, M, quantize ? 4096.0f : 0.0f, G, h, xq, scale, status};
+  return map_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_map_dd_soft(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M,
+                               int quantize, void* G, void* h, int8_t* xq, float* scale, float* zs, int32_t* status,
+                               void* stream) {
+  if (B < 0 || D < 1 || D > 128 || NR2 < 1 || NR2 > 1024 || !(M == 4 || M == 16 || M == 64)) return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!H || !y || !sigma2 || !G || !h || !xq || !scale || !zs) return ARP_ERR_ARG;
+  MapParams a{H, y, sigma2, B, NR2, D, M, quantize ? 4096.0f : 0.0f, G, h, xq, scale, status};
+  a.zs = zs;
   return map_dispatch(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 

@@ -1,0 +1,583 @@
+// Learned warm start for first-accept annealing: a per-coordinate MLP (features -> 512 -> 512 -> P+1 logits,
+// BF16 weights and activations, FP32 accumulate) trained and run by this file's kernels.
+//
+//   k_gemm_bf16   C = A B^T on the 5th-generation tensor cores: a 128 x BN output tile per CTA accumulates in
+//                 TMEM (tcgen05.mma kind::f16, one issuing thread), operands staged by cp.async into the
+//                 canonical no-swizzle shared-memory layouts (K-major or MN-major per operand, so forward and
+//                 both backward products use the same kernel), a 4-slot ring whose slots are released by
+//                 tcgen05.commit on per-slot mbarriers; fused epilogues (bias + ReLU to bf16, bias to f32,
+//                 ReLU-mask to bf16, f32 store, f32 accumulate for split K) read TMEM with tcgen05.ld.
+//   k_warm_features  per-coordinate features of a mapped dDI problem (and training labels).
+//   k_warm_loss      softmax cross-entropy over the P+1 classes of the spin sum, its gradient in bf16.
+//   k_colsum_bf16    bias gradients.
+//   k_adam           Adam on FP32 master weights, writing the BF16 copies.
+//   k_warm_start     logits -> per-coordinate start (spin sum m_j), flip-test order, start energy, fallback.
+//
+// The reference has no learned component; nothing here has a reference counterpart.
+#include <cuda_bf16.h>
+
+#include "../../include/arpeggio_b200.h"
+#include "arp_common.cuh"
+#include "umma.cuh"
+
+namespace arp {
+
+using bf16 = __nv_bfloat16;
+
+struct GemmParams {
+  const bf16* A;
+  const bf16* B;
+  int lda, ldb;
+  int M, N, K;
+  int epi;
+  const float* bias;
+  const bf16* aux;
+  int ldaux;
+  void* C;
+  int ldc;
+  int kt_per;  // k tiles (of 64) per split
+  int32_t* status;
+};
+
+constexpr int kStages = 4;
+
+// Stages one operand tile (R rows along M or N, 64 along K) into the canonical layout; zero fill outside.
+template <bool MN, int R>
+__device__ __forceinline__ void load_tile(uint32_t sbase, const bf16* g, int ld, int mn0, int mnlim, int k0, int K,
+                                          int tid) {
+  constexpr int CH = R * 8;
+#pragma unroll
+  for (int c = tid; c < CH; c += 128) {
+    int mn, k;
+    uint32_t off;
+    const bf16* src;
+    if constexpr (!MN) {
+      const int row = c >> 3, kc = c & 7;
+      mn = mn0 + row;
+      k = k0 + kc * 8;
+      off = (uint32_t)((row >> 3) * 1024 + kc * 128 + (row & 7) * 16);
+      src = g + (size_t)mn * ld + k;
+    } else {
+      const int kr = c / (R / 8), mc = c - kr * (R / 8);
+      k = k0 + kr;
+      mn = mn0 + mc * 8;
+      off = (uint32_t)((kr >> 3) * (R * 16) + mc * 128 + (kr & 7) * 16);
+      src = g + (size_t)k * ld + mn;
+    }
+    const bool valid = mn < mnlim && k < K;
+    umma::cp16(sbase + off, valid ? (const void*)src : (const void*)g, valid);
+  }
+}
+
+enum { EPI_F32 = 0, EPI_F32_ACC = 1, EPI_BIAS_RELU_BF16 = 2, EPI_BIAS_F32 = 3, EPI_MASK_BF16 = 4 };
+
+template <int CW>
+__device__ __forceinline__ void epilogue(const GemmParams& p, int row, int n, const uint32_t (&v)[32]) {
+#pragma unroll
+  for (int g = 0; g < CW; g += 16) {
+    const int nn = n + g;
+    if (nn >= p.N) break;
+    float f[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) f[i] = __uint_as_float(v[g + i]);
+    if (p.epi == EPI_F32 || p.epi == EPI_BIAS_F32) {
+      if (p.epi == EPI_BIAS_F32)
+#pragma unroll
+        for (int i = 0; i < 16; ++i) f[i] += p.bias[nn + i];
+      float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.C) + (size_t)row * p.ldc + nn);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) o[i] = make_float4(f[4 * i], f[4 * i + 1], f[4 * i + 2], f[4 * i + 3]);
+    } else if (p.epi == EPI_F32_ACC) {
+      float* o = reinterpret_cast<float*>(p.C) + (size_t)row * p.ldc + nn;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) atomicAdd(o + i, f[i]);
+    } else {
+      if (p.epi == EPI_BIAS_RELU_BF16) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) f[i] = fmaxf(f[i] + p.bias[nn + i], 0.0f);
+      } else {  // EPI_MASK_BF16: ReLU backward through the stored activation
+        const uint4* ax = reinterpret_cast<const uint4*>(p.aux + (size_t)row * p.ldaux + nn);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const uint4 u = ax[q];
+          const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
+            if (!(__low2float(h2) > 0.0f)) f[8 * q + 2 * i] = 0.0f;
+            if (!(__high2float(h2) > 0.0f)) f[8 * q + 2 * i + 1] = 0.0f;
+          }
+        }
+      }
+      uint32_t pk[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+        pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
+      }
+      uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(p.C) + (size_t)row * p.ldc + nn);
+      o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    }
+  }
+}
+
+template <int BN, bool AMN, bool BMN>
+__global__ void __launch_bounds__(128) k_gemm_bf16(const GemmParams p) {
+  constexpr int S = kStages;
+  constexpr uint32_t ABYTES = 128 * 128, BBYTES = BN * 128, SBYTES = ABYTES + BBYTES;
+  constexpr uint32_t NCOL = BN < 32 ? 32 : BN;
+  constexpr int CW = BN < 32 ? BN : 32;
+  constexpr uint32_t IDESC = umma::idesc_bf16(BN, AMN, BMN);
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bars[S];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * 128, n0 = blockIdx.y * BN;
+  const int nkt = (p.K + 63) / 64;
+  const int kt0 = blockIdx.z * p.kt_per;
+  const int kt1 = min(nkt, kt0 + p.kt_per);
+  const int nk = kt1 - kt0;
+  if (nk <= 0) return;
+  const uint32_t sbase = umma::su32(smem);
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) umma::mbar_init(&bars[s], 1);
+    umma::fence_mbar_init();
+    s_abort = 0;
+  }
+  if (warp == 0) umma::tmem_alloc(&s_tmem, NCOL);
+  umma::tc_before_sync();
+  __syncthreads();
+  umma::tc_after_sync();
+  const uint32_t tmem = s_tmem;
+
+  auto load = [&](int t, int slot) {
+    const uint32_t sa = sbase + (uint32_t)slot * SBYTES;
+    const int k0 = (kt0 + t) * 64;
+    load_tile<AMN, 128>(sa, p.A, p.lda, m0, p.M, k0, p.K, tid);
+    load_tile<BMN, BN>(sa + ABYTES, p.B, p.ldb, n0, p.N, k0, p.K, tid);
+  };
+#pragma unroll
+  for (int i = 0; i < S - 2; ++i) {
+    if (i < nk) load(i, i);
+    umma::cp_commit();
+  }
+  bool ok = true;
+  for (int t = 0; t < nk; ++t) {
+    const int tl = t + S - 2;
+    if (tl < nk) {
+      // slot tl % S was last read by the MMAs of tile t - 2
+      if (t >= 2 && !umma::mbar_wait(&bars[(t - 2) % S], ((t - 2) / S) & 1)) s_abort = 1;
+      load(tl, tl % S);
+    }
+    umma::cp_commit();
+    umma::cp_wait<S - 2>();
+    umma::fence_async_smem();
+    __syncthreads();
+    if (s_abort) {
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      umma::tc_after_sync();
+      const int slot = t % S;
+      const uint32_t sa = sbase + (uint32_t)slot * SBYTES, sb = sa + ABYTES;
+      const int krem = p.K - (kt0 + t) * 64;
+      const int nmma = krem >= 64 ? 4 : (krem + 15) / 16;
+      for (int kk = 0; kk < nmma; ++kk) {
+        const uint64_t ad = AMN ? umma::sdesc(sa + kk * 2 * (128 * 16), 128 * 16, 128)
+                                : umma::sdesc(sa + kk * 256, 128, 1024);
+        const uint64_t bd = BMN ? umma::sdesc(sb + kk * 2 * (BN * 16), BN * 16, 128)
+                                : umma::sdesc(sb + kk * 256, 128, 1024);
+        umma::mma(tmem, ad, bd, IDESC, (t > 0 || kk > 0) ? 1u : 0u);
+      }
+      umma::commit(&bars[slot]);
+    }
+  }
+  if (ok && !umma::mbar_wait(&bars[(nk - 1) % S], ((nk - 1) / S) & 1)) s_abort = 1;
+  umma::cp_wait<0>();
+  __syncthreads();
+  umma::tc_after_sync();
+  if (!s_abort) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += CW) {
+      if (n0 + c >= p.N) break;
+      uint32_t v[32];
+      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+      if constexpr (CW == 32)
+        umma::tmem_ld32(ta, v);
+      else
+        umma::tmem_ld16(ta, v);
+      if (row < p.M) epilogue<CW>(p, row, n0 + c, v);
+    }
+  } else if (tid == 0) {
+    set_status(p.status, ARP_ERR_TIMEOUT);
+  }
+  umma::tc_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tmem, NCOL);
+}
+
+template <int BN, bool AMN, bool BMN>
+static cudaError_t launch_gemm(GemmParams p, cudaStream_t st) {
+  constexpr size_t smem = (size_t)kStages * (128 * 128 + BN * 128);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN, AMN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int gx = (p.M + 127) / 128, gy = (p.N + BN - 1) / BN, nkt = (p.K + 63) / 64;
+  int split = 1;
+  if (p.epi == EPI_F32_ACC) {
+    const int want = (2 * 148 + gx * gy - 1) / (gx * gy);
+    split = want < nkt ? want : nkt;
+    if (split < 1) split = 1;
+  }
+  p.kt_per = (nkt + split - 1) / split;
+  split = (nkt + p.kt_per - 1) / p.kt_per;
+  dim3 grid(gx, gy, split);
+  k_gemm_bf16<BN, AMN, BMN><<<grid, 128, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <int BN>
+static cudaError_t gemm_bn(const GemmParams& p, bool amn, bool bmn, cudaStream_t st) {
+  if (!amn && !bmn) return launch_gemm<BN, false, false>(p, st);
+  if (!amn && bmn) return launch_gemm<BN, false, true>(p, st);
+  if (amn && !bmn) return launch_gemm<BN, true, false>(p, st);
+  return launch_gemm<BN, true, true>(p, st);
+}
+
+// ------------------------------------------------------------------------------------------------ features
+constexpr int kFeat = 16;
+
+template <typename GT>
+__global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G, const GT* __restrict__ h,
+                                                       const int8_t* __restrict__ xq, const float* __restrict__ zs,
+                                                       const float* __restrict__ snr_db, int B, int D, int M, int P,
+                                                       bf16* __restrict__ X, const int8_t* __restrict__ levels,
+                                                       int8_t* __restrict__ labels) {
+  const int b = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (b >= B) return;
+  const GT* Gb = G + (size_t)b * D * D;
+  float dg[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
+  for (int i = 0; i < D; ++i) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int j = t * 32 + lane;
+      if (j < D) {
+        const float g = (float)Gb[(size_t)i * D + j];
+        if (i == j)
+          dg[t] = g;
+        else
+          ss[t] = fmaf(g, g, ss[t]);
+      }
+    }
+  }
+  float sdg = dg[0] + dg[1] + dg[2] + dg[3];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sdg += __shfl_xor_sync(0xffffffffu, sdg, o);
+  const float mdg = sdg / (float)D;
+  const int Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
+  const float snr = snr_db ? snr_db[b] * 0.05f : 0.0f;
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int j = t * 32 + lane;
+    if (j >= D) continue;
+    const size_t row = (size_t)b * D + j;
+    const int x = xq[row];
+    float f[kFeat];
+#pragma unroll
+    for (int i = 0; i < kFeat; ++i) f[i] = 0.0f;
+    const float hj = (float)h[row];
+    f[0] = dg[t] > 0.0f ? hj / (4.0f * dg[t]) : 0.0f;  // best single-coordinate move, in level steps
+    f[1] = mdg > 0.0f ? dg[t] / mdg : 0.0f;
+    f[2] = dg[t] > 0.0f ? sqrtf(ss[t]) / dg[t] : 0.0f;  // coupling of this coordinate to the others
+    f[3] = snr;
+    f[4] = (float)x / (float)Lmax;
+    f[5] = x == Lmax ? 1.0f : 0.0f;
+    f[6] = x == -Lmax ? 1.0f : 0.0f;
+    f[7] = zs ? fminf(fmaxf(0.5f * (zs[row] - (float)x), -4.0f), 4.0f) : 0.0f;  // MMSE soft residual
+    f[8] = 1.0f;
+    f[0] = fminf(fmaxf(f[0], -8.0f), 8.0f);
+    f[2] = fminf(f[2], 64.0f);
+    uint32_t pk[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+      pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
+    }
+    uint4* o = reinterpret_cast<uint4*>(X + row * kFeat);
+    o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    if (labels) {
+      int c = (levels[row] - x) / 2 + P / 2;
+      labels[row] = (int8_t)(c < 0 ? 0 : (c > P ? P : c));
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ loss
+__global__ void __launch_bounds__(256) k_warm_loss(const float* __restrict__ logits, int ldl,
+                                                   const int8_t* __restrict__ labels, int rows, int C,
+                                                   bf16* __restrict__ dl, int ldd, float* loss_sum, int* correct) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.0f;
+  int ok = 0;
+  if (row < rows) {
+    const float* z = logits + (size_t)row * ldl;
+    float zm = -INFINITY;
+    int am = 0;
+    for (int c = 0; c < C; ++c)
+      if (z[c] > zm) {
+        zm = z[c];
+        am = c;
+      }
+    float se = 0.0f;
+    for (int c = 0; c < C; ++c) se += __expf(z[c] - zm);
+    const int lab = labels[row];
+    if (lab >= 0) {
+      l = __logf(se) + zm - z[lab];
+      ok = am == lab;
+    }
+    bf16* g = dl + (size_t)row * ldd;
+    for (int c = 0; c < ldd; ++c) {
+      float v = 0.0f;
+      if (c < C && lab >= 0) v = __expf(z[c] - zm) / se - (c == lab ? 1.0f : 0.0f);
+      g[c] = __float2bfloat16_rn(v);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+    ok += __shfl_xor_sync(0xffffffffu, ok, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (loss_sum) atomicAdd(loss_sum, l);
+    if (correct) atomicAdd(correct, ok);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ bias grads
+__global__ void __launch_bounds__(256) k_colsum_bf16(const bf16* __restrict__ X, int rows, int cols, int ld,
+                                                     float* __restrict__ out) {
+  __shared__ float part[8][33];
+  const int c = blockIdx.x * 32 + (threadIdx.x & 31), ty = threadIdx.x >> 5;
+  float acc = 0.0f;
+  if (c < cols)
+    for (int r = blockIdx.y * 8 + ty; r < rows; r += gridDim.y * 8) acc += __bfloat162float(X[(size_t)r * ld + c]);
+  part[ty][threadIdx.x & 31] = acc;
+  __syncthreads();
+  if (ty == 0 && c < cols) {
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += part[i][threadIdx.x & 31];
+    atomicAdd(out + c, s);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ Adam
+__global__ void __launch_bounds__(256) k_adam(float* __restrict__ w, bf16* __restrict__ wb,
+                                              const float* __restrict__ g, float* __restrict__ m,
+                                              float* __restrict__ v, int n, float lr, float b1, float b2, float eps,
+                                              float bc1, float bc2, float gscale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i] * gscale;
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16_rn(wi);
+}
+
+// ------------------------------------------------------------------------------------------------ warm start
+// One warp per problem.  Class c of coordinate j means the spin sum m_j = 2c - P (the move away from the guess in
+// level units), clamped so the level stays in the constellation.  Flip-test order: coordinates by descending
+// 1 - p(m_j = 0), ties by index.  The start is kept only when its energy e0 = 2 (m^T G m - h^T m) (the dDI energy
+// change from the guess, in the units of the anneal's out_de) is no worse than the guess's (0); otherwise the
+// problem falls back to the plain MMSE start (m = 0) in index order.
+template <typename GT, typename ET>
+__global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ logits, int ldl,
+                                                    const GT* __restrict__ G, const GT* __restrict__ h,
+                                                    const int8_t* __restrict__ xq, int B, int D, int P, int M,
+                                                    int8_t* __restrict__ m0, uint8_t* __restrict__ perm,
+                                                    ET* __restrict__ e0, int32_t* __restrict__ kept) {
+  const int b = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (b >= B) return;
+  const int C = P + 1, Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
+  int mv[4];
+  float sc[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int j = t * 32 + lane;
+    mv[t] = 0;
+    sc[t] = -1.0f;
+    if (j >= D) continue;
+    const float* z = logits + ((size_t)b * D + j) * ldl;
+    float zm = z[0];
+    int am = 0;
+    for (int c = 1; c < C; ++c)
+      if (z[c] > zm) {
+        zm = z[c];
+        am = c;
+      }
+    float se = 0.0f;
+    for (int c = 0; c < C; ++c) se += __expf(z[c] - zm);
+    sc[t] = 1.0f - __expf(z[P / 2] - zm) / se;
+    int m = 2 * am - P;
+    const int x = xq[(size_t)b * D + j];
+    if (x + m > Lmax) m = Lmax - x;
+    if (x + m < -Lmax) m = -Lmax - x;
+    mv[t] = m;
+  }
+  // start energy m^T G m - h^T m
+  ET e = ET(0);
+  const GT* Gb = G + (size_t)b * D * D;
+  for (int i = 0; i < D; ++i) {
+    const int mi = __shfl_sync(0xffffffffu, mv[i >> 5], i & 31);
+    if (mi == 0) continue;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int j = t * 32 + lane;
+      if (j < D && mv[t] != 0) e += (ET)Gb[(size_t)i * D + j] * (ET)(mi * mv[t]);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int j = t * 32 + lane;
+    if (j < D) e -= (ET)h[(size_t)b * D + j] * (ET)mv[t];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  e = e + e;  // the anneal's energy units: a flip moves out_de by 4 s w_j + 8 G_jj = 2 x the change of this form
+  const bool keep = e <= ET(0);
+  // ranks by descending score
+  int rk[4] = {0, 0, 0, 0};
+  for (int i = 0; i < D; ++i) {
+    const float si = __shfl_sync(0xffffffffu, sc[i >> 5], i & 31);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int j = t * 32 + lane;
+      if (si > sc[t] || (si == sc[t] && i < j)) ++rk[t];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int j = t * 32 + lane;
+    if (j >= D) continue;
+    m0[(size_t)b * D + j] = (int8_t)(keep ? mv[t] : 0);
+    perm[(size_t)b * D + (keep ? rk[t] : j)] = (uint8_t)j;
+  }
+  if (lane == 0) {
+    if (e0) e0[b] = keep ? e : ET(0);
+    if (kept) kept[b] = keep ? 1 : 0;
+  }
+}
+
+}  // namespace arp
+
+using namespace arp;
+
+static bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+extern "C" int arp_gemm_bf16(const void* A, int a_mn_major, int lda, const void* B, int b_mn_major, int ldb, int M,
+                             int N, int K, int epilogue, const float* bias, const void* aux, int ld_aux, void* C,
+                             int ldc, int32_t* status, void* stream) {
+  if (M < 0 || N < 0 || K < 0) return ARP_ERR_SHAPE;
+  if (M == 0 || N == 0) return ARP_OK;
+  if (K == 0 || N % 16 || K % 16 || lda % 8 || ldb % 8 || ldc % 8) return ARP_ERR_SHAPE;
+  if (a_mn_major && M % 8) return ARP_ERR_SHAPE;
+  if (epilogue < EPI_F32 || epilogue > EPI_MASK_BF16) return ARP_ERR_ARG;
+  if (!A || !B || !C || !al16(A) || !al16(B) || !al16(C)) return ARP_ERR_ARG;
+  if ((epilogue == EPI_BIAS_RELU_BF16 || epilogue == EPI_BIAS_F32) && !bias) return ARP_ERR_ARG;
+  if (epilogue == EPI_MASK_BF16 && (!aux || !al16(aux) || ld_aux % 8)) return ARP_ERR_ARG;
+  GemmParams p{(const bf16*)A, (const bf16*)B, lda, ldb, M, N, K, epilogue, bias, (const bf16*)aux, ld_aux, C, ldc, 0,
+               status};
+  const bool amn = a_mn_major != 0, bmn = b_mn_major != 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (N <= 16)
+    e = gemm_bn<16>(p, amn, bmn, st);
+  else if (N <= 64)
+    e = gemm_bn<64>(p, amn, bmn, st);
+  else if (N <= 128)
+    e = gemm_bn<128>(p, amn, bmn, st);
+  else
+    e = gemm_bn<256>(p, amn, bmn, st);
+  return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_warm_features(const void* G, const void* h, const int8_t* xq, const float* zs, const float* snr_db,
+                                 int B, int D, int M, int P, int quantized, void* X, const int8_t* levels,
+                                 int8_t* labels, void* stream) {
+  if (B < 0 || D < 1 || D > 128 || !(M == 4 || M == 16 || M == 64) || P < 1 || P > 6) return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!G || !h || !xq || !X || !al16(X) || (labels && !levels)) return ARP_ERR_ARG;
+  const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (quantized)
+    k_warm_features<int32_t><<<nb, th, 0, st>>>((const int32_t*)G, (const int32_t*)h, xq, zs, snr_db, B, D, M, P,
+                                                (bf16*)X, levels, labels);
+  else
+    k_warm_features<float><<<nb, th, 0, st>>>((const float*)G, (const float*)h, xq, zs, snr_db, B, D, M, P, (bf16*)X,
+                                              levels, labels);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_warm_loss(const float* logits, int ldl, const int8_t* labels, int rows, int classes, void* dlogits,
+                             int ldd, float* loss_sum, int32_t* correct, void* stream) {
+  if (rows < 0 || classes < 2 || classes > ldl || classes > ldd || classes > 8) return ARP_ERR_SHAPE;
+  if (rows == 0) return ARP_OK;
+  if (!logits || !labels || !dlogits) return ARP_ERR_ARG;
+  k_warm_loss<<<(rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(logits, ldl, labels, rows, classes, (bf16*)dlogits,
+                                                                    ldd, loss_sum, correct);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_colsum_bf16(const void* X, int rows, int cols, int ld, float* out, void* stream) {
+  if (rows < 0 || cols < 0 || ld < cols) return ARP_ERR_SHAPE;
+  if (rows == 0 || cols == 0) return ARP_OK;
+  if (!X || !out) return ARP_ERR_ARG;
+  int gy = (rows + 8 * 64 - 1) / (8 * 64);
+  if (gy > 256) gy = 256;
+  dim3 grid((cols + 31) / 32, gy);
+  k_colsum_bf16<<<grid, 256, 0, (cudaStream_t)stream>>>((const bf16*)X, rows, cols, ld, out);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, float lr, float beta1,
+                        float beta2, float eps, int step, float grad_scale, void* stream) {
+  if (n < 0 || step < 1) return ARP_ERR_SHAPE;
+  if (n == 0) return ARP_OK;
+  if (!w || !grad || !m || !v) return ARP_ERR_ARG;
+  const float bc1 = 1.0f - powf(beta1, (float)step), bc2 = 1.0f - powf(beta2, (float)step);
+  k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(w, (bf16*)w_bf16, grad, m, v, n, lr, beta1, beta2, eps,
+                                                            bc1, bc2, grad_scale);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const void* h, const int8_t* xq, int B,
+                              int D, int P, int M, int quantized, int8_t* m0, uint8_t* perm, void* e0,
+                              int32_t* kept, void* stream) {
+  if (B < 0 || D < 1 || D > 128 || P < 1 || P > 6 || ldl < P + 1 || !(M == 4 || M == 16 || M == 64))
+    return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!logits || !G || !h || !xq || !m0 || !perm) return ARP_ERR_ARG;
+  const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (quantized)
+    k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
+                                                        P, M, m0, perm, (long long*)e0, kept);
+  else
+    k_warm_start<float, float><<<nb, th, 0, st>>>(logits, ldl, (const float*)G, (const float*)h, xq, B, D, P, M, m0,
+                                                  perm, (float*)e0, kept);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}

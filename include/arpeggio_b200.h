@@ -175,6 +175,65 @@ int arp_mdi_update(const float* H, const float* y, const int32_t* idx, int n, in
 int arp_mdi_select(const int8_t* cur, const float* dist, int B, int D, int G, int M, int8_t* levels, int8_t* bits,
                    void* stream);
 
+/* ---- Learned warm start for first-accept annealing.  No counterpart in the reference, which has no learned
+ * component: a per-coordinate MLP (16 features -> 512 -> 512 -> P+1 logits over the coordinate's spin sum
+ * m_j = 2c - P, BF16 weights and activations, FP32 accumulate) emits the start state and the flip-test order.
+ * bf16 arrays are passed as void* (2-byte IEEE bfloat16). */
+
+/* arp_map_dd plus zs (B, D) float: the bias-corrected MMSE soft estimate z / mu behind x_q (a feature of the
+ * warm start).  Same map as arp_map_dd (mimo.mmse, mimo._mu and mimo.ising_delta_at, arpeggio/mimo/mimo.py:98-109,
+ * 176-182, 506-523). */
+int arp_map_dd_soft(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M, int quantize,
+                    void* G, void* h, int8_t* xq, float* scale, float* zs, int32_t* status, void* stream);
+
+/* C (M, N) = A B^T on the tensor cores (tcgen05.mma kind::f16, bf16 operands, fp32 accumulate in TMEM).
+ * A is (M, K) row-major with row stride lda (a_mn_major = 0) or (K, M) row-major (a_mn_major = 1); B is (N, K)
+ * (b_mn_major = 0) or (K, N) (b_mn_major = 1).  N and K multiples of 16, leading dimensions multiples of 8
+ * elements, pointers 16-byte aligned.  epilogue: 0 C = acc (float), 1 C += acc (float; K is split over CTAs,
+ * the caller zeroes C first), 2 C = bf16(max(acc + bias, 0)), 3 C = acc + bias (float), 4 C = bf16(acc if
+ * aux > 0 else 0) with aux (M, N) bf16 of row stride ld_aux (the ReLU backward). */
+int arp_gemm_bf16(const void* A, int a_mn_major, int lda, const void* B, int b_mn_major, int ldb, int M, int N, int K,
+                  int epilogue, const float* bias, const void* aux, int ld_aux, void* C, int ldc, int32_t* status,
+                  void* stream);
+
+/* Per-coordinate features X (B*D, 16) bf16 of mapped dDI problems G (B, D, D), h (B, D) (int32 when quantized,
+ * else float), guesses xq (B, D), MMSE soft estimates zs (B, D) (may be NULL), snr_db (B) (may be NULL).  With
+ * levels (B, D) given, labels (B*D) int8 receive the class (levels - xq)/2 + P/2 of each coordinate. */
+int arp_warm_features(const void* G, const void* h, const int8_t* xq, const float* zs, const float* snr_db, int B,
+                      int D, int M, int P, int quantized, void* X, const int8_t* levels, int8_t* labels, void* stream);
+
+/* Softmax cross-entropy over the first `classes` logits of each row (row stride ldl), labels < 0 ignored:
+ * dlogits (rows, ldd) bf16 = softmax - onehot (zero beyond `classes`); loss_sum and correct (may be NULL) are
+ * incremented by the summed loss and the number of argmax hits. */
+int arp_warm_loss(const float* logits, int ldl, const int8_t* labels, int rows, int classes, void* dlogits, int ldd,
+                  float* loss_sum, int32_t* correct, void* stream);
+
+/* out (cols) += column sums of X (rows, cols) bf16 with row stride ld (bias gradients). */
+int arp_colsum_bf16(const void* X, int rows, int cols, int ld, float* out, void* stream);
+
+/* One Adam step on n FP32 master weights w with gradient grad * grad_scale, moments m and v, bias-corrected
+ * for step `step` (1-based); w_bf16 (may be NULL) receives the rounded weights. */
+int arp_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, float lr, float beta1, float beta2,
+             float eps, int step, float grad_scale, void* stream);
+
+/* Warm start from the logits (B*D, ldl): m0 (B, D) the start spin sum of each coordinate (argmax class, clamped
+ * to the constellation), perm (B, D) the flip-test order (position j' tests coordinate perm[j'], by descending
+ * 1 - p(m = 0)), e0 (B) the start's energy 2 (m^T G m - h^T m) relative to the guess, in the units of the
+ * anneal's out_de (int64 when quantized, else float; may be NULL),
+ * kept (B) 1 where the start is no worse than the guess (e0 <= 0); elsewhere m0 = 0 and perm is the index
+ * order, i.e. the plain MMSE start. */
+int arp_warm_start(const float* logits, int ldl, const void* G, const void* h, const int8_t* xq, int B, int D, int P,
+                   int M, int quantized, int8_t* m0, uint8_t* perm, void* e0, int32_t* kept, void* stream);
+
+/* arp_anneal_first_accept (P = 2) from a given start: coordinate perm[j'] is tested at scan position j' (its
+ * Philox counters are those of position j'), and starts with spin sum m0 (m = 0: the 'bal' pattern of
+ * position j''s draw; m = +-2: both copies +-1).  Outputs in coordinate order; out_de is relative to the start
+ * (add e0 for the change from the guess).  perm entries outside 0..D-1 give ARP_ERR_RANGE in status. */
+int arp_anneal_first_accept_warm(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P, int R,
+                                 int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1, const int8_t* m0,
+                                 const uint8_t* perm, int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status,
+                                 void* stream);
+
 /* arp_detect_dd without a workspace argument, for callers that cannot allocate device memory: a receive
  * chain with a hard per-frame latency budget cannot call cudaMalloc on the frame path (it synchronises the
  * device and takes unbounded time), and a plugin inside a host program that owns all device memory may not

@@ -126,12 +126,21 @@ typedef struct {
   int start, policy;
   int8_t* out_s;
   int64_t *out_de, *out_st;
+  const int8_t* m0; /* start == 2: given spin sums (B, D) */
 } dd_ctx;
 
 /* Start spins of one anneal (arpeggio_ref59.py:44-49, arpeggio_fx.cu:48-57). s is P x D. */
 static void start_spins(int start, int P, int D, uint32_t r, uint32_t inst, uint32_t k0, uint32_t k1,
-                        int8_t* s) {
-  if (start == 0) {
+                        const int8_t* m0, int8_t* s) {
+  if (start == 2) { /* given spin sums: m = 0 takes the 'bal' pattern, m != 0 sets copies p < (m + P) / 2 */
+    uint64_t C = (uint64_t)bal_count(P);
+    for (int j = 0; j < D; j++) {
+      uint32_t w0 = philox_word(0xFFFFFFFFu, (uint32_t)j, r, inst, k0, k1, 0);
+      int m = m0[j] < -P ? -P : (m0[j] > P ? P : m0[j]);
+      int pat = m == 0 ? bal_pat(P, (uint32_t)(((uint64_t)w0 * C) >> 32)) : (1 << ((m + P) / 2)) - 1;
+      for (int p = 0; p < P; p++) s[p * D + j] = ((pat >> p) & 1) ? 1 : -1;
+    }
+  } else if (start == 0) {
     for (int p = 0; p < P; p++)
       for (int j = 0; j < D; j++)
         s[p * D + j] = philox_word(0xFFFFFFFFu, (uint32_t)(p * D + j), r, inst, k0, k1, 0) >= 0x80000000u ? 1 : -1;
@@ -156,7 +165,7 @@ static void dd_job(void* vctx, long t) {
   uint8_t pf[6 * 128];
   int64_t w[128];
   uint8_t F[128];
-  start_spins(x->start, P, D, r, inst, x->k0, x->k1, s);
+  start_spins(x->start, P, D, r, inst, x->k0, x->k1, x->m0 ? x->m0 + (size_t)b * D : NULL, s);
   memcpy(bs, s, (size_t)P * D);
   memset(pf, 0, sizeof pf);
   for (int i = 0; i < D; i++) { /* w_i = h_i - 2 sum_j G_ij m_j (arpeggio_ref59.py:50-51) */
@@ -235,7 +244,18 @@ int orc_anneal_dd(const int32_t* G, const int32_t* h, int B, int D, int P, int R
                   int policy, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
     return 1;
-  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st};
+  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL};
+  orc_run(dd_job, &x, (long)B * R, nthreads);
+  return 0;
+}
+
+/* First accept from given spin sums m0 (B, D) (start 2 of start_spins); the caller permutes the problem into
+ * scan order first (the device's flip-test order is a relabelling of the coordinates). */
+int orc_anneal_dd_warm(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T, int L,
+                       int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1, const int8_t* m0, int8_t* out_s,
+                       int64_t* out_de, int64_t* out_st, int nthreads) {
+  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || L < 1 || R < 1 || B < 0 || !m0) return 1;
+  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }
@@ -364,7 +384,7 @@ static void f32_job(void* vctx, long t) {
   int8_t s[6 * 128], bs[6 * 128];
   uint8_t pf[6 * 128], F[128];
   float w[128];
-  start_spins(x->start, P, D, r, inst, x->k0, x->k1, s);
+  start_spins(x->start, P, D, r, inst, x->k0, x->k1, NULL, s);
   memcpy(bs, s, (size_t)P * D);
   memset(pf, 0, sizeof pf);
   for (int i = 0; i < D; i++) {

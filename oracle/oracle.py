@@ -337,3 +337,147 @@ def list_llr(H, y, N0, allc, d, best, M, clip=50.0):
     m1 = np.where(bits, d2[..., None], np.inf).min(1)
     m0 = np.where(~bits, d2[..., None], np.inf).min(1)
     return np.clip((m0 - m1) / N0, -clip, clip)
+
+
+# ---------------------------------------------------------------- learned warm start (no reference counterpart)
+# The reference has no learned component, so these restate this package's own warm-start definitions (feature
+# map, bf16 MLP, warm start, warm anneal) for the GPU parity tests; parity here is self-consistency, not a pin
+# to the reference.
+NF, NH, NO = 16, 512, 16
+
+
+def bf16(x):
+    """Round float32 to bfloat16 (nearest, ties to even), returned as float32."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    u = x.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return (r & 0xFFFFFFFF).astype(np.uint32).view(np.float32).reshape(x.shape)
+
+
+def warm_features(G, h, xq, zs, snr_db, M, P, levels=None):
+    """Per-coordinate features (B*D, 16) float32 before bf16 rounding, and labels (levels - xq)/2 + P/2."""
+    G = np.asarray(G, dtype=np.float64)
+    h = np.asarray(h, dtype=np.float64)
+    B, D, _ = G.shape
+    dg = np.diagonal(G, axis1=1, axis2=2)
+    off = G.copy()
+    off[:, np.arange(D), np.arange(D)] = 0
+    ss = (off ** 2).sum(1)
+    mdg = dg.mean(1, keepdims=True)
+    Lmax = {4: 1, 16: 3, 64: 7}[M]
+    x = np.asarray(xq, dtype=np.float64)
+    f = np.zeros((B, D, NF))
+    with np.errstate(divide='ignore', invalid='ignore'):
+        f[..., 0] = np.clip(np.where(dg > 0, h / (4 * dg), 0), -8, 8)
+        f[..., 1] = np.where(mdg > 0, dg / mdg, 0)
+        f[..., 2] = np.minimum(np.where(dg > 0, np.sqrt(ss) / dg, 0), 64)
+    f[..., 3] = 0 if snr_db is None else np.asarray(snr_db, dtype=np.float64)[:, None] * 0.05
+    f[..., 4] = x / Lmax
+    f[..., 5] = x == Lmax
+    f[..., 6] = x == -Lmax
+    f[..., 7] = 0 if zs is None else np.clip(0.5 * (np.asarray(zs, dtype=np.float64) - x), -4, 4)
+    f[..., 8] = 1
+    lab = None
+    if levels is not None:
+        lab = np.clip((np.asarray(levels, dtype=np.int64) - np.asarray(xq, dtype=np.int64)) // 2 + P // 2, 0, P)
+        lab = lab.reshape(-1).astype(np.int8)
+    return f.reshape(B * D, NF).astype(np.float32), lab
+
+
+def mlp_forward(X, W1, b1, W2, b2, W3t, b3):
+    """The warm-start MLP with the device's roundings: bf16 operands, fp32 accumulate, bf16 hidden activations."""
+    Xb = bf16(X)
+    H1 = bf16(np.maximum(Xb @ bf16(W1).T + b1, 0))
+    H2 = bf16(np.maximum(H1 @ bf16(W2).T + b2, 0))
+    Z = H2 @ bf16(W3t) + b3
+    return H1, H2, Z.astype(np.float32)
+
+
+def mlp_backward(X, labels, C, W1, W2, W3t, H1, H2, Z):
+    """Gradients of the summed softmax cross-entropy (over the first C logits) with the device's roundings
+    (bf16 logit gradients and masked hidden gradients).  Returns dict of sums over rows (unscaled)."""
+    lab = np.asarray(labels, dtype=np.int64)
+    z = Z[:, :C].astype(np.float64)
+    zm = z.max(1, keepdims=True)
+    e = np.exp(z - zm)
+    p = e / e.sum(1, keepdims=True)
+    valid = lab >= 0
+    g = np.zeros((Z.shape[0], NO))
+    g[:, :C] = p
+    g[np.arange(len(lab))[valid], lab[valid]] -= 1
+    g[~valid] = 0
+    loss = float((np.log(e.sum(1)) + zm[:, 0] - z[np.arange(len(lab)), np.maximum(lab, 0)])[valid].sum())
+    dZ3 = bf16(g.astype(np.float32))
+    gW3t = H2.T.astype(np.float64) @ dZ3
+    gb3 = dZ3.sum(0)
+    dZ2 = bf16(np.where(H2 > 0, dZ3 @ bf16(W3t).T, 0).astype(np.float32))
+    gW2 = dZ2.T.astype(np.float64) @ H1
+    gb2 = dZ2.sum(0)
+    dZ1 = bf16(np.where(H1 > 0, dZ2 @ bf16(W2), 0).astype(np.float32))
+    gW1 = dZ1.T.astype(np.float64) @ bf16(X)
+    gb1 = dZ1.sum(0)
+    return dict(W1=gW1, b1=gb1, W2=gW2, b2=gb2, W3t=gW3t, b3=gb3, loss=loss, dZ3=dZ3, dZ2=dZ2, dZ1=dZ1)
+
+
+def warm_start(logits, G, h, xq, P, M):
+    """Start spin sums m0 (B, D), flip-test order perm (B, D), start energy e0 (B) and kept (B): argmax class
+    c -> m = 2c - P clamped to the constellation; order by descending 1 - p(m = 0) (ties by index); the start
+    is kept iff e0 = 2 (m^T G m - h^T m) <= 0 (the anneal's energy units), else m = 0 in index order."""
+    G = np.asarray(G)
+    B, D, _ = G.shape
+    C = P + 1
+    Lmax = {4: 1, 16: 3, 64: 7}[M]
+    z = np.asarray(logits, dtype=np.float32).reshape(B, D, -1)[..., :C].astype(np.float64)
+    am = z.argmax(-1)
+    e = np.exp(z - z.max(-1, keepdims=True))
+    pz = e[..., P // 2] / e.sum(-1)
+    sc = (1 - pz).astype(np.float32)
+    x = np.asarray(xq, dtype=np.int64)
+    m = 2 * am - P
+    m = np.where(x + m > Lmax, Lmax - x, m)
+    m = np.where(x + m < -Lmax, -Lmax - x, m)
+    integer = np.issubdtype(G.dtype, np.integer)
+    Gd = G.astype(np.int64) if integer else G.astype(np.float64)
+    hd = np.asarray(h).astype(np.int64) if integer else np.asarray(h, dtype=np.float64)
+    e0 = 2 * (np.einsum('bi,bij,bj->b', m, Gd, m) - (hd * m).sum(1))
+    keep = e0 <= 0
+    perm = np.zeros((B, D), dtype=np.uint8)
+    m0 = np.where(keep[:, None], m, 0).astype(np.int8)
+    for b in range(B):
+        if keep[b]:
+            order = sorted(range(D), key=lambda j: (-float(sc[b, j]), j))
+            perm[b] = order
+        else:
+            perm[b] = np.arange(D)
+    return m0, perm, np.where(keep, e0, 0), keep.astype(np.int32)
+
+
+def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1):
+    """First accept from the given start in the given flip-test order: the problem relabelled into scan order
+    (position j' = coordinate perm[j']), annealed from spin sums m0 with the 'bal' pattern where m0 = 0, and the
+    spins relabelled back."""
+    G = np.asarray(G, dtype=np.int32)
+    h = np.asarray(h, dtype=np.int32)
+    B, D, _ = G.shape
+    pm = np.asarray(perm, dtype=np.int64)
+    bi = np.arange(B)[:, None]
+    Gp = np.ascontiguousarray(G[bi[:, :, None], pm[:, :, None], pm[:, None, :]], dtype=np.int32)
+    hp = np.ascontiguousarray(h[bi, pm], dtype=np.int32)
+    mp = np.ascontiguousarray(np.asarray(m0, dtype=np.int8)[bi, pm], dtype=np.int8)
+    T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    out_s = np.zeros((B, R, P * D), dtype=np.int8)
+    out_de = np.zeros((B, R), dtype=np.int64)
+    out_st = np.zeros((B, R, 2), dtype=np.int64)
+    L = lib()
+    L.orc_anneal_dd_warm.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int,
+                                     ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_int]
+    rc = L.orc_anneal_dd_warm(_ptr(Gp), _ptr(hp), B, D, P, R, _ptr(T), len(T), int(q), _ptr(it), key & MASK,
+                              (key >> 32) & MASK, _ptr(mp), _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_dd_warm: unsupported shape')
+    s = out_s.reshape(B, R, P, D)
+    back = np.empty_like(s)
+    back[np.arange(B)[:, None, None, None], np.arange(R)[None, :, None, None], np.arange(P)[None, None, :, None],
+         pm[:, None, None, :]] = s
+    return back.reshape(B, R, P * D), out_de, out_st

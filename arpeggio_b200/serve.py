@@ -1,0 +1,169 @@
+"""Serving: continuous batching of per-frame detection requests of mixed sizes.
+
+A frame is one channel use of some size class (users, antennas, constellation).  Each class has an arrival
+stream in pinned host memory: H (n, 2 nr, 2 nt), y (n, 2 nr), N0 (n), arrival times (n, seconds, ascending)
+and request ids.  The server keeps, per class, `inflight` lanes -- a preallocated detector of `slots` uses
+(channel state stays on the device), its own CUDA stream and staging buffers -- and runs this loop:
+
+  * admission: a free lane takes every request of its class that has arrived and is not yet taken, up to its
+    slot count (slots are fixed by the HBM budget at construction; a class is accepted only if its kernels'
+    shared memory fits), copies their H, y and noise in, detects, copies bits and distances out and records
+    an event -- all on the lane's stream, so batches of one class and of different classes overlap on the GPU;
+  * completion: a lane whose event has completed hands its results to the requests' rows of the class's
+    output arrays and becomes free; each request's latency is completion time minus arrival time.
+
+A request's result does not depend on what it is batched with: every problem anneals with the server's Philox
+key and the request id as its instance number (the kernels' per-problem counters), and every stage works per
+problem.  Requests that arrive while others are on the GPU are taken by the next free lane."""
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .detector import PAM, el2
+from .warm import NF, NH, NO, WarmDetector
+
+
+class _Lane:
+    def __init__(self, cls, slots, anneals, sweeps, mlp, device):
+        nt, nr, M = cls
+        self.det = WarmDetector(slots, nt, nr, M, anneals=anneals, sweeps=sweeps, mlp=mlp, device=device)
+        self.stream = torch.cuda.Stream(device=device)
+        self.Hd = torch.empty(slots, 2 * nr, 2 * nt, dtype=torch.float32, device=device)
+        self.yd = torch.empty(slots, 2 * nr, dtype=torch.float32, device=device)
+        self.instd = torch.empty(slots, dtype=torch.int32, device=device)
+        self.done = torch.cuda.Event()
+        self.busy = None  # (first, last) rows of the class stream in flight
+
+
+def shared_bytes(cls, anneals):
+    """The largest per-block shared memory of the class's kernels: the anneal's G (D rows padded to 32-lane
+    slots, int32) and the readout's transposed H, residual and candidates."""
+    nt, nr, M = cls
+    D, NR2 = 2 * nt, 2 * nr
+    anneal = D * 32 * (-(-D // 32)) * 4
+    readout = 4 * (D * (NR2 + 1) + NR2 + 8) + 32 + (anneals + 1) * D + 16
+    return max(anneal, readout)
+
+
+def lane_bytes(cls, slots, anneals, warm):
+    """Device bytes of one lane: detector workspace and buffers, MLP activations, staging."""
+    nt, nr, M = cls
+    D, NR2, P = 2 * nt, 2 * nr, 2
+    offs = (__import__('ctypes').c_size_t * 7)()
+    ws = _lib.lib().arp_detect_dd_workspace(slots, D, P, anneals, 0, offs)
+    nb = D * PAM[M]['bits']
+    per = D * (4 + NF * 2 + 2) + 8 + 4 + 4 + D + nb + 4 + 4 + 4 * (NR2 * D + NR2) + 12
+    if warm:
+        per += D * (2 * NH * 2 + NO * 4)
+    return ws + slots * per
+
+
+class Server:
+    """Continuous-batching detection server over size classes (nt, nr, M)."""
+
+    def __init__(self, classes, mlp=None, anneals=32, sweeps=None, slots=4096, inflight=2, hbm_budget=8 << 30,
+                 seed=0x5EED, device='cuda'):
+        self.device = torch.device(device)
+        self.key = seed & 0xFFFFFFFFFFFFFFFF
+        self.classes = [tuple(c) for c in classes]
+        self.lanes, self.slots = {}, {}
+        share = hbm_budget // max(1, len(self.classes))
+        for cls in self.classes:
+            nt, nr, M = cls
+            if 2 * nt > 128 or M not in PAM:
+                raise ValueError('size class %s: the anneal keeps at most 128 coordinates in shared memory' % (cls,))
+            if shared_bytes(cls, anneals) > 227 * 1024:
+                raise ValueError('size class %s: shared memory beyond 227 KB per block' % (cls,))
+            cap = slots
+            while cap > 1 and inflight * lane_bytes(cls, cap, anneals, mlp is not None) > share:
+                cap //= 2
+            self.slots[cls] = cap
+            self.lanes[cls] = [_Lane(cls, cap, anneals, sweeps, mlp, self.device) for _ in range(inflight)]
+        self.streams = {}
+
+    def open(self, cls, H, y, N0, t_arrival, rid):
+        """Registers the arrival stream of a class (pinned host tensors; t_arrival ascending, seconds) and output
+        buffers for it (bits (n, D log2(M)/2) int8, dist (n), done (n) completion times)."""
+        cls = tuple(cls)
+        nt, nr, M = cls
+        n = H.shape[0]
+        N0 = torch.as_tensor(N0, dtype=torch.float64).reshape(-1).expand(n)
+        st = {'H': H, 'y': y, 't': np.asarray(t_arrival, dtype=np.float64), 'rid': rid,
+              's2': ((N0 / 2) / el2(M)).float().contiguous().pin_memory(),
+              'snr': (10 * torch.log10(nt / N0)).float().contiguous().pin_memory(),
+              'rid_t': torch.as_tensor(np.asarray(rid, dtype=np.int64) & 0xFFFFFFFF).to(torch.int32).pin_memory(),
+              'bits': torch.empty(n, 2 * nt * PAM[M]['bits'], dtype=torch.int8).pin_memory(),
+              'dist': torch.empty(n, dtype=torch.float32).pin_memory(),
+              'done': np.full(n, np.nan), 'next': 0, 'batches': 0}
+        self.streams[cls] = st
+        return st
+
+    def _launch(self, cls, lane, a, b):
+        st, det, k = self.streams[cls], lane.det, b - a
+        with torch.cuda.stream(lane.stream):
+            lane.Hd[:k].copy_(st['H'][a:b], non_blocking=True)
+            lane.yd[:k].copy_(st['y'][a:b], non_blocking=True)
+            lane.instd[:k].copy_(st['rid_t'][a:b], non_blocking=True)
+            det.sigma2[:k].copy_(st['s2'][a:b], non_blocking=True)
+            det.snr_db[:k].copy_(st['snr'][a:b], non_blocking=True)
+        bits, _, dist = det.run(lane.Hd[:k], lane.yd[:k], self.key, n=k, stream=lane.stream, inst=lane.instd[:k])
+        with torch.cuda.stream(lane.stream):
+            st['bits'][a:b].copy_(bits, non_blocking=True)
+            st['dist'][a:b].copy_(dist, non_blocking=True)
+        lane.done.record(lane.stream)
+        lane.busy = (a, b)
+        st['batches'] += 1
+
+    def step(self, now):
+        """One pass of the loop at time `now` (seconds on the arrival clock): completions, then admissions.
+        Returns the number of requests still pending or in flight."""
+        left = 0
+        for cls, lanes in self.lanes.items():
+            st = self.streams.get(cls)
+            if st is None:
+                continue
+            for lane in lanes:
+                if lane.busy is not None and lane.done.query():
+                    a, b = lane.busy
+                    st['done'][a:b] = now
+                    lane.busy = None
+            arrived = int(np.searchsorted(st['t'], now, side='right'))
+            for lane in lanes:
+                if lane.busy is None and st['next'] < arrived:
+                    a = st['next']
+                    b = min(arrived, a + self.slots[cls])
+                    self._launch(cls, lane, a, b)
+                    st['next'] = b
+            left += (len(st['t']) - st['next']) + sum(1 for ln in lanes if ln.busy is not None)
+        return left
+
+    def serve(self, clock=None, timeout=120.0):
+        """Runs the loop until every registered request is done.  clock(): seconds on the arrival clock
+        (default: wall time since the call).  Returns per-class latency statistics."""
+        t0 = time.perf_counter()
+        clock = clock or (lambda: time.perf_counter() - t0)
+        while True:
+            now = clock()
+            if self.step(now) == 0:
+                break
+            if time.perf_counter() - t0 > timeout:
+                raise TimeoutError('serving loop did not drain within %.0f s' % timeout)
+        for lanes in self.lanes.values():
+            for lane in lanes:
+                lane.stream.synchronize()
+                lane.det.check()
+        out = {}
+        for cls, st in self.streams.items():
+            lat = (st['done'] - st['t']) * 1e6
+            out['%dx%d %d-QAM' % (cls[0], cls[1], cls[2])] = {
+                'requests': int(len(lat)), 'batches': st['batches'], 'slots': self.slots[cls],
+                'p50_us': float(np.percentile(lat, 50)), 'p99_us': float(np.percentile(lat, 99)),
+                'max_us': float(lat.max())}
+        return out
+
+
+def poisson_arrivals(n, rate, rng):
+    """n arrival times (s) of a Poisson process of `rate` frames/s."""
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))

@@ -86,17 +86,30 @@ class WarmMLP:
             self._train = True
         self._rows = rows
 
-    def forward(self, X, rows, stream=None):
-        """logits (rows, 16) float32 of features X (rows, 16) bf16; stream-ordered, allocation-free after reserve."""
-        self.reserve(rows)
+    def scratch(self, rows):
+        """Activation buffers for inference on up to `rows` rows, owned by the caller (one per concurrent stream)."""
+        rows = -(-rows // 128) * 128
+        dev, b16 = self.device, torch.bfloat16
+        return {'H1': torch.empty(rows, NH, dtype=b16, device=dev), 'H2': torch.empty(rows, NH, dtype=b16, device=dev),
+                'Z': torch.empty(rows, NO, dtype=torch.float32, device=dev)}
+
+    def forward(self, X, rows, stream=None, scratch=None):
+        """logits (rows, 16) float32 of features X (rows, 16) bf16; stream-ordered and allocation-free, in the
+        network's own buffers (after reserve) or in `scratch` (from self.scratch)."""
+        if scratch is None:
+            self.reserve(rows)
+            scratch = {'H1': self.H1, 'H2': self.H2, 'Z': self.Z}
+        H1, H2, Z = scratch['H1'], scratch['H2'], scratch['Z']
+        if H1.shape[0] < rows:
+            raise ValueError('scratch holds %d rows, %d requested' % (H1.shape[0], rows))
         wb, st = self.wb, self.status
-        gemm(X, 0, NF, self.view(wb, 'W1'), 0, NF, rows, NH, NF, EPI_RELU_BF16, self.H1, NH,
+        gemm(X, 0, NF, self.view(wb, 'W1'), 0, NF, rows, NH, NF, EPI_RELU_BF16, H1, NH,
              bias=self.view(self.w, 'b1'), status=st, stream=stream)
-        gemm(self.H1, 0, NH, self.view(wb, 'W2'), 0, NH, rows, NH, NH, EPI_RELU_BF16, self.H2, NH,
+        gemm(H1, 0, NH, self.view(wb, 'W2'), 0, NH, rows, NH, NH, EPI_RELU_BF16, H2, NH,
              bias=self.view(self.w, 'b2'), status=st, stream=stream)
-        gemm(self.H2, 0, NH, self.view(wb, 'W3t'), 1, NO, rows, NO, NH, EPI_BIAS_F32, self.Z, NO,
+        gemm(H2, 0, NH, self.view(wb, 'W3t'), 1, NO, rows, NO, NH, EPI_BIAS_F32, Z, NO,
              bias=self.view(self.w, 'b3'), status=st, stream=stream)
-        return self.Z[:rows]
+        return Z[:rows]
 
     def backward(self, X, labels, rows, stream=None):
         """Summed softmax cross-entropy over the rows' labels (< 0: ignored) and its gradients into self.grad
@@ -171,8 +184,7 @@ class WarmDetector(Detector):
         self.e0 = torch.zeros(B, dtype=torch.int64, device=dev)
         self.kept = torch.zeros(B, dtype=torch.int32, device=dev)
         self.snr_db = torch.zeros(B, dtype=torch.float32, device=dev)
-        if mlp is not None:
-            mlp.reserve(B * D)
+        self.mlp_scratch = mlp.scratch(B * D) if mlp is not None else None
 
     def set_noise(self, snr_db=None, N0=None, n=None):
         super().set_noise(snr_db, N0, n)
@@ -183,18 +195,23 @@ class WarmDetector(Detector):
             s = 10 * torch.log10(self.nt / torch.as_tensor(N0, dtype=torch.float64).reshape(-1))
         self.snr_db[:n].copy_(s.float().expand(n) if s.numel() == 1 else s.float(), non_blocking=True)
 
-    def run(self, H, y, seed, n=None, inst0=0, stream=None, events=None, off=0, warm=True):
-        """Stream-ordered detection of uses off .. off+n-1 (instance numbers inst0 + off + i): map with the MMSE
-        soft estimate, then (warm and an MLP present) features -> MLP -> warm start -> warm anneal, else the plain
-        MMSE-started anneal, then the readout.  events: 4 CUDA events (before map, anneal, readout, after) or 5
-        (before map, warm start, anneal, readout, after).  Returns views (bits, levels, dist)."""
+    def run(self, H, y, seed, n=None, inst0=0, stream=None, events=None, off=0, warm=True, inst=None):
+        """Stream-ordered detection of uses off .. off+n-1 (instance numbers inst0 + off + i, or the device int32
+        tensor `inst` (n,)): map with the MMSE soft estimate, then (warm and an MLP present) features -> MLP ->
+        warm start -> warm anneal, else the plain MMSE-started anneal, then the readout.  events: 4 CUDA events
+        (before map, anneal, readout, after) or 5 (before map, warm start, anneal, readout, after).  Returns
+        views (bits, levels, dist)."""
         n = self.B - off if n is None else n
         if off < 0 or n < 0 or off + n > self.B:
             raise ValueError('slots %d..%d outside the detector batch %d' % (off, off + n, self.B))
         ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
         e5 = events is not None and len(events) == 5
         key = (inst0, off, n)
-        if self._inst_base != key:
+        if inst is not None:
+            with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+                self.inst[off:off + n].copy_(inst[:n], non_blocking=True)
+            self._inst_base = None
+        elif self._inst_base != key:
             iv = (np.arange(inst0 + off, inst0 + off + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
             self.inst[off:off + n].copy_(torch.from_numpy(iv))
             self._inst_base = key
@@ -218,7 +235,7 @@ class WarmDetector(Detector):
             _lib.check(L.arp_warm_features(_lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), _lib.ptr(zs),
                                            _lib.ptr(self.snr_db[sl]), n, D, self.M, P, 1, _lib.ptr(X), None, None, sp),
                        'warm_features')
-            Z = self.mlp.forward(X, n * D, stream)
+            Z = self.mlp.forward(X, n * D, stream, scratch=self.mlp_scratch)
             _lib.check(L.arp_warm_start(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P, self.M, 1,
                                         _lib.ptr(self.m0[sl]), _lib.ptr(self.perm[sl]), _lib.ptr(self.e0[sl]),
                                         _lib.ptr(self.kept[sl]), sp), 'warm_start')

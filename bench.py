@@ -141,6 +141,142 @@ def job_throughput(uses_per_rank, world, ms_max):
     return world * uses_per_rank / (ms_max / 1e3)
 
 
+# ---------------------------------------------------------------- learned warm start vs plain
+def frame_latency(det, f, stream, n):
+    """Device time per replay of a captured one-frame graph (pinned H, y in; bits, distance out)."""
+    import torch
+    Hh1, yh1 = f['H'].cpu().pin_memory(), f['y'].cpu().pin_memory()
+    bo1 = torch.empty(det.bits.shape, dtype=torch.int8).pin_memory()
+    do1 = torch.empty(1, dtype=torch.float32).pin_memory()
+    g = det.capture(Hh1, yh1, 5, bo1, do1, torch.empty_like(f['H']), torch.empty_like(f['y']))
+    for _ in range(50):
+        g.replay()
+    torch.cuda.synchronize()
+    le = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    for i in range(n):
+        le[i][0].record(stream)
+        g.replay()
+        le[i][1].record(stream)
+    torch.cuda.synchronize()
+    det.check()
+    us = sorted(1e3 * a_.elapsed_time(b_) for a_, b_ in le)
+    return {'frames': n, 'p50_us': us[n // 2], 'p99_us': us[min(n - 1, int(0.99 * n))], 'max_us': us[-1]}
+
+
+def warm_vs_plain(args, dev, stream, rank):
+    """Trains the warm-start MLP on the GPU (plain MMSE-started Arpeggio at the full budget labels seeded 32-user
+    16-QAM instances, SNR uniform 8-20 dB), then detects fresh 32-user and 64-user batches with the plain
+    MMSE-started annealer at the full budget and with the warm start at 1/2 and 3/4 of the sweeps: detections/s,
+    stage times, BER per SNR point and the paired BER ratio warm/plain with its bootstrap interval
+    (arpeggio_b200.stats.boot_ratio), final energies, and the one-frame latency of each at 32 users."""
+    import torch
+    from arpeggio_b200 import channel, stats, warm
+    mlp = warm.WarmMLP(P=2, seed=0)
+    t0 = time.time()
+    hist = warm.train(mlp, nt=32, instances=args.warm_train, batch=16384, anneals=32, sweeps=32,
+                      rows_per_step=65536, lr=2e-3, lr_end=1e-4, seed=11 + rank, device=dev)
+    torch.cuda.synchronize()
+    out = {'training': {'instances': args.warm_train, 'seconds': time.time() - t0, 'final_loss': hist[-1][1],
+                        'final_accuracy': hist[-1][2], 'labels': 'plain MMSE-started Arpeggio, 32 anneals x 32 sweeps',
+                        'optimizer': 'Adam, lr 2e-3 -> 1e-4, 65536 rows per step'},
+           'plain': 'MMSE-started (bal) Arpeggio first accept, fixed point, full sweep budget',
+           'warm': 'MLP warm start (kept only where its energy is no worse than the MMSE guess), learned flip-test '
+                   'order, same kernel and anneals, reduced sweeps'}
+    for nt, B, snrs, full, R in ((32, args.batch, list(range(6, 23, 2)), 32, 32),
+                                 (64, max(1024, args.batch // 4), list(range(10, 25, 2)), 64, 64)):
+        snr = torch.tensor([float(snrs[i % len(snrs)]) for i in range(B)])
+        d = channel.draw_device(9000 + nt + rank, snr, B, nt, 16, dev=dev)
+        bt = channel.levels_to_bits(d['l'], 16)
+        res = {}
+        base_err = None
+        for name, net, S in (('plain_full', None, full), ('warm_half', mlp, full // 2),
+                             ('warm_three_quarter', mlp, 3 * full // 4)):
+            det = warm.WarmDetector(B, nt, anneals=R, sweeps=S, mlp=net, device=dev)
+            det.set_noise(N0=d['N0'])
+            for i in range(2):
+                det.run(d['H'], d['y'], seed=20 + i)
+            torch.cuda.synchronize()
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(3)]
+            x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            x0.record(stream)
+            for i in range(3):
+                det.run(d['H'], d['y'], seed=30 + i, events=ev[i])
+            x1.record(stream)
+            torch.cuda.synchronize()
+            det.check()
+            ms = x0.elapsed_time(x1) / 3
+            st = [sum(ev[i][s].elapsed_time(ev[i][s + 1]) for i in range(3)) / 3 for s in range(4)]
+            err = (det.bits != bt).sum(-1).cpu().numpy()
+            sn = snr.numpy()
+            nb = bt.shape[1]
+            r = {'sweeps': S, 'anneals': R, 'value': B / (ms / 1e3), 'unit': 'detections/s', 'ms_per_step': ms,
+                 'stages_ms': {'map': st[0], 'warm_start': st[1], 'anneal': st[2], 'readout': st[3]},
+                 'mean_final_energy': float(det.energies().min(1).values.clamp(max=0).double().mean()),
+                 'ber': {'%d dB' % v: float(err[sn == v].sum()) / ((sn == v).sum() * nb) for v in snrs}}
+            if net is not None:
+                r['kept_fraction'] = float(det.kept.float().mean())
+                r['ber_ratio_vs_plain'] = {}
+                for v in snrs:
+                    m = sn == v
+                    rr, lo, hi = stats.boot_ratio(err[m], base_err[m], B=1000)
+                    r['ber_ratio_vs_plain']['%d dB' % v] = [rr, lo, hi]
+                r['speedup_vs_plain'] = r['value'] / res['plain_full']['value']
+            else:
+                base_err = err
+            if nt == 32 and args.latency_frames > 0:
+                f = channel.draw_device(77 + rank, 14.0, 1, nt, 16, dev=dev)
+                d1 = warm.WarmDetector(1, nt, anneals=R, sweeps=S, mlp=net, device=dev)
+                d1.set_noise(N0=f['N0'])
+                r['frame_latency'] = frame_latency(d1, f, stream, min(args.latency_frames, 1000))
+                del d1
+            res[name] = r
+            del det
+        out['x%d' % nt] = res
+    return out
+
+
+SERVE_CLASSES = [(8, 16, 4), (16, 16, 16), (24, 36, 64), (32, 32, 16), (48, 72, 4), (64, 64, 16)]
+
+
+def serving(args, dev, rank, mlp=None):
+    """Mixed-size frames (users x antennas x constellation as SERVE_CLASSES, SNR uniform 5-25 dB) arriving as
+    Poisson streams at each offered rate, served by the continuous-batching loop (arpeggio_b200.serve.Server,
+    2 lanes per class, 32 anneals at each class's Arpeggio budget, plain MMSE start unless an MLP is given):
+    per-class p50/p99 latency (arrival to completion seen by the loop) and the achieved frames/s."""
+    import torch
+    from arpeggio_b200 import channel, serve
+    out = {'classes': ['%d users x %d antennas %d-QAM' % c for c in SERVE_CLASSES],
+           'start': 'warm (MLP)' if mlp is not None else 'plain MMSE start', 'rates': {}}
+    for rate, seconds in ((1e5, 0.2), (1e6, 0.05)):
+        rng = np.random.default_rng(17 + rank)
+        n_all = int(rate * seconds)
+        share = rng.multinomial(n_all, [1.0 / len(SERVE_CLASSES)] * len(SERVE_CLASSES))
+        srv = serve.Server(SERVE_CLASSES, mlp=mlp, anneals=32, slots=4096, inflight=2, hbm_budget=24 << 30,
+                           device=dev)
+        t_all = serve.poisson_arrivals(n_all, rate, rng)
+        cls_of = rng.integers(0, len(SERVE_CLASSES), n_all)
+        for ci, cls in enumerate(SERVE_CLASSES):
+            nt, nr, M = cls
+            t = t_all[cls_of == ci]
+            n = len(t)
+            if n == 0:
+                continue
+            snr = torch.tensor(rng.uniform(5, 25, n), dtype=torch.float32)
+            d = channel.draw_device(500 + ci, snr, n, nt, M, nr=nr, dev=dev)
+            srv.open(cls, d['H'].cpu().pin_memory(), d['y'].cpu().pin_memory(), d['N0'].cpu(), t,
+                     np.arange(n) + (ci << 24))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = srv.serve(timeout=300)
+        wall = time.perf_counter() - t0
+        out['rates']['%.0e frames/s' % rate] = {'frames': n_all, 'seconds_offered': float(t_all[-1]),
+                                                'seconds_to_drain': wall,
+                                                'achieved_frames_per_s': n_all / wall, 'per_class': st}
+        del srv
+        torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
@@ -306,6 +442,12 @@ def run_ours(args):
                     'reference_recorded_source': 'data/results/a513_fixed/x16/arpeggiofx_64_0.1_0.1_0_rand_32/'
                                                  'snr_20.00 (B200 anneal + 4 CPU threads)'}
 
+    # ---- learned warm start against the plain MMSE-started annealer (the metric's "warm vs plain")
+    warm_line = None
+    if args.warm_train > 0:
+        warm_line = warm_vs_plain(args, dev, stream, rank)
+    serve_line = serving(args, dev, rank) if args.serve else None
+
     # ---- integer-issue peak (calibration kernel) and the anneal kernel's algorithmic work
     L = _lib.lib()
     buf = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -366,6 +508,8 @@ def run_ours(args):
         'latency': lat,
         'ber': ber,
         'mdi_x16': mdi_line,
+        'warm_vs_plain': warm_line,
+        'serving': serve_line,
         'extra': extra,
         'gpu_launches': 3 * K,
         'clocks': ck,
@@ -420,6 +564,9 @@ def main():
     ap.add_argument('--latency-frames', type=int, default=2000, help='single-frame replays for p50/p99 latency')
     ap.add_argument('--mdi-batch', type=int, default=16384, help='uses of the multi-stage (MDI) line; 0 skips it')
     ap.add_argument('--no-extras', dest='extras', action='store_false', help='skip the Chord and 64-user lines')
+    ap.add_argument('--no-serve', dest='serve', action='store_false', help='skip the serving-loop block')
+    ap.add_argument('--warm-train', type=int, default=2_000_000,
+                    help='training instances of the warm-start MLP for the warm-vs-plain block; 0 skips it')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.rank = int(os.environ.get('RANK', 0))

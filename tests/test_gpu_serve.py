@@ -1,0 +1,54 @@
+"""The serving loop: continuous batching of mixed-size frames (users, antennas, constellations) arriving as a
+Poisson stream; every request's bits and distance equal those of the same request detected alone."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+CLASSES = [(8, 16, 4), (24, 36, 64), (32, 32, 16)]
+
+
+def _streams(n, seed):
+    from arpeggio_b200 import channel, serve
+    rng = np.random.default_rng(seed)
+    out = {}
+    for ci, (nt, nr, M) in enumerate(CLASSES):
+        snr = torch.tensor(rng.uniform(5, 25, n), dtype=torch.float32)
+        d = channel.draw_device(seed * 10 + ci, snr, n, nt, M, nr=nr, dev='cpu')
+        t = serve.poisson_arrivals(n, 2e4, rng)
+        rid = 1000 * (ci + 1) + np.arange(n)
+        out[(nt, nr, M)] = (d['H'].pin_memory(), d['y'].pin_memory(), d['N0'], t, rid)
+    return out
+
+
+@pytest.mark.parametrize('warm_start', [False, True])
+def test_each_result_is_the_same_alone_and_in_the_mix(warm_start):
+    from arpeggio_b200 import serve, warm
+    mlp = warm.WarmMLP(P=2, seed=3) if warm_start else None
+    srv = serve.Server(CLASSES, mlp=mlp, anneals=8, sweeps=8, slots=64, inflight=2, hbm_budget=1 << 30)
+    streams = _streams(300, 5)
+    for cls, (H, y, N0, t, rid) in streams.items():
+        srv.open(cls, H, y, N0, t, rid)
+    stats = srv.serve()
+    for cls, (H, y, N0, t, rid) in streams.items():
+        st = srv.streams[cls]
+        key = '%dx%d %d-QAM' % cls
+        assert stats[key]['requests'] == 300
+        assert stats[key]['batches'] > 1  # continuous batching, not one batch
+        assert not np.isnan(st['done']).any()
+        nt, nr, M = cls
+        alone = warm.WarmDetector(1, nt, nr, M, anneals=8, sweeps=8, mlp=mlp)
+        for i in np.random.default_rng(1).choice(300, 40, replace=False):
+            alone.set_noise(N0=N0[i:i + 1])
+            inst = torch.tensor([int(rid[i])], dtype=torch.int32, device='cuda')
+            bits, _, dist = alone.run(H[i:i + 1].cuda(), y[i:i + 1].cuda(), srv.key, n=1, inst=inst)
+            torch.cuda.synchronize()
+            assert torch.equal(bits[0].cpu(), st['bits'][i]), (cls, i)
+            assert float(dist[0]) == float(st['dist'][i]), (cls, i)
+
+
+def test_server_rejects_classes_beyond_shared_memory():
+    from arpeggio_b200 import serve
+    with pytest.raises(ValueError):
+        serve.Server([(96, 96, 16)], anneals=8, sweeps=8, slots=16)

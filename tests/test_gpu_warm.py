@@ -141,7 +141,7 @@ def test_warm_start_and_warm_anneal_match_oracle():
     w.run(d['H'], d['y'], seed=77)
     torch.cuda.synchronize()
     w.check()
-    Z = mlp.Z[:64 * 64].cpu().numpy()
+    Z = w.mlp_scratch['Z'][:64 * 64].cpu().numpy()
     G, h, xq = w.G.cpu().numpy(), w.h.cpu().numpy(), w.xq.cpu().numpy()
     m0, perm, e0, kept = O.warm_start(Z, G, h, xq, 2, 16)
     assert np.array_equal(w.m0.cpu().numpy(), m0)

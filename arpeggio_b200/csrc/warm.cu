@@ -581,3 +581,288 @@ extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const
                                                   perm, (float*)e0, kept);
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
+
+// ------------------------------------------------------------------------------------------------ fused inference
+// The whole network for a 128-row tile in one CTA (persistent over tiles, 8 warps, one CTA per SM):
+//   L1: D[0:512) = X W1^T      (X tile 128 x 16 and W1 staged in shared memory; two N = 256 MMAs)
+//   epilogue 1: TMEM -> bias + ReLU -> bf16 -> H tile (128 x 512, K-major canonical layout, shared memory)
+//   L2: D[0:512) = H1 W2^T     W2 streamed in 32 chunks (256 rows x 32 k, 16 KB each, one bulk copy from the packed
+//                              copy W2p) through a 4-slot ring: thread 0 produces (full barrier with the byte
+//                              count), thread 32 issues the MMAs and releases each slot with tcgen05.commit on
+//                              its empty barrier
+//   epilogue 2: TMEM -> bias + ReLU -> bf16 -> the same H tile (every L2 MMA has completed)
+//   L3: D[0:16) = H2 W3        (W3t (512 x 16) staged MN-major; 32 MMAs of K = 16)
+//   epilogue 3: TMEM -> + b3 -> logits (rows, 16) float in global memory
+// Only X and the logits touch HBM; the weights come from L2.  Shared memory: H 128 KB + X 4 KB + ring 64 KB.
+// Slot layout of a W2 chunk (K-major, no swizzle): byte(n, k) = (k / 8) 4096 + n 16 + (k % 8) 2, i.e. SBO 128 B
+// between 8-row groups and LBO 4096 B between k-groups; arp_mlp_pack_w2 writes W2 in this order once per weight
+// update, so a chunk is one contiguous 16 KB copy (whole L2 sectors, no gather).
+namespace arp {
+
+constexpr int kMlpThreads = 256;
+constexpr uint32_t kHsBytes = 128 * 512 * 2, kXsBytes = 128 * 16 * 2, kSlotBytes = 256 * 32 * 2;
+constexpr uint32_t kMlpSmem = kHsBytes + kXsBytes + 4 * kSlotBytes;
+
+struct MlpParams {
+  const bf16* X;
+  const bf16 *W1, *W2p, *W3t;
+  const float *b1, *b2, *b3;
+  float* logits;
+  int rows;
+  int32_t* status;
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::su32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// One contiguous global -> shared bulk copy (no tensor map), completing `bytes` on the mbarrier.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(umma::su32(bar))
+               : "memory");
+}
+
+// W2 (512 x 512, row-major) -> chunk order of the fused kernel's ring: chunk t = rows [256 (t / 16), +256) and
+// k [32 (t % 16), +32), within a chunk k-group b (8 wide) then row n then element: W2p[t][b][n][e].
+__global__ void __launch_bounds__(256) k_pack_w2(const bf16* __restrict__ W2, bf16* __restrict__ W2p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one 16-byte group of 8 elements
+  if (i >= 512 * 64) return;
+  const int t = i >> 10, b = (i >> 8) & 3, n = i & 255;  // 1024 groups per chunk, 256 per k-group
+  const int row = (t >> 4) * 256 + n, k = (t & 15) * 32 + b * 8;
+  reinterpret_cast<uint4*>(W2p)[i] = *reinterpret_cast<const uint4*>(W2 + (size_t)row * 512 + k);
+}
+
+// TMEM -> bias (shared memory) + ReLU -> bf16 -> H tile; warp w drains rows 32 (w % 4) .. and columns
+// [256 (w / 4), +256).
+__device__ __forceinline__ void mlp_epi_hidden(uint32_t tmem, uint32_t hs, const float* bias, int warp,
+                                               int lane) {
+  const int m = (warp & 3) * 32 + lane, half = warp >> 2;
+#pragma unroll 1
+  for (int cc = 0; cc < 8; ++cc) {
+    const int c0 = half * 256 + cc * 32;
+    uint32_t v[32];
+    umma::tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 bl = *reinterpret_cast<const float4*>(bias + c0 + q * 8);
+      const float4 bh = *reinterpret_cast<const float4*>(bias + c0 + q * 8 + 4);
+      const float bb[8] = {bl.x, bl.y, bl.z, bl.w, bh.x, bh.y, bh.z, bh.w};
+      uint32_t pk[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int j = q * 8 + 2 * i;
+        const float a = fmaxf(__uint_as_float(v[j]) + bb[2 * i], 0.0f);
+        const float b = fmaxf(__uint_as_float(v[j + 1]) + bb[2 * i + 1], 0.0f);
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+        pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
+      }
+      const uint32_t addr = hs + (uint32_t)((m >> 3) * 8192 + ((c0 >> 3) + q) * 128 + (m & 7) * 16);
+      asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
+                   "r"(pk[3])
+                   : "memory");
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t full[4], empty[4];
+  __shared__ __align__(8) uint64_t bar_l1, bar_l2, bar_l3;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  __shared__ __align__(16) float s_b1[512], s_b2[512];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = (p.rows + 127) / 128;
+  if ((int)blockIdx.x >= ntiles) return;
+  for (int i = tid; i < 512; i += kMlpThreads) {
+    s_b1[i] = p.b1[i];
+    s_b2[i] = p.b2[i];
+  }
+  const uint32_t hs = umma::su32(smem), xs = hs + kHsBytes, ring = xs + kXsBytes;
+  const uint32_t w1s = ring + 3 * kSlotBytes, w3s = ring + 2 * kSlotBytes;
+  constexpr uint32_t ID_HID = umma::idesc_bf16(256, false, false), ID_OUT = umma::idesc_bf16(16, false, true);
+  if (tid == 0) {
+    for (int s = 0; s < 4; ++s) {
+      umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&empty[s], 1);
+    }
+    umma::mbar_init(&bar_l1, 1);
+    umma::mbar_init(&bar_l2, 1);
+    umma::mbar_init(&bar_l3, 1);
+    umma::fence_mbar_init();
+    s_abort = 0;
+  }
+  if (warp == 0) umma::tmem_alloc(&s_tmem, 512);
+  umma::tc_before_sync();
+  __syncthreads();
+  umma::tc_after_sync();
+  const uint32_t tmem = s_tmem;
+
+  auto load_x = [&](int tile) {  // 128 x 16: one 16-byte chunk per thread
+    const int row = tid >> 1, kc = tid & 1, m = tile * 128 + row;
+    const bool ok = m < p.rows;
+    umma::cp16(xs + (uint32_t)((row >> 3) * 256 + kc * 128 + (row & 7) * 16),
+               ok ? (const void*)(p.X + (size_t)m * 16 + kc * 8) : (const void*)p.X, ok);
+  };
+  auto load_w1 = [&]() {  // 512 x 16, K-major, SBO 256
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tid + i * kMlpThreads, row = c >> 1, kc = c & 1;
+      umma::cp16(w1s + (uint32_t)((row >> 3) * 256 + kc * 128 + (row & 7) * 16), p.W1 + (size_t)row * 16 + kc * 8,
+                 true);
+    }
+  };
+  auto load_w3 = [&]() {  // W3t (512 k x 16 n), MN-major: LBO 256 between k-groups, SBO 128
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tid + i * kMlpThreads, kr = c >> 1, nc = c & 1;
+      umma::cp16(w3s + (uint32_t)((kr >> 3) * 256 + nc * 128 + (kr & 7) * 16), p.W3t + (size_t)kr * 16 + nc * 8,
+                 true);
+    }
+  };
+  // W2 chunk g (global count of this CTA's chunks): slot g % 4, rows 256 ((g % 32) / 16), k 32 (g % 16)
+  auto produce = [&](int g) -> bool {
+    const int s = g & 3, t = g & 31;
+    if (g >= 4 && !umma::mbar_wait(&empty[s], ((g >> 2) - 1) & 1)) return false;
+    mbar_expect_tx(&full[s], kSlotBytes);
+    bulk_load(ring + (uint32_t)s * kSlotBytes, p.W2p + (size_t)t * (kSlotBytes / 2), kSlotBytes, &full[s]);
+    return true;
+  };
+
+  load_x(blockIdx.x);
+  load_w1();
+  umma::cp_commit();
+  int it = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int g0 = it * 32;
+    // ---- layer 1 (X and W1 landed; the previous tile's TMEM reads are done)
+    umma::cp_wait<0>();
+    umma::fence_async_smem();
+    umma::tc_before_sync();
+    __syncthreads();
+    if (s_abort) break;
+    if (tid == 32) {
+      umma::tc_after_sync();
+      const uint64_t ad = umma::sdesc(xs, 128, 256);
+      umma::mma(tmem, ad, umma::sdesc(w1s, 128, 256), ID_HID, 0u);
+      umma::mma(tmem + 256, ad, umma::sdesc(w1s + 8192, 128, 256), ID_HID, 0u);
+      umma::commit(&bar_l1);
+    }
+    if (tid == 0)  // chunks 0-2 go to slots 0-2 (free: the previous tile's L2 and L3 have completed)
+      for (int g = g0; g < g0 + 3; ++g)
+        if (!produce(g)) s_abort = 1;
+    if (!umma::mbar_wait(&bar_l1, it & 1)) s_abort = 1;
+    umma::tc_after_sync();
+    mlp_epi_hidden(tmem, hs, s_b1, warp, lane);
+    umma::fence_async_smem();
+    umma::tc_before_sync();
+    __syncthreads();
+    if (s_abort) break;
+    // ---- layer 2: producer thread 0, MMA thread 32; everyone else waits for the last commit
+    if (tid == 0) {
+      for (int g = g0 + 3; g < g0 + 32; ++g)  // slot 3 held W1: free since L1 completed
+        if (!produce(g)) {
+          s_abort = 1;
+          break;
+        }
+    } else if (tid == 32) {
+      bool ok = true;
+      for (int t = 0; t < 32; ++t) {
+        const int g = g0 + t, s = g & 3;
+        if (!umma::mbar_wait(&full[s], (g >> 2) & 1)) {
+          ok = false;
+          break;
+        }
+        umma::tc_after_sync();
+        const int c32 = t & 15;
+        const uint32_t d = tmem + (uint32_t)((t >> 4) * 256), slot = ring + (uint32_t)s * kSlotBytes;
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk)
+          umma::mma(d, umma::sdesc(hs + (uint32_t)((c32 * 4 + kk * 2) * 128), 128, 8192),
+                    umma::sdesc(slot + (uint32_t)(kk * 8192), 4096, 128), ID_HID, (c32 > 0 || kk > 0) ? 1u : 0u);
+        umma::commit(&empty[s]);
+      }
+      if (ok)
+        umma::commit(&bar_l2);
+      else
+        s_abort = 1;
+    }
+    __syncwarp();
+    if (!umma::mbar_wait(&bar_l2, it & 1)) s_abort = 1;
+    load_w3();  // slot 2 and slot 3 are free: every L2 MMA has completed
+    if (tile + (int)gridDim.x < ntiles) {
+      load_x(tile + gridDim.x);
+      load_w1();
+    }
+    umma::cp_commit();
+    umma::tc_after_sync();
+    mlp_epi_hidden(tmem, hs, s_b2, warp, lane);
+    umma::cp_wait<0>();
+    umma::fence_async_smem();
+    umma::tc_before_sync();
+    __syncthreads();
+    if (s_abort) break;
+    // ---- layer 3
+    if (tid == 32) {
+      umma::tc_after_sync();
+#pragma unroll 4
+      for (int kk = 0; kk < 32; ++kk)
+        umma::mma(tmem, umma::sdesc(hs + (uint32_t)(kk * 256), 128, 8192), umma::sdesc(w3s + (uint32_t)(kk * 512), 256, 128),
+                  ID_OUT, kk > 0 ? 1u : 0u);
+      umma::commit(&bar_l3);
+    }
+    if (!umma::mbar_wait(&bar_l3, it & 1)) s_abort = 1;
+    umma::tc_after_sync();
+    if (warp < 4) {
+      uint32_t v[32];
+      umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+      const int row = tile * 128 + warp * 32 + lane;
+      if (row < p.rows && !s_abort) {
+        float4* o = reinterpret_cast<float4*>(p.logits + (size_t)row * 16);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          o[i] = make_float4(__uint_as_float(v[4 * i]) + __ldg(p.b3 + 4 * i),
+                             __uint_as_float(v[4 * i + 1]) + __ldg(p.b3 + 4 * i + 1),
+                             __uint_as_float(v[4 * i + 2]) + __ldg(p.b3 + 4 * i + 2),
+                             __uint_as_float(v[4 * i + 3]) + __ldg(p.b3 + 4 * i + 3));
+      }
+    }
+  }
+  umma::cp_wait<0>();
+  umma::tc_before_sync();
+  __syncthreads();
+  if (s_abort && tid == 0) set_status(p.status, ARP_ERR_TIMEOUT);
+  if (warp == 0) umma::tmem_free(tmem, 512);
+}
+
+}  // namespace arp
+
+extern "C" int arp_mlp_forward(const void* X, int rows, const void* W1, const float* b1, const void* W2p,
+                               const float* b2, const void* W3t, const float* b3, float* logits, int32_t* status,
+                               void* stream) {
+  if (rows < 0) return ARP_ERR_SHAPE;
+  if (rows == 0) return ARP_OK;
+  if (!X || !W1 || !b1 || !W2p || !b2 || !W3t || !b3 || !logits) return ARP_ERR_ARG;
+  if (!al16(X) || !al16(W1) || !al16(W2p) || !al16(W3t) || !al16(logits)) return ARP_ERR_ARG;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem) != cudaSuccess)
+      return ARP_ERR_LAUNCH;
+    attr = true;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ntiles = (rows + 127) / 128;
+  MlpParams p{(const bf16*)X, (const bf16*)W1, (const bf16*)W2p, (const bf16*)W3t, b1, b2, b3, logits, rows, status};
+  k_mlp_fused<<<ntiles < sms ? ntiles : sms, kMlpThreads, kMlpSmem, (cudaStream_t)stream>>>(p);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_mlp_pack_w2(const void* W2, void* W2p, void* stream) {
+  if (!W2 || !W2p || !al16(W2) || !al16(W2p)) return ARP_ERR_ARG;
+  k_pack_w2<<<(512 * 64 + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const bf16*)W2, (bf16*)W2p);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}

@@ -22,7 +22,7 @@ import torch
 
 from . import _lib
 from .detector import PAM, el2
-from .warm import NF, NH, NO, WarmDetector
+from .warm import NF, NO, WarmDetector
 
 
 class _Lane:
@@ -56,7 +56,7 @@ def lane_bytes(cls, slots, anneals, warm):
     nb = D * PAM[M]['bits']
     per = D * (4 + NF * 2 + 2) + 8 + 4 + 4 + D + nb + 4 + 4 + 4 * (NR2 * D + NR2) + 12
     if warm:
-        per += D * (2 * NH * 2 + NO * 4)
+        per += D * NO * 4  # logits; the fused network keeps its hidden activations on chip
     return ws + slots * per
 
 

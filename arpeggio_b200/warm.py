@@ -53,6 +53,8 @@ class WarmMLP:
             w[oo:oo + int(np.prod(shp))] = torch.randn(int(np.prod(shp)), generator=g) * std
         self.w = w.to(self.device)
         self.wb = self.w.to(torch.bfloat16)
+        self.w2p = torch.empty(NH * NH, dtype=torch.bfloat16, device=self.device)  # W2 in the fused kernel's order
+        self.pack()
         self.grad = torch.zeros_like(self.w)
         self.m = torch.zeros_like(self.w)
         self.v = torch.zeros_like(self.w)
@@ -111,6 +113,22 @@ class WarmMLP:
              bias=self.view(self.w, 'b3'), status=st, stream=stream)
         return Z[:rows]
 
+    def pack(self, stream=None):
+        """Refreshes the packed copy of W2 that the fused forward streams (after every weight change)."""
+        _lib.check(_lib.lib().arp_mlp_pack_w2(_lib.ptr(self.view(self.wb, 'W2')), _lib.ptr(self.w2p),
+                                              _lib.stream_ptr(stream)), 'mlp_pack_w2')
+
+    def infer(self, X, rows, Z, stream=None):
+        """logits Z (rows, 16) float32 of features X (rows, 16) bf16 in one fused persistent launch
+        (arp_mlp_forward): the hidden activations stay on chip; same roundings and summation order as forward()."""
+        wb, w = self.wb, self.w
+        _lib.check(_lib.lib().arp_mlp_forward(_lib.ptr(X), rows, _lib.ptr(self.view(wb, 'W1')),
+                                              _lib.ptr(self.view(w, 'b1')), _lib.ptr(self.w2p),
+                                              _lib.ptr(self.view(w, 'b2')), _lib.ptr(self.view(wb, 'W3t')),
+                                              _lib.ptr(self.view(w, 'b3')), _lib.ptr(Z), _lib.ptr(self.status),
+                                              _lib.stream_ptr(stream)), 'mlp_forward')
+        return Z[:rows]
+
     def backward(self, X, labels, rows, stream=None):
         """Summed softmax cross-entropy over the rows' labels (< 0: ignored) and its gradients into self.grad
         (zeroed first); the forward pass must have run on the same X.  rows: a multiple of 16."""
@@ -141,6 +159,7 @@ class WarmMLP:
         _lib.check(_lib.lib().arp_adam(_lib.ptr(self.w), _lib.ptr(self.wb), _lib.ptr(self.grad), _lib.ptr(self.m),
                                        _lib.ptr(self.v), self.n, float(lr), float(beta1), float(beta2), float(eps),
                                        self.steps, float(scale), _lib.stream_ptr(stream)), 'adam')
+        self.pack(stream)
 
     def train_step(self, X, labels, rows, lr=1e-3, stream=None):
         """Forward, backward and one Adam step on the mean loss over `rows` rows (a multiple of 16)."""
@@ -158,6 +177,7 @@ class WarmMLP:
     def load_state_dict(self, d):
         self.w.copy_(torch.as_tensor(np.asarray(d['w'], dtype=np.float32)))
         self.wb.copy_(self.w.to(torch.bfloat16))
+        self.pack()
         self.steps = int(d.get('steps', 0))
 
     def numpy_params(self):
@@ -184,7 +204,7 @@ class WarmDetector(Detector):
         self.e0 = torch.zeros(B, dtype=torch.int64, device=dev)
         self.kept = torch.zeros(B, dtype=torch.int32, device=dev)
         self.snr_db = torch.zeros(B, dtype=torch.float32, device=dev)
-        self.mlp_scratch = mlp.scratch(B * D) if mlp is not None else None
+        self.Z = torch.empty(B * D, NO, dtype=torch.float32, device=dev) if mlp is not None else None
 
     def set_noise(self, snr_db=None, N0=None, n=None):
         super().set_noise(snr_db, N0, n)
@@ -235,7 +255,7 @@ class WarmDetector(Detector):
             _lib.check(L.arp_warm_features(_lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), _lib.ptr(zs),
                                            _lib.ptr(self.snr_db[sl]), n, D, self.M, P, 1, _lib.ptr(X), None, None, sp),
                        'warm_features')
-            Z = self.mlp.forward(X, n * D, stream, scratch=self.mlp_scratch)
+            Z = self.mlp.infer(X, n * D, self.Z[off * D:(off + n) * D], stream)
             _lib.check(L.arp_warm_start(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P, self.M, 1,
                                         _lib.ptr(self.m0[sl]), _lib.ptr(self.perm[sl]), _lib.ptr(self.e0[sl]),
                                         _lib.ptr(self.kept[sl]), sp), 'warm_start')
@@ -305,3 +325,33 @@ def train(mlp, nt=32, M=16, instances=2_000_000, batch=16384, snr=(8.0, 20.0), a
     plain.check()
     mlp.check()
     return hist
+
+
+def _profile_main(argv):
+    """python -m arpeggio_b200.warm profile --batch B: trains a network briefly (262144 instances), then runs
+    three warm detections of B seeded 32-user uses (32 anneals x 16 sweeps) and prints their stage times."""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument('mode', choices=['profile'])
+    ap.add_argument('--batch', type=int, default=16384)
+    ap.add_argument('--train', type=int, default=262144)
+    a = ap.parse_args(argv)
+    mlp = WarmMLP(P=2, seed=0)
+    train(mlp, nt=32, instances=a.train, batch=min(a.train, 16384), anneals=32, sweeps=32, seed=11)
+    B = a.batch
+    snr = torch.tensor([float(v) for v in np.repeat([10, 14, 18, 22], -(-B // 4))[:B]])
+    d = channel.draw_device(5, snr, B, 32, 16)
+    det = WarmDetector(B, 32, anneals=32, sweeps=16, mlp=mlp)
+    det.set_noise(N0=d['N0'])
+    for i in range(2):
+        det.run(d['H'], d['y'], seed=i)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    det.run(d['H'], d['y'], seed=9, events=ev)
+    torch.cuda.synchronize()
+    det.check()
+    print('stages ms (map, warm start, anneal, readout):', [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(4)])
+
+
+if __name__ == '__main__':
+    import sys
+    _profile_main(sys.argv[1:])

@@ -216,6 +216,18 @@ int arp_colsum_bf16(const void* X, int rows, int cols, int ld, float* out, void*
 int arp_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, float lr, float beta1, float beta2,
              float eps, int step, float grad_scale, void* stream);
 
+/* W2 (512, 512) bf16 row-major -> W2p, the same 512 x 512 values in the order arp_mlp_forward streams them
+ * (32 chunks of 256 rows x 32 k; within a chunk k-group of 8, then row, then element).  Once per weight update. */
+int arp_mlp_pack_w2(const void* W2, void* W2p, void* stream);
+
+/* The network's forward pass in one persistent launch (no reference counterpart): logits (rows, 16) float =
+ * relu(relu(X W1^T + b1) W2^T + b2) W3t + b3 with X (rows, 16), W1 (512, 16), W2 (512, 512) given packed as W2p
+ * (arp_mlp_pack_w2), W3t (512, 16) bf16 and fp32 biases; per 128-row tile the hidden activations stay in TMEM and
+ * shared memory (bf16, the same roundings and summation order as the three arp_gemm_bf16 calls of the training
+ * path). */
+int arp_mlp_forward(const void* X, int rows, const void* W1, const float* b1, const void* W2p, const float* b2,
+                    const void* W3t, const float* b3, float* logits, int32_t* status, void* stream);
+
 /* Warm start from the logits (B*D, ldl): m0 (B, D) the start spin sum of each coordinate (argmax class, clamped
  * to the constellation), perm (B, D) the flip-test order (position j' tests coordinate perm[j'], by descending
  * 1 - p(m = 0)), e0 (B) the start's energy 2 (m^T G m - h^T m) relative to the guess, in the units of the

@@ -131,6 +131,22 @@ def test_mlp_forward_and_gradients_match_oracle():
     assert abs(float(mlp.loss.item()) - gr['loss']) <= 1e-3 * abs(gr['loss']) + 1e-2
 
 
+@pytest.mark.parametrize('rows', [64, 128, 1000, 4096, 40000])
+def test_fused_forward_equals_the_layer_by_layer_forward(rows):
+    """One persistent launch (hidden activations on chip) against the three GEMM launches of the training path:
+    same bf16 roundings and summation order, so the logits agree to the last bit."""
+    from arpeggio_b200 import warm
+    g = torch.Generator().manual_seed(rows)
+    mlp = warm.WarmMLP(P=2, seed=rows)
+    X = (torch.randn(rows, 16, generator=g) * 2).to(torch.bfloat16).cuda()
+    ref = mlp.forward(X, rows).clone()
+    Z = torch.full((rows, 16), float('nan'), device='cuda')
+    mlp.infer(X, rows, Z)
+    torch.cuda.synchronize()
+    mlp.check()
+    torch.testing.assert_close(Z, ref, rtol=0, atol=0)
+
+
 def test_warm_start_and_warm_anneal_match_oracle():
     from arpeggio_b200 import _lib, warm
     d, det = _problems(64, 32, 16.0, 21)
@@ -141,7 +157,7 @@ def test_warm_start_and_warm_anneal_match_oracle():
     w.run(d['H'], d['y'], seed=77)
     torch.cuda.synchronize()
     w.check()
-    Z = w.mlp_scratch['Z'][:64 * 64].cpu().numpy()
+    Z = w.Z[:64 * 64].cpu().numpy()
     G, h, xq = w.G.cpu().numpy(), w.h.cpu().numpy(), w.xq.cpu().numpy()
     m0, perm, e0, kept = O.warm_start(Z, G, h, xq, 2, 16)
     assert np.array_equal(w.m0.cpu().numpy(), m0)

@@ -284,6 +284,48 @@ __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G,
   for (int o = 16; o > 0; o >>= 1) sdg += __shfl_xor_sync(0xffffffffu, sdg, o);
   const float mdg = sdg / (float)D;
   const int Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
+  // Two Jacobi refinements of the single-coordinate move: u_j = (h_j - 2 sum_{i != j} G_ij m_i) / 4 G_jj (level
+  // steps) with every other coordinate at its previous greedy move m_i = 2 clamp(rint(u_i), -1, 1), kept inside
+  // the constellation.  They see the coupling G m, which the per-coordinate network cannot.
+  float u1[4], u2[4];
+  {
+    float hv[4];
+    int mq[4], xv[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int j = t * 32 + lane;
+      hv[t] = j < D ? (float)h[(size_t)b * D + j] : 0.0f;
+      xv[t] = j < D ? xq[(size_t)b * D + j] : 0;
+    }
+    auto quant = [&](float u, int x) {
+      int m = 2 * (int)fminf(fmaxf(rintf(u), -1.0f), 1.0f);
+      if (x + m > Lmax) m = Lmax - x;
+      if (x + m < -Lmax) m = -Lmax - x;
+      return m;
+    };
+#pragma unroll
+    for (int t = 0; t < 4; ++t) mq[t] = dg[t] > 0.0f ? quant(hv[t] / (4.0f * dg[t]), xv[t]) : 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      float acc[4] = {0, 0, 0, 0};
+      for (int i = 0; i < D; ++i) {
+        const int mi = __shfl_sync(0xffffffffu, mq[i >> 5], i & 31);
+        if (mi == 0) continue;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int j = t * 32 + lane;
+          if (j < D && j != i) acc[t] = fmaf((float)Gb[(size_t)i * D + j], (float)mi, acc[t]);
+        }
+      }
+      float* u = pass == 0 ? u1 : u2;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const float v = dg[t] > 0.0f ? (hv[t] - 2.0f * acc[t]) / (4.0f * dg[t]) : 0.0f;
+        u[t] = fminf(fmaxf(v, -8.0f), 8.0f);
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) mq[t] = (t * 32 + lane) < D && dg[t] > 0.0f ? quant(u[t], xv[t]) : 0;
+    }
+  }
   const float snr = snr_db ? snr_db[b] * 0.05f : 0.0f;
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
@@ -306,6 +348,8 @@ __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G,
     f[8] = 1.0f;
     f[0] = fminf(fmaxf(f[0], -8.0f), 8.0f);
     f[2] = fminf(f[2], 64.0f);
+    f[9] = u1[t];
+    f[10] = u2[t];
     uint32_t pk[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {

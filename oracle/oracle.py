@@ -377,6 +377,20 @@ def warm_features(G, h, xq, zs, snr_db, M, P, levels=None):
     f[..., 6] = x == -Lmax
     f[..., 7] = 0 if zs is None else np.clip(0.5 * (np.asarray(zs, dtype=np.float64) - x), -4, 4)
     f[..., 8] = 1
+    # two Jacobi refinements of the single-coordinate move (others at their previous greedy move)
+    xi = np.asarray(xq, dtype=np.int64)
+
+    def quant(u):
+        m = 2 * np.clip(np.rint(u), -1, 1).astype(np.int64)
+        m = np.where(xi + m > Lmax, Lmax - xi, m)
+        return np.where(xi + m < -Lmax, -Lmax - xi, m)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        m = np.where(dg > 0, quant(np.where(dg > 0, h / (4 * dg), 0)), 0)
+        for k in (9, 10):
+            acc = np.einsum('bij,bi->bj', off, m.astype(np.float64))
+            u = np.clip(np.where(dg > 0, (h - 2 * acc) / (4 * dg), 0), -8, 8)
+            f[..., k] = u
+            m = np.where(dg > 0, quant(u), 0)
     lab = None
     if levels is not None:
         lab = np.clip((np.asarray(levels, dtype=np.int64) - np.asarray(xq, dtype=np.int64)) // 2 + P // 2, 0, P)

@@ -36,6 +36,7 @@ SIGNATURES = {
     'arp_mdi_map': [_P, _P, _P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P],
     'arp_mdi_update': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P],
     'arp_mdi_select': [_P, _P, _I, _I, _I, _I, _P, _P, _P],
+    'arp_anneal_tune': [_I, _I, _I, _I, _I],
     'arp_map_dd_soft': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
     'arp_gemm_bf16': [_P, _I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P],
     'arp_warm_features': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P],

@@ -607,6 +607,10 @@ static int pick_warps(K kern, size_t smem, int R) {
   return best_w;
 }
 
+// Warps per block chosen by a caller's autotuner per (slots NS, copies P, policy, FP32 fields); 0 = occupancy
+// heuristic.  Process-wide, set through arp_anneal_tune.
+static int g_tuned_warps[5][7][2][2];
+
 template <int NS, int P, bool CHORD, bool FLT, bool WARM = false>
 static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   constexpr bool CACHE = P * NS <= 8;
@@ -621,6 +625,7 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   static size_t cached_smem = 0;
   static int cached_w = 0;
   static int cached_nb = 0, sms = 0;
+  int per_sm = cached_nb > 0 ? cached_nb : 1;
   if (warps <= 0) {
     if (cached_w == 0 || cached_smem != smem) {
       cached_w = pick_warps(kern, smem, 8);
@@ -632,12 +637,18 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
     warps = cached_w;
+    per_sm = cached_nb > 0 ? cached_nb : 1;
+    const int tw = g_tuned_warps[NS][P][CHORD ? 1 : 0][FLT ? 1 : 0];
+    if (tw > 0 && tw != warps) {  // same resident warps per SM, another width
+      per_sm = cached_nb * cached_w / tw > 0 ? cached_nb * cached_w / tw : 1;
+      warps = tw;
+    }
     while (warps > 1 && warps > a.R) warps >>= 1;
   }
   // Small batches: split each problem's anneals over several blocks so the batch still fills the GPU.
   DDParams b = a;
   b.split = 1;
-  const long long slots = (long long)(cached_nb > 0 ? cached_nb : 1) * (sms > 0 ? sms : 148);
+  const long long slots = (long long)per_sm * (sms > 0 ? sms : 148);
   if ((long long)a.B < slots) {
     const int most = (a.R + warps - 1) / warps;
     long long sp = (slots + a.B - 1) / a.B;
@@ -749,4 +760,13 @@ extern "C" int arp_anneal_first_accept_warm(const int32_t* Gt, const int32_t* h,
   a.m0 = m0;
   a.perm = perm;
   return launch_warm(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_anneal_tune(int D, int P, int policy, int precision, int warps) {
+  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || (policy != 0 && policy != 1) ||
+      (precision != 0 && precision != 1))
+    return ARP_ERR_SHAPE;
+  if (!(warps == 0 || warps == 1 || warps == 2 || warps == 4 || warps == 8)) return ARP_ERR_ARG;
+  g_tuned_warps[(D + 31) / 32][P][policy][precision] = warps;
+  return ARP_OK;
 }

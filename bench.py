@@ -235,6 +235,34 @@ def warm_vs_plain(args, dev, stream, rank):
     return out
 
 
+def mixed_batch(args, dev, rank):
+    """1 M detections (per rank) drawn uniformly over the 54 size classes users {8..64} x antennas {1, 1.5, 2} x
+    {QPSK, 16-QAM, 64-QAM}, SNR uniform 5-25 dB, plain MMSE-started Arpeggio at the picks' budgets with 32 anneals,
+    launch widths chosen by the autotuner, all classes in one captured CUDA graph on 8 forked streams."""
+    import torch
+    from arpeggio_b200 import mixed
+    total = args.mixed
+    counts = mixed.mixed_counts(total, seed=1 + rank)
+    mb = mixed.MixedBatch(counts, anneals=32, streams=8, device=dev)
+    mb.draw(7 + rank)
+    tuner = mixed.Autotuner()
+    t0 = time.time()
+    mb.tune(tuner)
+    tune_s = time.time() - t0
+    g = mb.capture(seed=3)
+    ms = mixed.timed_replay(g, reps=3)
+    mb.check()
+    out = {'value': total / (ms / 1e3), 'unit': 'detections/s', 'detections': total, 'classes': len(counts),
+           'ms_per_replay': ms, 'ber': mb.ber(), 'tune_seconds': tune_s,
+           'tuned_warps_per_block': {'D=%d' % k[0]: v['warps'] for k, v in tuner.table.items()},
+           'config': 'users {8,16,24,32,48,64} x antennas {1,1.5,2}x users x {QPSK,16-QAM,64-QAM}, SNR U[5,25] dB, '
+                     'MMSE-started Arpeggio first accept, 32 anneals, one CUDA graph (8 streams)'}
+    tuner.reset()
+    del g, mb
+    torch.cuda.empty_cache()
+    return out
+
+
 SERVE_CLASSES = [(8, 16, 4), (16, 16, 16), (24, 36, 64), (32, 32, 16), (48, 72, 4), (64, 64, 16)]
 
 
@@ -447,6 +475,7 @@ def run_ours(args):
     if args.warm_train > 0:
         warm_line = warm_vs_plain(args, dev, stream, rank)
     serve_line = serving(args, dev, rank) if args.serve else None
+    mixed_line = mixed_batch(args, dev, rank) if args.mixed > 0 else None
 
     # ---- integer-issue peak (calibration kernel) and the anneal kernel's algorithmic work
     L = _lib.lib()
@@ -510,6 +539,7 @@ def run_ours(args):
         'mdi_x16': mdi_line,
         'warm_vs_plain': warm_line,
         'serving': serve_line,
+        'mixed': mixed_line,
         'extra': extra,
         'gpu_launches': 3 * K,
         'clocks': ck,
@@ -565,6 +595,7 @@ def main():
     ap.add_argument('--mdi-batch', type=int, default=16384, help='uses of the multi-stage (MDI) line; 0 skips it')
     ap.add_argument('--no-extras', dest='extras', action='store_false', help='skip the Chord and 64-user lines')
     ap.add_argument('--no-serve', dest='serve', action='store_false', help='skip the serving-loop block')
+    ap.add_argument('--mixed', type=int, default=1_000_000, help='detections of the mixed-size graph block; 0 skips')
     ap.add_argument('--warm-train', type=int, default=2_000_000,
                     help='training instances of the warm-start MLP for the warm-vs-plain block; 0 skips it')
     args = ap.parse_args()

@@ -175,6 +175,12 @@ int arp_mdi_update(const float* H, const float* y, const int32_t* idx, int n, in
 int arp_mdi_select(const int8_t* cur, const float* dist, int B, int D, int G, int M, int8_t* levels, int8_t* bits,
                    void* stream);
 
+/* Autotuner hook (no reference counterpart): warps per block (1, 2, 4 or 8; 0 restores the occupancy heuristic)
+ * of the compressed-problem anneal kernels for problems of D coordinates (by 32-wide slot count), P copies,
+ * policy (0 first accept, incl. the warm variant; 1 Chord round) and precision (0 int32, 1 FP32 fields).
+ * Process-wide; results do not depend on it (anneals are independent of their block). */
+int arp_anneal_tune(int D, int P, int policy, int precision, int warps);
+
 /* ---- Learned warm start for first-accept annealing.  No counterpart in the reference, which has no learned
  * component: a per-coordinate MLP (16 features -> 512 -> 512 -> P+1 logits over the coordinate's spin sum
  * m_j = 2c - P, BF16 weights and activations, FP32 accumulate) emits the start state and the flip-test order.

@@ -1,0 +1,111 @@
+"""CPU checks of the warm-start oracle and of the serving / mixed-batch host logic (no GPU): the oracle's MLP
+gradients against finite differences of its own loss, the warm anneal of an identity order and zero start
+against the plain 'bal' anneal, a relabelled problem against the same problem, the warm start's fallback rule,
+and the admission arithmetic of the server."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def _mlp(seed, scale=0.3):
+    r = np.random.default_rng(seed)
+    return {'W1': r.normal(0, scale, (O.NH, O.NF)).astype(np.float32), 'b1': r.normal(0, 0.1, O.NH).astype(np.float32),
+            'W2': r.normal(0, scale / 8, (O.NH, O.NH)).astype(np.float32),
+            'b2': r.normal(0, 0.1, O.NH).astype(np.float32),
+            'W3t': r.normal(0, scale / 8, (O.NH, O.NO)).astype(np.float32),
+            'b3': r.normal(0, 0.1, O.NO).astype(np.float32)}
+
+
+def _loss64(X, lab, p, C=3):
+    """The same loss in float64 without bf16 roundings (the quantity the gradients differentiate)."""
+    H1 = np.maximum(X @ p['W1'].T.astype(np.float64) + p['b1'], 0)
+    H2 = np.maximum(H1 @ p['W2'].T.astype(np.float64) + p['b2'], 0)
+    Z = (H2 @ p['W3t'].astype(np.float64) + p['b3'])[:, :C]
+    zm = Z.max(1, keepdims=True)
+    lse = np.log(np.exp(Z - zm).sum(1)) + zm[:, 0]
+    v = lab >= 0
+    return float((lse - Z[np.arange(len(lab)), np.maximum(lab, 0)])[v].sum())
+
+
+def test_oracle_mlp_gradients_match_finite_differences():
+    r = np.random.default_rng(0)
+    X = O.bf16(r.normal(0, 1, (24, O.NF)).astype(np.float32))
+    lab = r.integers(-1, 3, 24)
+    p = {k: O.bf16(v) for k, v in _mlp(1).items()}
+    H1, H2, Z = O.mlp_forward(X, p['W1'], p['b1'], p['W2'], p['b2'], p['W3t'], p['b3'])
+    g = O.mlp_backward(X, lab, 3, p['W1'], p['W2'], p['W3t'], H1, H2, Z)
+    pd = {k: v.astype(np.float64) for k, v in p.items()}
+    eps = 1e-4
+    for name, idx in (('b3', (1,)), ('W3t', (5, 2)), ('b2', (7,)), ('W2', (3, 11)), ('W1', (9, 4)), ('b1', (2,))):
+        hi, lo = {k: v.copy() for k, v in pd.items()}, {k: v.copy() for k, v in pd.items()}
+        hi[name][idx] += eps
+        lo[name][idx] -= eps
+        fd = (_loss64(X, lab, hi) - _loss64(X, lab, lo)) / (2 * eps)
+        # the oracle keeps the device's bf16 roundings of dZ and the hidden activations: agreement to ~1 %
+        assert abs(g[name][idx] - fd) <= 0.02 * abs(fd) + 2e-3, (name, g[name][idx], fd)
+
+
+def _problem(B, D, seed):
+    r = np.random.default_rng(seed)
+    A = r.normal(0, 1, (B, D, D))
+    G = np.round(np.einsum('bij,bkj->bik', A, A) / D * 600).astype(np.int32)
+    h = np.round(r.normal(0, 800, (B, D))).astype(np.int32)
+    return G, h
+
+
+def test_oracle_warm_anneal_identity_is_the_bal_anneal():
+    G, h = _problem(6, 40, 2)
+    T = [400] * 16
+    s0, de0, st0 = O.anneal_dd(G, h, 2, 4, T, 0, np.arange(6), 99, 'bal')
+    s1, de1, st1 = O.anneal_dd_warm(G, h, 2, 4, T, 0, np.arange(6), 99, np.zeros((6, 40), np.int8),
+                                    np.tile(np.arange(40, dtype=np.uint8), (6, 1)))
+    assert np.array_equal(s0, s1) and np.array_equal(de0, de1) and np.array_equal(st0, st1)
+
+
+def test_oracle_warm_anneal_is_the_anneal_of_the_relabelled_problem():
+    G, h = _problem(4, 33, 3)
+    T = [300] * 12
+    r = np.random.default_rng(4)
+    perm = np.stack([r.permutation(33) for _ in range(4)]).astype(np.uint8)
+    m0 = (2 * r.integers(-1, 2, (4, 33))).astype(np.int8)
+    s, de, st = O.anneal_dd_warm(G, h, 2, 3, T, 0, np.arange(4), 7, m0, perm)
+    # relabel by hand and anneal with the identity order: the same trajectories, spins relabelled back
+    bi = np.arange(4)[:, None]
+    Gp = G[bi[:, :, None], perm[:, :, None].astype(np.int64), perm[:, None, :].astype(np.int64)]
+    hp = h[bi, perm.astype(np.int64)]
+    mp = m0[bi, perm.astype(np.int64)]
+    ident = np.tile(np.arange(33, dtype=np.uint8), (4, 1))
+    s2, de2, st2 = O.anneal_dd_warm(Gp, hp, 2, 3, T, 0, np.arange(4), 7, mp, ident)
+    assert np.array_equal(de, de2) and np.array_equal(st, st2)
+    s2 = s2.reshape(4, 3, 2, 33)
+    back = np.empty_like(s2)
+    for b in range(4):
+        back[b][..., perm[b].astype(np.int64)] = s2[b]
+    assert np.array_equal(s, back.reshape(4, 3, 66))
+
+
+def test_oracle_warm_start_falls_back_when_worse_than_the_guess():
+    G, h = _problem(3, 16, 5)
+    logits = np.zeros((3 * 16, 16), np.float32)
+    logits[:, 2] = 5.0  # every coordinate up by one level step
+    xq = np.full((3, 16), -1, np.int8)
+    h = -np.abs(h)  # the guess is a strict minimiser along +moves: moving up costs energy
+    m0, perm, e0, kept = O.warm_start(logits, G, h, xq, 2, 16)
+    assert (kept == 0).all() and (m0 == 0).all() and (e0 == 0).all()
+    assert np.array_equal(perm, np.tile(np.arange(16, dtype=np.uint8), (3, 1)))
+    m0, perm, e0, kept = O.warm_start(logits, G, -h, xq, 2, 16)  # now the move is downhill along h
+    assert kept.dtype == np.int32
+
+
+def test_serving_admission_and_mixed_classes():
+    from arpeggio_b200 import mixed, serve
+    cls = mixed.mixed_classes()
+    assert len(cls) == 54 and (64, 128, 64) in cls and (8, 12, 4) in cls
+    n = mixed.mixed_counts(1_000_000, seed=1)
+    assert sum(n.values()) == 1_000_000
+    # every class of the mix fits the kernels' shared memory; a 96-user class does not (D > 128)
+    assert all(serve.shared_bytes(c, 32) <= 227 * 1024 for c in cls)
+    assert serve.shared_bytes((64, 128, 16), 32) > serve.shared_bytes((64, 64, 16), 32)
+    arrivals = serve.poisson_arrivals(10000, 1e5, np.random.default_rng(0))
+    assert np.all(np.diff(arrivals) > 0) and abs(arrivals[-1] - 0.1) < 0.01

@@ -18,6 +18,8 @@ Fixtures (all small, numpy .npz):
                       as softlib.detect_llr) on fixed spin sets.
   golden_a513_b0.npz  batch 0 of the recorded B200 runs data/results/a513_fixed/{x16,x32}: per-use bit
                       errors, anneals per use, per-K [flips, tests, anneals] (`... /root/reference a513`).
+  golden_a513_points.npz  every recorded batch's per-use bit errors at the three recorded points
+                      (x16 20 dB, x32 22 dB, x64 22 dB) for the BER-inside-CI gate (`... /root/reference a513_points`).
   golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
                       (sim/a56an.py:74-108) on seeded per-use error vectors (`... /root/reference stats`).
 """
@@ -215,6 +217,30 @@ def a513_fixture():
     np.savez_compressed(os.path.join(OUT, 'golden_a513_b0.npz'), **out)
 
 
+def a513_points_fixture():
+    """Every recorded batch of the three recorded B200 points (data/results/a513_fixed/{x16,x32,x64}): the per-use
+    bit errors, for the gate "BER inside the reference's bootstrap CI" on the same draws."""
+    import glob
+    import json
+    pts = {'x16': ('x16/arpeggiofx_64_0.1_0.1_0_rand_32/snr_20.00', 16, 20.0, 102, 'abl_far_64_0.1_0.1_0_rand_32'),
+           'x32': ('x32/arpeggiofx_32_0.1_0.1_0_rand_8/snr_22.00', 32, 22.0, 102, 'abl_far_32_0.1_0.1_0_rand_8'),
+           'x64': ('x64/arpeggiofx_64_0.1_0.1_0_bal_8/snr_22.00', 64, 22.0, 344, 'abl_far_64_0.1_0.1_0_bal_8')}
+    out = {}
+    for tag, (rel, nt, snr, seed, pick) in pts.items():
+        files = sorted(glob.glob(os.path.join(REF, 'data/results/a513_fixed', rel, 'b*.npz')))
+        be = []
+        for i, f in enumerate(files):
+            assert os.path.basename(f) == 'b%05d.npz' % i
+            z = np.load(f)
+            be.append(z['biterr'].astype(np.uint8))
+        m = int(json.loads(str(np.load(files[0])['info']))['m'])
+        out[tag + '/biterr'] = np.stack(be)  # (batches, uses)
+        out[tag + '/meta'] = np.array([nt, snr, seed, m], dtype=np.float64)
+        out[tag + '/pick'] = np.array(pick)
+        print('a513 points', tag, len(files), 'batches', int(out[tag + '/biterr'].sum()), 'bit errors')
+    np.savez_compressed(os.path.join(OUT, 'golden_a513_points.npz'), **out)
+
+
 def stats_fixture():
     """stats_chord.boot_ber, a56an.boot_ratio and a56an.mcnemar on seeded per-use error vectors."""
     import importlib.util
@@ -239,9 +265,11 @@ def stats_fixture():
 
 if __name__ == '__main__':
     if len(sys.argv) > 2:
-        {'stats': stats_fixture, 'a513': a513_fixture, 'mapping': mapping_fixture}[sys.argv[2]]()
+        {'stats': stats_fixture, 'a513': a513_fixture, 'mapping': mapping_fixture,
+         'a513_points': a513_points_fixture}[sys.argv[2]]()
         sys.exit(0)
     a513_fixture()
+    a513_points_fixture()
     stats_fixture()
     philox_fixture()
     arpeggio_fixture()

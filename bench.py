@@ -263,6 +263,68 @@ def mixed_batch(args, dev, rank):
     return out
 
 
+def equal_budget(args, dev, rank, nt=64, snrs=tuple(range(10, 25, 2)), R=64):
+    """Both flip policies at equal modelled cycle budgets (the reference's model F: steps or tests plus flips per
+    anneal) at 64 users x 64 antennas 16-QAM: default Chord (128 steps per copy pair, T 0.3, q 0.4, random start)
+    sets the budget; Arpeggio (MMSE start, T 0.1, q 0) takes the largest sweep count whose cost stays within it,
+    chosen on the first 2048 uses; then both detect the whole batch (one-stage dDI, int32 fields)."""
+    import torch
+    from arpeggio_b200 import channel, detector, stats
+    B = max(2048, args.batch // 4)
+    snr = torch.tensor([float(snrs[i % len(snrs)]) for i in range(B)])
+    d = channel.draw_device(6000 + rank, snr, B, nt, 16, dev=dev)
+    bt = channel.levels_to_bits(d['l'], 16)
+
+    def make(policy, n, sweeps=None):
+        det = (detector.Detector(n, nt, nt, 16, 'chord', R, 1, precision='int', device=dev) if policy == 'chord' else
+               detector.Detector(n, nt, nt, 16, 'arpeggio', R, 1, sweeps=sweeps, T0=0.1, T1=0.1, q=0.0, start='bal',
+                                 precision='int', device=dev))
+        det.set_noise(N0=d['N0'][:n])
+        return det
+
+    def cost(det):
+        st = det.st.double()
+        return float((st[..., 0] + st[..., 1]).mean())  # flips + (steps | tests) per anneal
+    nt_ = 2048
+    ch = make('chord', nt_)
+    ch.run(d['H'][:nt_], d['y'][:nt_], seed=1)
+    torch.cuda.synchronize()
+    budget = cost(ch)
+    grid, xs = (8, 12, 16, 24, 32, 48, 64, 96, 128), {}
+    for S in grid:
+        a = make('arpeggio', nt_, S)
+        a.run(d['H'][:nt_], d['y'][:nt_], seed=1)
+        torch.cuda.synchronize()
+        xs[S] = cost(a) / budget
+    ok = [S for S in grid if xs[S] <= 1.0]
+    S_star = max(ok) if ok else grid[0]
+    out = {'users': nt, 'uses': B, 'anneals': R, 'chord_cost_per_anneal': budget,
+           'arpeggio_cost_ratio_by_sweeps': xs, 'arpeggio_sweeps': S_star}
+    errs = {}
+    for name, det in (('chord', make('chord', B)), ('arpeggio', make('arpeggio', B, S_star))):
+        det.run(d['H'], d['y'], seed=2)
+        torch.cuda.synchronize()
+        x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        x0.record()
+        for i in range(2):
+            det.run(d['H'], d['y'], seed=3 + i)
+        x1.record()
+        torch.cuda.synchronize()
+        det.check()
+        e = (det.bits != bt).sum(-1).cpu().numpy()
+        errs[name] = e
+        sn = snr.numpy()
+        out[name] = {'value': B / (x0.elapsed_time(x1) / 2 / 1e3), 'unit': 'detections/s',
+                     'cost_per_anneal': cost(det),
+                     'ber': {'%d dB' % v: float(e[sn == v].sum()) / ((sn == v).sum() * bt.shape[1]) for v in snrs}}
+        del det
+    sn = snr.numpy()
+    out['ber_ratio_arpeggio_vs_chord'] = {'%d dB' % v: list(stats.boot_ratio(errs['arpeggio'][sn == v],
+                                                                             errs['chord'][sn == v], B=1000))
+                                          for v in snrs}
+    return out
+
+
 SERVE_CLASSES = [(8, 16, 4), (16, 16, 16), (24, 36, 64), (32, 32, 16), (48, 72, 4), (64, 64, 16)]
 
 
@@ -476,6 +538,7 @@ def run_ours(args):
         warm_line = warm_vs_plain(args, dev, stream, rank)
     serve_line = serving(args, dev, rank) if args.serve else None
     mixed_line = mixed_batch(args, dev, rank) if args.mixed > 0 else None
+    budget_line = equal_budget(args, dev, rank) if args.extras else None
 
     # ---- integer-issue peak (calibration kernel) and the anneal kernel's algorithmic work
     L = _lib.lib()
@@ -540,6 +603,7 @@ def run_ours(args):
         'warm_vs_plain': warm_line,
         'serving': serve_line,
         'mixed': mixed_line,
+        'equal_budget_x64': budget_line,
         'extra': extra,
         'gpu_launches': 3 * K,
         'clocks': ck,

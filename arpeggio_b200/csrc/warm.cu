@@ -266,6 +266,8 @@ __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G,
   if (b >= B) return;
   const GT* Gb = G + (size_t)b * D * D;
   float dg[4] = {0, 0, 0, 0}, ss[4] = {0, 0, 0, 0};
+  // the row loops carry no load dependence: unrolled so one warp keeps several rows of G in flight
+#pragma unroll 8
   for (int i = 0; i < D; ++i) {
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
@@ -305,25 +307,50 @@ __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G,
     };
 #pragma unroll
     for (int t = 0; t < 4; ++t) mq[t] = dg[t] > 0.0f ? quant(hv[t] / (4.0f * dg[t]), xv[t]) : 0;
+#pragma unroll
     for (int pass = 0; pass < 2; ++pass) {
       float acc[4] = {0, 0, 0, 0};
-      for (int i = 0; i < D; ++i) {
-        const int mi = __shfl_sync(0xffffffffu, mq[i >> 5], i & 31);
-        if (mi == 0) continue;
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int j = t * 32 + lane;
-          if (j < D && j != i) acc[t] = fmaf((float)Gb[(size_t)i * D + j], (float)mi, acc[t]);
+      for (int ti = 0; ti < 4; ++ti) {  // rows i = 32 ti + l with m_i != 0, in order, four loads in flight
+        if (ti * 32 >= D) break;
+        const int src = mq[ti];
+        uint32_t mk = __ballot_sync(0xffffffffu, src != 0);
+        while (mk) {
+          int li[4];
+          float g[4][4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            li[u] = mk ? __ffs(mk) - 1 : -1;
+            if (mk) mk &= mk - 1u;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+              const int j = t * 32 + lane;
+              g[u][t] = (li[u] >= 0 && j < D) ? (float)Gb[(size_t)(ti * 32 + li[u]) * D + j] : 0.0f;
+            }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (li[u] < 0) break;
+            const int i = ti * 32 + li[u];
+            const float mi = (float)__shfl_sync(0xffffffffu, src, li[u]);
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+              if (t * 32 + lane < D && t * 32 + lane != i) acc[t] = fmaf(g[u][t], mi, acc[t]);
+          }
         }
       }
-      float* u = pass == 0 ? u1 : u2;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const float v = dg[t] > 0.0f ? (hv[t] - 2.0f * acc[t]) / (4.0f * dg[t]) : 0.0f;
-        u[t] = fminf(fmaxf(v, -8.0f), 8.0f);
+        const float uc = fminf(fmaxf(v, -8.0f), 8.0f);
+        if (pass == 0)
+          u1[t] = uc;
+        else
+          u2[t] = uc;
+        mq[t] = (t * 32 + lane) < D && dg[t] > 0.0f ? quant(uc, xv[t]) : 0;
       }
-#pragma unroll
-      for (int t = 0; t < 4; ++t) mq[t] = (t * 32 + lane) < D && dg[t] > 0.0f ? quant(u[t], xv[t]) : 0;
     }
   }
   const float snr = snr_db ? snr_db[b] * 0.05f : 0.0f;
@@ -485,13 +512,34 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
   // start energy m^T G m - h^T m
   ET e = ET(0);
   const GT* Gb = G + (size_t)b * D * D;
-  for (int i = 0; i < D; ++i) {
-    const int mi = __shfl_sync(0xffffffffu, mv[i >> 5], i & 31);
-    if (mi == 0) continue;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int j = t * 32 + lane;
-      if (j < D && mv[t] != 0) e += (ET)Gb[(size_t)i * D + j] * (ET)(mi * mv[t]);
+  for (int ti = 0; ti < 4; ++ti) {  // rows with m_i != 0 only, four loads in flight
+    if (ti * 32 >= D) break;
+    const int src = mv[ti];
+    uint32_t mk = __ballot_sync(0xffffffffu, src != 0);
+    while (mk) {
+      int li[4];
+      GT g[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        li[u] = mk ? __ffs(mk) - 1 : -1;
+        if (mk) mk &= mk - 1u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int j = t * 32 + lane;
+          g[u][t] = (li[u] >= 0 && j < D) ? Gb[(size_t)(ti * 32 + li[u]) * D + j] : GT(0);
+        }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (li[u] < 0) break;
+        const int mi = __shfl_sync(0xffffffffu, src, li[u]);
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if (t * 32 + lane < D) e += (ET)g[u][t] * (ET)(mi * mv[t]);
+      }
     }
   }
 #pragma unroll
@@ -505,12 +553,20 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
   const bool keep = e <= ET(0);
   // ranks by descending score
   int rk[4] = {0, 0, 0, 0};
-  for (int i = 0; i < D; ++i) {
-    const float si = __shfl_sync(0xffffffffu, sc[i >> 5], i & 31);
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int j = t * 32 + lane;
-      if (si > sc[t] || (si == sc[t] && i < j)) ++rk[t];
+  for (int ti = 0; ti < 4; ++ti) {
+    if (ti * 32 >= D) break;
+    const float src = sc[ti];
+    const int nl = min(32, D - ti * 32);
+#pragma unroll 8
+    for (int l = 0; l < nl; ++l) {
+      const int i = ti * 32 + l;
+      const float si = __shfl_sync(0xffffffffu, src, l);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int j = t * 32 + lane;
+        if (si > sc[t] || (si == sc[t] && i < j)) ++rk[t];
+      }
     }
   }
 #pragma unroll

@@ -115,8 +115,12 @@ class Detector:
         self.sigma2 = torch.empty(B, dtype=torch.float32, device=dev)
         self.inst = torch.empty(B, dtype=torch.int32, device=dev)
         self.levels = torch.empty(B, D, dtype=torch.int8, device=dev)
-        self.bits = torch.empty(B, D * PAM[M]['bits'], dtype=torch.int8, device=dev)
-        self.dist = torch.empty(B, dtype=torch.float32, device=dev)
+        # bits and distances side by side in one allocation, so a frame's results leave in one copy
+        nb = B * D * PAM[M]['bits']
+        self._out_off = -(-nb // 16) * 16
+        self._out = torch.empty(self._out_off + 4 * B, dtype=torch.uint8, device=dev)
+        self.bits = self._out[:nb].view(torch.int8).view(B, D * PAM[M]['bits'])
+        self.dist = self._out[self._out_off:].view(torch.float32)
         self.pick = torch.empty(B, dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self._inst_base = None
@@ -248,6 +252,23 @@ class Detector:
                 bits_out[a:b].copy_(bits, non_blocking=True)
                 dist_out[a:b].copy_(dist, non_blocking=True)
 
+    def frame_buffers(self):
+        """Buffers for captured frames: pinned host and device inputs with H and y side by side (one copy in) and a
+        pinned output mirroring the device's bits + distances (one copy out).  Returns
+        (Hh, yh, Hd, yd, bits_out, dist_out) for capture()."""
+        B, NR2, D = self.B, self.NR2, self.D
+        nH = B * NR2 * D
+        hin = torch.empty(nH + B * NR2, dtype=torch.float32).pin_memory()
+        din = torch.empty(nH + B * NR2, dtype=torch.float32, device=self.device)
+        hout = torch.empty(self._out.numel(), dtype=torch.uint8).pin_memory()
+        nb = self.bits.numel()
+        return (hin[:nH].view(B, NR2, D), hin[nH:].view(B, NR2), din[:nH].view(B, NR2, D), din[nH:].view(B, NR2),
+                hout[:nb].view(torch.int8).view(self.bits.shape), hout[self._out_off:].view(torch.float32))
+
+    @staticmethod
+    def _adjacent(a, b):
+        return a.is_contiguous() and b.is_contiguous() and b.data_ptr() == a.data_ptr() + a.numel() * a.element_size()
+
     def capture(self, Hh, yh, seed, bits_out, dist_out, Hd, yd):
         """A CUDA graph of one whole-batch detection from pinned host buffers: copy H, y in, detect, copy bits
         and distances out.  Replaying it re-runs the same seed on whatever the pinned inputs hold, with no host
@@ -263,13 +284,24 @@ class Detector:
                 self.run(Hd, yd, seed)
         torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
+        one_in = self._adjacent(Hh, yh) and self._adjacent(Hd, yd)
+        n_out = self._out_off + 4 * self.B
+        one_out = (bits_out.data_ptr() + self._out_off == dist_out.data_ptr() and bits_out.is_contiguous()
+                   and dist_out.numel() == self.B)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            Hd.copy_(Hh, non_blocking=True)
-            yd.copy_(yh, non_blocking=True)
+            if one_in:  # H and y side by side on both ends: one copy
+                n_in = Hh.numel() + yh.numel()
+                Hd.view(-1).as_strided((n_in,), (1,)).copy_(Hh.view(-1).as_strided((n_in,), (1,)), non_blocking=True)
+            else:
+                Hd.copy_(Hh, non_blocking=True)
+                yd.copy_(yh, non_blocking=True)
             bits, _, dist = self.run(Hd, yd, seed)
-            bits_out.copy_(bits, non_blocking=True)
-            dist_out.copy_(dist, non_blocking=True)
+            if one_out:
+                bits_out.view(-1).view(torch.uint8).as_strided((n_out,), (1,)).copy_(self._out, non_blocking=True)
+            else:
+                bits_out.copy_(bits, non_blocking=True)
+                dist_out.copy_(dist, non_blocking=True)
         return g
 
     def check(self):

@@ -266,3 +266,24 @@ def test_trained_network_beats_the_plain_start_at_the_same_budget():
         res[name] = (float(e.double().mean()), int((det.bits != bt).sum()))
     assert res['warm'][0] < res['plain'][0], res
     assert res['warm'][1] <= res['plain'][1] * 1.02, res
+
+
+@pytest.mark.parametrize('warm_start', [False, True])
+def test_frame_graph_with_one_copy_each_way_equals_run(warm_start):
+    """A captured frame whose H and y sit side by side (one copy in) and whose bits and distances leave in one copy
+    gives the detector's own results."""
+    from arpeggio_b200 import channel, warm
+    mlp = warm.WarmMLP(P=2, seed=2) if warm_start else None
+    f = channel.draw_device(31, 12.0, 4, 32, 16)
+    det = warm.WarmDetector(4, 32, anneals=16, sweeps=8, mlp=mlp)
+    det.set_noise(N0=f['N0'])
+    bits, _, dist = det.run(f['H'], f['y'], 5)
+    ref_bits, ref_dist = bits.clone(), dist.clone()
+    Hh, yh, Hd, yd, bo, do = det.frame_buffers()
+    Hh.copy_(f['H'].cpu())
+    yh.copy_(f['y'].cpu())
+    g = det.capture(Hh, yh, 5, bo, do, Hd, yd)
+    det.bits.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(bo, ref_bits.cpu()) and torch.equal(do, ref_dist.cpu())

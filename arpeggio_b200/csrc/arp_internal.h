@@ -28,6 +28,7 @@ struct DDParams {
   // (position j' of the scan tests coordinate perm[j']); null for the reference's starts and index order
   const int8_t* m0 = nullptr;
   const uint8_t* perm = nullptr;
+  int warm_r = 1 << 30;  // anneals r < warm_r start from m0; the others from the MMSE start (m = 0), same order
 };
 
 struct MapParams {

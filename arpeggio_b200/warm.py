@@ -191,12 +191,13 @@ class WarmDetector(Detector):
     that also records the features' inputs (used to make training labels)."""
 
     def __init__(self, B, nt, nr=None, M=16, anneals=32, sweeps=None, mlp=None, T0=None, T1=None, q=None,
-                 device='cuda'):
+                 device='cuda', warm_anneals=None):
         super().__init__(B, nt, nr, M, 'arpeggio', anneals, 1, sweeps=sweeps, T0=T0, T1=T1, q=q, start='bal',
                          precision='int', device=device)
         dev = self.device
         B, D = self.B, self.D
         self.mlp = mlp
+        self.warm_anneals = anneals if warm_anneals is None else warm_anneals  # the rest start from the guess
         self.zs = torch.empty(B, D, dtype=torch.float32, device=dev)
         self.X = torch.empty(B * D, NF, dtype=torch.bfloat16, device=dev)
         self.m0 = torch.zeros(B, D, dtype=torch.int8, device=dev)
@@ -260,9 +261,9 @@ class WarmDetector(Detector):
                                         _lib.ptr(self.m0[sl]), _lib.ptr(self.perm[sl]), _lib.ptr(self.e0[sl]),
                                         _lib.ptr(self.kept[sl]), sp), 'warm_start')
             ev(2 if e5 else 1)
-            rc = L.arp_anneal_first_accept_warm(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P, R, D,
-                                                n, _lib.ptr(inst), k0, k1, _lib.ptr(self.m0[sl]),
-                                                _lib.ptr(self.perm[sl]), *outs)
+            rc = L.arp_anneal_first_accept_warm_mix(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P, R,
+                                                    D, n, _lib.ptr(inst), k0, k1, _lib.ptr(self.m0[sl]),
+                                                    _lib.ptr(self.perm[sl]), int(self.warm_anneals), *outs)
         else:
             ev(2 if e5 else 1)
             rc = L.arp_anneal_first_accept(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P, R, D, n,

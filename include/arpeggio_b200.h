@@ -252,6 +252,14 @@ int arp_anneal_first_accept_warm(const int32_t* Gt, const int32_t* h, const int3
                                  const uint8_t* perm, int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status,
                                  void* stream);
 
+/* arp_anneal_first_accept_warm where only anneals r < warm_r start from m0 and the others from the MMSE start
+ * (m = 0, the 'bal' pattern), all in the given flip-test order: a mix of start diversity.  No counterpart in
+ * the reference. */
+int arp_anneal_first_accept_warm_mix(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P,
+                                     int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                                     const int8_t* m0, const uint8_t* perm, int warm_r, int8_t* out_s,
+                                     int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);
+
 /* arp_detect_dd without a workspace argument, for callers that cannot allocate device memory: a receive
  * chain with a hard per-frame latency budget cannot call cudaMalloc on the frame path (it synchronises the
  * device and takes unbounded time), and a plugin inside a host program that owns all device memory may not

@@ -127,6 +127,7 @@ typedef struct {
   int8_t* out_s;
   int64_t *out_de, *out_st;
   const int8_t* m0; /* start == 2: given spin sums (B, D) */
+  int warm_r;       /* start == 2: anneals r >= warm_r start from m = 0 */
 } dd_ctx;
 
 /* Start spins of one anneal (arpeggio_ref59.py:44-49, arpeggio_fx.cu:48-57). s is P x D. */
@@ -165,7 +166,9 @@ static void dd_job(void* vctx, long t) {
   uint8_t pf[6 * 128];
   int64_t w[128];
   uint8_t F[128];
-  start_spins(x->start, P, D, r, inst, x->k0, x->k1, x->m0 ? x->m0 + (size_t)b * D : NULL, s);
+  static const int8_t zeros[128] = {0};
+  start_spins(x->start, P, D, r, inst, x->k0, x->k1,
+              x->m0 ? ((int)r < x->warm_r ? x->m0 + (size_t)b * D : zeros) : NULL, s);
   memcpy(bs, s, (size_t)P * D);
   memset(pf, 0, sizeof pf);
   for (int i = 0; i < D; i++) { /* w_i = h_i - 2 sum_j G_ij m_j (arpeggio_ref59.py:50-51) */
@@ -244,18 +247,19 @@ int orc_anneal_dd(const int32_t* G, const int32_t* h, int B, int D, int P, int R
                   int policy, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
     return 1;
-  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL};
+  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL, 0};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }
 
-/* First accept from given spin sums m0 (B, D) (start 2 of start_spins); the caller permutes the problem into
- * scan order first (the device's flip-test order is a relabelling of the coordinates). */
+/* First accept from given spin sums m0 (B, D) (start 2 of start_spins) for anneals r < warm_r, from m = 0 for
+ * the others; the caller permutes the problem into scan order first (the device's flip-test order is a
+ * relabelling of the coordinates). */
 int orc_anneal_dd_warm(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T, int L,
-                       int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1, const int8_t* m0, int8_t* out_s,
-                       int64_t* out_de, int64_t* out_st, int nthreads) {
+                       int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1, const int8_t* m0, int warm_r,
+                       int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || L < 1 || R < 1 || B < 0 || !m0) return 1;
-  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0};
+  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0, warm_r};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }

@@ -466,7 +466,7 @@ def warm_start(logits, G, h, xq, P, M):
     return m0, perm, np.where(keep, e0, 0), keep.astype(np.int32)
 
 
-def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1):
+def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=None):
     """First accept from the given start in the given flip-test order: the problem relabelled into scan order
     (position j' = coordinate perm[j']), annealed from spin sums m0 with the 'bal' pattern where m0 = 0, and the
     spins relabelled back."""
@@ -485,9 +485,11 @@ def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1):
     out_st = np.zeros((B, R, 2), dtype=np.int64)
     L = lib()
     L.orc_anneal_dd_warm.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int,
-                                     ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_int]
+                                     ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_int, _P, _P, _P,
+                                     ctypes.c_int]
     rc = L.orc_anneal_dd_warm(_ptr(Gp), _ptr(hp), B, D, P, R, _ptr(T), len(T), int(q), _ptr(it), key & MASK,
-                              (key >> 32) & MASK, _ptr(mp), _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+                              (key >> 32) & MASK, _ptr(mp), R if warm_r is None else int(warm_r), _ptr(out_s),
+                              _ptr(out_de), _ptr(out_st), nthreads)
     if rc:
         raise ValueError('orc_anneal_dd_warm: unsupported shape')
     s = out_s.reshape(B, R, P, D)

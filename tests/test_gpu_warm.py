@@ -287,3 +287,31 @@ def test_frame_graph_with_one_copy_each_way_equals_run(warm_start):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(bo, ref_bits.cpu()) and torch.equal(do, ref_dist.cpu())
+
+
+def test_warm_start_mix_matches_oracle():
+    """Only anneals r < warm_r start from the given spin sums; the rest start from the MMSE guess in the same
+    order: bit-exact against the oracle."""
+    from arpeggio_b200 import _lib
+    d, det = _problems(48, 32, 15.0, 8)
+    g = np.random.default_rng(9)
+    m0 = (2 * g.integers(-1, 2, size=(48, 64))).astype(np.int8)
+    perm = np.stack([g.permutation(64) for _ in range(48)]).astype(np.uint8)
+    m0d, pd = torch.from_numpy(m0).cuda(), torch.from_numpy(perm).cuda()
+    T = det.schedule['T']
+    Tt = torch.tensor(T, dtype=torch.int32, device='cuda')
+    inst = torch.arange(48, dtype=torch.int32, device='cuda')
+    so = torch.empty(48, 8, 128, dtype=torch.int8, device='cuda')
+    deo = torch.empty(48, 8, dtype=torch.int64, device='cuda')
+    sto = torch.empty(48, 8, 2, dtype=torch.int64, device='cuda')
+    stat = torch.zeros(1, dtype=torch.int32, device='cuda')
+    for wr in (0, 3, 8):
+        _lib.check(_lib.lib().arp_anneal_first_accept_warm_mix(
+            _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(Tt), len(T), 0, 2, 8, 64, 48, _lib.ptr(inst), 99, 1,
+            _lib.ptr(m0d), _lib.ptr(pd), wr, _lib.ptr(so), _lib.ptr(deo), _lib.ptr(sto), _lib.ptr(stat),
+            _lib.stream_ptr()), 'warm mix')
+        torch.cuda.synchronize()
+        s, de, st = O.anneal_dd_warm(det.G.cpu().numpy(), det.h.cpu().numpy(), 2, 8, T, 0, np.arange(48),
+                                     99 | (1 << 32), m0, perm, nthreads=NTH, warm_r=wr)
+        assert np.array_equal(so.cpu().numpy(), s) and np.array_equal(deo.cpu().numpy(), de), wr
+        assert np.array_equal(sto.cpu().numpy(), st), wr

@@ -88,22 +88,11 @@ class WarmMLP:
             self._train = True
         self._rows = rows
 
-    def scratch(self, rows):
-        """Activation buffers for inference on up to `rows` rows, owned by the caller (one per concurrent stream)."""
-        rows = -(-rows // 128) * 128
-        dev, b16 = self.device, torch.bfloat16
-        return {'H1': torch.empty(rows, NH, dtype=b16, device=dev), 'H2': torch.empty(rows, NH, dtype=b16, device=dev),
-                'Z': torch.empty(rows, NO, dtype=torch.float32, device=dev)}
-
-    def forward(self, X, rows, stream=None, scratch=None):
-        """logits (rows, 16) float32 of features X (rows, 16) bf16; stream-ordered and allocation-free, in the
-        network's own buffers (after reserve) or in `scratch` (from self.scratch)."""
-        if scratch is None:
-            self.reserve(rows)
-            scratch = {'H1': self.H1, 'H2': self.H2, 'Z': self.Z}
-        H1, H2, Z = scratch['H1'], scratch['H2'], scratch['Z']
-        if H1.shape[0] < rows:
-            raise ValueError('scratch holds %d rows, %d requested' % (H1.shape[0], rows))
+    def forward(self, X, rows, stream=None):
+        """logits (rows, 16) float32 of features X (rows, 16) bf16, layer by layer with the hidden activations
+        kept for backward (the training path); stream-ordered and allocation-free after reserve."""
+        self.reserve(rows)
+        H1, H2, Z = self.H1, self.H2, self.Z
         wb, st = self.wb, self.status
         gemm(X, 0, NF, self.view(wb, 'W1'), 0, NF, rows, NH, NF, EPI_RELU_BF16, H1, NH,
              bias=self.view(self.w, 'b1'), status=st, stream=stream)

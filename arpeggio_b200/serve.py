@@ -9,6 +9,8 @@ and request ids.  The server keeps, per class, `inflight` lanes -- a preallocate
     slot count (slots are fixed by the HBM budget at construction; a class is accepted only if its kernels'
     shared memory fits), copies their H, y and noise in, detects, copies bits and distances out and records
     an event -- all on the lane's stream, so batches of one class and of different classes overlap on the GPU;
+    a batch of at most GRAPH_MAX uses is staged into the lane's pinned buffers and replays a graph captured at
+    construction for the next power-of-two size (one launch; the padding uses are detected and discarded);
   * completion: a lane whose event has completed hands its results to the requests' rows of the class's
     output arrays and becomes free; each request's latency is completion time minus arrival time.
 
@@ -25,8 +27,11 @@ from .detector import PAM, el2
 from .warm import NF, NO, WarmDetector
 
 
+GRAPH_MAX = 64  # batches of up to this many uses replay a captured graph (one launch instead of ~15)
+
+
 class _Lane:
-    def __init__(self, cls, slots, anneals, sweeps, mlp, device):
+    def __init__(self, cls, slots, anneals, sweeps, mlp, device, key):
         nt, nr, M = cls
         self.det = WarmDetector(slots, nt, nr, M, anneals=anneals, sweeps=sweeps, mlp=mlp, device=device)
         self.stream = torch.cuda.Stream(device=device)
@@ -34,7 +39,46 @@ class _Lane:
         self.yd = torch.empty(slots, 2 * nr, dtype=torch.float32, device=device)
         self.instd = torch.empty(slots, dtype=torch.int32, device=device)
         self.done = torch.cuda.Event()
-        self.busy = None  # (first, last) rows of the class stream in flight
+        self.busy = None  # (first, last, graph bucket or 0) rows of the class stream in flight
+        self.key = key
+        # small batches: fixed pinned staging and one captured graph per power-of-two size
+        g = min(GRAPH_MAX, slots)
+        self.Hh = torch.empty(g, 2 * nr, 2 * nt, dtype=torch.float32).pin_memory()
+        self.yh = torch.empty(g, 2 * nr, dtype=torch.float32).pin_memory()
+        self.insth = torch.empty(g, dtype=torch.int32).pin_memory()
+        self.s2h = torch.zeros(g, dtype=torch.float32).pin_memory()
+        self.snrh = torch.zeros(g, dtype=torch.float32).pin_memory()
+        self.bitsh = torch.empty(g, self.det.bits.shape[1], dtype=torch.int8).pin_memory()
+        self.disth = torch.empty(g, dtype=torch.float32).pin_memory()
+        self.graphs = {}
+        kb = 1
+        while kb <= g:
+            self.graphs[kb] = self._capture(kb)
+            kb *= 2
+
+    def _body(self, kb):
+        det = self.det
+        self.Hd[:kb].copy_(self.Hh[:kb], non_blocking=True)
+        self.yd[:kb].copy_(self.yh[:kb], non_blocking=True)
+        self.instd[:kb].copy_(self.insth[:kb], non_blocking=True)
+        det.sigma2[:kb].copy_(self.s2h[:kb], non_blocking=True)
+        det.snr_db[:kb].copy_(self.snrh[:kb], non_blocking=True)
+        bits, _, dist = det.run(self.Hd[:kb], self.yd[:kb], self.key, n=kb, inst=self.instd[:kb])
+        self.bitsh[:kb].copy_(bits, non_blocking=True)
+        self.disth[:kb].copy_(dist, non_blocking=True)
+
+    def _capture(self, kb):
+        self.Hh[:kb].zero_()
+        self.yh[:kb].zero_()
+        self.insth[:kb].zero_()
+        self.s2h[:kb].fill_(1.0)
+        with torch.cuda.stream(self.stream):
+            self._body(kb)  # settles launch widths and kernel attributes outside the capture
+        self.stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream):
+            self._body(kb)
+        return g
 
 
 def shared_bytes(cls, anneals):
@@ -80,7 +124,7 @@ class Server:
             while cap > 1 and inflight * lane_bytes(cls, cap, anneals, mlp is not None) > share:
                 cap //= 2
             self.slots[cls] = cap
-            self.lanes[cls] = [_Lane(cls, cap, anneals, sweeps, mlp, self.device) for _ in range(inflight)]
+            self.lanes[cls] = [_Lane(cls, cap, anneals, sweeps, mlp, self.device, self.key) for _ in range(inflight)]
         self.streams = {}
 
     def open(self, cls, H, y, N0, t_arrival, rid):
@@ -102,6 +146,20 @@ class Server:
 
     def _launch(self, cls, lane, a, b):
         st, det, k = self.streams[cls], lane.det, b - a
+        if k <= len(lane.Hh):
+            # small batch: stage into the lane's pinned buffers, replay the graph of the next power of two
+            kb = 1 << (k - 1).bit_length()
+            lane.Hh[:k].copy_(st['H'][a:b])
+            lane.yh[:k].copy_(st['y'][a:b])
+            lane.insth[:k].copy_(st['rid_t'][a:b])
+            lane.s2h[:k].copy_(st['s2'][a:b])
+            lane.snrh[:k].copy_(st['snr'][a:b])
+            with torch.cuda.stream(lane.stream):
+                lane.graphs[kb].replay()
+            lane.done.record(lane.stream)
+            lane.busy = (a, b, kb)
+            st['batches'] += 1
+            return
         with torch.cuda.stream(lane.stream):
             lane.Hd[:k].copy_(st['H'][a:b], non_blocking=True)
             lane.yd[:k].copy_(st['y'][a:b], non_blocking=True)
@@ -113,7 +171,7 @@ class Server:
             st['bits'][a:b].copy_(bits, non_blocking=True)
             st['dist'][a:b].copy_(dist, non_blocking=True)
         lane.done.record(lane.stream)
-        lane.busy = (a, b)
+        lane.busy = (a, b, 0)
         st['batches'] += 1
 
     def step(self, now):
@@ -126,7 +184,10 @@ class Server:
                 continue
             for lane in lanes:
                 if lane.busy is not None and lane.done.query():
-                    a, b = lane.busy
+                    a, b, kb = lane.busy
+                    if kb:  # results of a graph batch arrive in the lane's pinned staging
+                        st['bits'][a:b].copy_(lane.bitsh[:b - a])
+                        st['dist'][a:b].copy_(lane.disth[:b - a])
                     st['done'][a:b] = now
                     lane.busy = None
             arrived = int(np.searchsorted(st['t'], now, side='right'))

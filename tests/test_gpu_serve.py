@@ -9,25 +9,27 @@ pytestmark = pytest.mark.gpu
 CLASSES = [(8, 16, 4), (24, 36, 64), (32, 32, 16)]
 
 
-def _streams(n, seed):
+def _streams(n, seed, burst=False):
     from arpeggio_b200 import channel, serve
     rng = np.random.default_rng(seed)
     out = {}
     for ci, (nt, nr, M) in enumerate(CLASSES):
         snr = torch.tensor(rng.uniform(5, 25, n), dtype=torch.float32)
         d = channel.draw_device(seed * 10 + ci, snr, n, nt, M, nr=nr, dev='cpu')
-        t = serve.poisson_arrivals(n, 2e4, rng)
+        t = np.zeros(n) if burst else serve.poisson_arrivals(n, 2e4, rng)
         rid = 1000 * (ci + 1) + np.arange(n)
         out[(nt, nr, M)] = (d['H'].pin_memory(), d['y'].pin_memory(), d['N0'], t, rid)
     return out
 
 
-@pytest.mark.parametrize('warm_start', [False, True])
-def test_each_result_is_the_same_alone_and_in_the_mix(warm_start):
+@pytest.mark.parametrize('warm_start,slots,burst', [(False, 64, False), (True, 64, False), (False, 256, True)])
+def test_each_result_is_the_same_alone_and_in_the_mix(warm_start, slots, burst):
+    """Poisson arrivals (small batches: captured graphs) or one burst (a 256-use batch on the direct path, then
+    the rest)."""
     from arpeggio_b200 import serve, warm
     mlp = warm.WarmMLP(P=2, seed=3) if warm_start else None
-    srv = serve.Server(CLASSES, mlp=mlp, anneals=8, sweeps=8, slots=64, inflight=2, hbm_budget=1 << 30)
-    streams = _streams(300, 5)
+    srv = serve.Server(CLASSES, mlp=mlp, anneals=8, sweeps=8, slots=slots, inflight=2, hbm_budget=1 << 30)
+    streams = _streams(300, 5, burst)
     for cls, (H, y, N0, t, rid) in streams.items():
         srv.open(cls, H, y, N0, t, rid)
     stats = srv.serve()

@@ -3,7 +3,6 @@ gradients against finite differences of its own loss, the warm anneal of an iden
 against the plain 'bal' anneal, a relabelled problem against the same problem, the warm start's fallback rule,
 and the admission arithmetic of the server."""
 import numpy as np
-import pytest
 
 from oracle import oracle as O
 

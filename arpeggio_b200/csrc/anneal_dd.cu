@@ -407,7 +407,15 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
         const int j = t * 32 + lane;
         uint32_t c0 = 0xFFFFFFFFu, c1 = (uint32_t)j, c2 = (uint32_t)r, c3 = inst;
         philox10(c0, c1, c2, c3, K);
-        int mv = (j < D && r < a.warm_r) ? a.m0[(size_t)b * D + s_perm[j]] : 0;
+        int mv = 0;
+        if (j < D && r < a.warm_r) {
+          if (a.cdf && r > 0) {  // a sampled start: the position's own draw against the coordinate's thresholds
+            const uint2 th = reinterpret_cast<const uint2*>(a.cdf)[(size_t)b * D + s_perm[j]];
+            mv = c1 < th.x ? -2 : (c1 > th.y ? 2 : 0);
+          } else {
+            mv = a.m0[(size_t)b * D + s_perm[j]];
+          }
+        }
         mv = mv < -P ? -P : (mv > P ? P : mv);
         const int pat = mv == 0 ? bal_pattern(P, (uint32_t)(((uint64_t)c0 * (uint64_t)bal_choose(P)) >> 32))
                                 : (1 << ((mv + P) >> 1)) - 1;
@@ -746,6 +754,23 @@ extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, co
   DDParams a{Gt, h, T, c, L, 0, q, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
   cudaError_t e = anneal_dispatch(policy, true, a, P, default_warps(R), (cudaStream_t)stream);
   return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
+extern "C" int arp_anneal_first_accept_warm_sampled(const int32_t* Gt, const int32_t* h, const int32_t* T, int L,
+                                                    int q, int P, int R, int D, int B, const uint32_t* inst,
+                                                    uint32_t k0, uint32_t k1, const int8_t* m0, const uint32_t* cdf,
+                                                    const uint8_t* perm, int warm_r, int8_t* out_s, int64_t* out_de,
+                                                    int64_t* out_st, int32_t* status, void* stream) {
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, 1, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  if (P != 2) return ARP_ERR_SHAPE;
+  if (!m0 || !perm || !cdf || warm_r < 0) return ARP_ERR_ARG;
+  DDParams a{Gt, h, T, nullptr, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, 1, out_s, out_de, out_st, status};
+  a.m0 = m0;
+  a.perm = perm;
+  a.warm_r = warm_r;
+  a.cdf = cdf;
+  return launch_warm(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_anneal_first_accept_warm_mix(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q,

@@ -29,6 +29,9 @@ struct DDParams {
   const int8_t* m0 = nullptr;
   const uint8_t* perm = nullptr;
   int warm_r = 1 << 30;  // anneals r < warm_r start from m0; the others from the MMSE start (m = 0), same order
+  // per-coordinate sampling thresholds (B, D) x (t0, t1): anneals 0 < r < warm_r draw their start spin sum from
+  // word 1 of their start Philox block u: class 0 if u < t0, 2 if u > t1, else 1 (m = 2 class - P); null: m0
+  const uint32_t* cdf = nullptr;
 };
 
 struct MapParams {

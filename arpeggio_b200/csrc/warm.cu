@@ -480,12 +480,14 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
                                                     const GT* __restrict__ G, const GT* __restrict__ h,
                                                     const int8_t* __restrict__ xq, int B, int D, int P, int M,
                                                     int8_t* __restrict__ m0, uint8_t* __restrict__ perm,
-                                                    ET* __restrict__ e0, int32_t* __restrict__ kept) {
+                                                    ET* __restrict__ e0, int32_t* __restrict__ kept, float tau,
+                                                    uint2* __restrict__ cdf) {
   const int b = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (b >= B) return;
   const int C = P + 1, Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
   int mv[4];
   float sc[4];
+  uint2 th[4];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
     const int j = t * 32 + lane;
@@ -505,6 +507,13 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
     sc[t] = 1.0f - __expf(z[P / 2] - zm) / se;
     int m = 2 * am - P;
     const int x = xq[(size_t)b * D + j];
+    if (cdf && P == 2) {  // sampling thresholds of softmax(tau z) over the classes that stay in the constellation
+      const bool ok0 = x - 2 >= -Lmax, ok2 = x + 2 <= Lmax;
+      const float q0 = ok0 ? __expf(tau * (z[0] - zm)) : 0.0f, q1 = __expf(tau * (z[1] - zm));
+      const float q2 = ok2 ? __expf(tau * (z[2] - zm)) : 0.0f, qs = q0 + q1 + q2;
+      th[t].x = ok0 ? __float2uint_rz(q0 / qs * 4294967296.0f) : 0u;
+      th[t].y = ok2 ? __float2uint_rz((q0 + q1) / qs * 4294967296.0f) : 0xFFFFFFFFu;
+    }
     if (x + m > Lmax) m = Lmax - x;
     if (x + m < -Lmax) m = -Lmax - x;
     mv[t] = m;
@@ -575,6 +584,7 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
     if (j >= D) continue;
     m0[(size_t)b * D + j] = (int8_t)(keep ? mv[t] : 0);
     perm[(size_t)b * D + (keep ? rk[t] : j)] = (uint8_t)j;
+    if (cdf) cdf[(size_t)b * D + j] = keep ? th[t] : make_uint2(0u, 0xFFFFFFFFu);  // fallback: always m = 0
   }
   if (lane == 0) {
     if (e0) e0[b] = keep ? e : ET(0);
@@ -664,6 +674,23 @@ extern "C" int arp_adam(float* w, void* w_bf16, const float* grad, float* m, flo
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
+extern "C" int arp_warm_start_sampled(const float* logits, int ldl, const void* G, const void* h, const int8_t* xq,
+                                      int B, int D, int P, int M, int quantized, int8_t* m0, uint8_t* perm, void* e0,
+                                      int32_t* kept, float tau, uint32_t* cdf, void* stream) {
+  if (B < 0 || D < 1 || D > 128 || P != 2 || ldl < P + 1 || !(M == 4 || M == 16 || M == 64)) return ARP_ERR_SHAPE;
+  if (B == 0) return ARP_OK;
+  if (!logits || !G || !h || !xq || !m0 || !perm || !cdf || !(tau > 0.0f)) return ARP_ERR_ARG;
+  const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (quantized)
+    k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
+                                                        P, M, m0, perm, (long long*)e0, kept, tau, (uint2*)cdf);
+  else
+    k_warm_start<float, float><<<nb, th, 0, st>>>(logits, ldl, (const float*)G, (const float*)h, xq, B, D, P, M, m0,
+                                                  perm, (float*)e0, kept, tau, (uint2*)cdf);
+  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
+
 extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const void* h, const int8_t* xq, int B,
                               int D, int P, int M, int quantized, int8_t* m0, uint8_t* perm, void* e0,
                               int32_t* kept, void* stream) {
@@ -675,10 +702,10 @@ extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const
   cudaStream_t st = (cudaStream_t)stream;
   if (quantized)
     k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
-                                                        P, M, m0, perm, (long long*)e0, kept);
+                                                        P, M, m0, perm, (long long*)e0, kept, 1.0f, nullptr);
   else
     k_warm_start<float, float><<<nb, th, 0, st>>>(logits, ldl, (const float*)G, (const float*)h, xq, B, D, P, M, m0,
-                                                  perm, (float*)e0, kept);
+                                                  perm, (float*)e0, kept, 1.0f, nullptr);
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 

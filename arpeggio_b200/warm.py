@@ -176,11 +176,13 @@ class WarmMLP:
 class WarmDetector(Detector):
     """One-stage dDI detector (16/64-QAM or QPSK, K = 1, integer fields, Arpeggio first accept) whose anneals start
     from the MLP's warm start in its flip-test order; problems whose warm start is worse than the MMSE guess
-    anneal from the plain MMSE start ('bal') in index order.  With mlp=None it is the plain MMSE-started detector
-    that also records the features' inputs (used to make training labels)."""
+    anneal from the plain MMSE start ('bal') in index order.  With tau set, anneal 0 starts from the argmax and
+    every other warm anneal draws its start from softmax(tau z) of the network's logits (a different start per
+    anneal, from the anneal's own Philox counters).  With mlp=None it is the plain MMSE-started detector that
+    also records the features' inputs (used to make training labels)."""
 
     def __init__(self, B, nt, nr=None, M=16, anneals=32, sweeps=None, mlp=None, T0=None, T1=None, q=None,
-                 device='cuda', warm_anneals=None):
+                 device='cuda', warm_anneals=None, tau=None):
         super().__init__(B, nt, nr, M, 'arpeggio', anneals, 1, sweeps=sweeps, T0=T0, T1=T1, q=q, start='bal',
                          precision='int', device=device)
         dev = self.device
@@ -195,6 +197,8 @@ class WarmDetector(Detector):
         self.kept = torch.zeros(B, dtype=torch.int32, device=dev)
         self.snr_db = torch.zeros(B, dtype=torch.float32, device=dev)
         self.Z = torch.empty(B * D, NO, dtype=torch.float32, device=dev) if mlp is not None else None
+        self.tau = tau
+        self.cdf = torch.empty(B, D, 2, dtype=torch.int32, device=dev) if tau is not None else None
 
     def set_noise(self, snr_db=None, N0=None, n=None):
         super().set_noise(snr_db, N0, n)
@@ -246,13 +250,24 @@ class WarmDetector(Detector):
                                            _lib.ptr(self.snr_db[sl]), n, D, self.M, P, 1, _lib.ptr(X), None, None, sp),
                        'warm_features')
             Z = self.mlp.infer(X, n * D, self.Z[off * D:(off + n) * D], stream)
-            _lib.check(L.arp_warm_start(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P, self.M, 1,
-                                        _lib.ptr(self.m0[sl]), _lib.ptr(self.perm[sl]), _lib.ptr(self.e0[sl]),
-                                        _lib.ptr(self.kept[sl]), sp), 'warm_start')
+            starts = (_lib.ptr(self.m0[sl]), _lib.ptr(self.perm[sl]), _lib.ptr(self.e0[sl]), _lib.ptr(self.kept[sl]))
+            if self.tau is None:
+                _lib.check(L.arp_warm_start(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P, self.M, 1,
+                                            *starts, sp), 'warm_start')
+            else:
+                _lib.check(L.arp_warm_start_sampled(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P,
+                                                    self.M, 1, *starts, float(self.tau), _lib.ptr(self.cdf[sl]), sp),
+                           'warm_start')
             ev(2 if e5 else 1)
-            rc = L.arp_anneal_first_accept_warm_mix(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P, R,
-                                                    D, n, _lib.ptr(inst), k0, k1, _lib.ptr(self.m0[sl]),
-                                                    _lib.ptr(self.perm[sl]), int(self.warm_anneals), *outs)
+            if self.tau is None:
+                rc = L.arp_anneal_first_accept_warm_mix(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P,
+                                                        R, D, n, _lib.ptr(inst), k0, k1, _lib.ptr(self.m0[sl]),
+                                                        _lib.ptr(self.perm[sl]), int(self.warm_anneals), *outs)
+            else:
+                rc = L.arp_anneal_first_accept_warm_sampled(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt,
+                                                            int(self.q), P, R, D, n, _lib.ptr(inst), k0, k1,
+                                                            _lib.ptr(self.m0[sl]), _lib.ptr(self.cdf[sl]),
+                                                            _lib.ptr(self.perm[sl]), int(self.warm_anneals), *outs)
         else:
             ev(2 if e5 else 1)
             rc = L.arp_anneal_first_accept(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P, R, D, n,

@@ -167,7 +167,9 @@ def frame_latency(det, f, stream, n):
 def warm_vs_plain(args, dev, stream, rank):
     """Trains the warm-start MLP on the GPU (plain MMSE-started Arpeggio at the full budget labels seeded 32-user
     16-QAM instances, SNR uniform 8-20 dB), then detects fresh 32-user and 64-user batches with the plain
-    MMSE-started annealer at the full budget and with the warm start at 1/2 and 3/4 of the sweeps: detections/s,
+    MMSE-started annealer at the full budget, with the sampled warm start (anneal 0 from the network's argmax, the
+    others drawn from softmax(0.5 z)) at 1/2 and 3/4 of the sweeps, and with the argmax-only warm start (every
+    anneal from the argmax) at 1/2 of the sweeps: detections/s,
     stage times, BER per SNR point and the paired BER ratio warm/plain with its bootstrap interval
     (arpeggio_b200.stats.boot_ratio), final energies, and the one-frame latency of each at 32 users."""
     import torch
@@ -182,7 +184,11 @@ def warm_vs_plain(args, dev, stream, rank):
                         'optimizer': 'Adam, lr 2e-3 -> 1e-4, 65536 rows per step'},
            'plain': 'MMSE-started (bal) Arpeggio first accept, fixed point, full sweep budget',
            'warm': 'MLP warm start (kept only where its energy is no worse than the MMSE guess), learned flip-test '
-                   'order, same kernel and anneals, reduced sweeps'}
+                   'order, same kernel and anneals, reduced sweeps',
+           'starts': {'warm_half, warm_three_quarter': 'anneal 0 from the argmax class, anneals 1..R-1 each drawn '
+                                                       'per coordinate from softmax(0.5 z) (Philox word 1 of the '
+                                                       'start block)',
+                      'warm_half_argmax': 'every anneal from the argmax class (bal pattern where m = 0)'}}
     for nt, B, snrs, full, R in ((32, args.batch, list(range(6, 23, 2)), 32, 32),
                                  (64, max(1024, args.batch // 4), list(range(10, 25, 2)), 64, 64)):
         snr = torch.tensor([float(snrs[i % len(snrs)]) for i in range(B)])
@@ -190,9 +196,10 @@ def warm_vs_plain(args, dev, stream, rank):
         bt = channel.levels_to_bits(d['l'], 16)
         res = {}
         base_err = None
-        for name, net, S in (('plain_full', None, full), ('warm_half', mlp, full // 2),
-                             ('warm_three_quarter', mlp, 3 * full // 4)):
-            det = warm.WarmDetector(B, nt, anneals=R, sweeps=S, mlp=net, device=dev)
+        for name, net, S, tau in (('plain_full', None, full, None), ('warm_half', mlp, full // 2, 0.5),
+                                  ('warm_three_quarter', mlp, 3 * full // 4, 0.5),
+                                  ('warm_half_argmax', mlp, full // 2, None)):
+            det = warm.WarmDetector(B, nt, anneals=R, sweeps=S, mlp=net, device=dev, tau=tau)
             det.set_noise(N0=d['N0'])
             for i in range(2):
                 det.run(d['H'], d['y'], seed=20 + i)
@@ -224,9 +231,9 @@ def warm_vs_plain(args, dev, stream, rank):
                 r['speedup_vs_plain'] = r['value'] / res['plain_full']['value']
             else:
                 base_err = err
-            if nt == 32 and args.latency_frames > 0:
+            if nt == 32 and args.latency_frames > 0 and name != 'warm_half_argmax':
                 f = channel.draw_device(77 + rank, 14.0, 1, nt, 16, dev=dev)
-                d1 = warm.WarmDetector(1, nt, anneals=R, sweeps=S, mlp=net, device=dev)
+                d1 = warm.WarmDetector(1, nt, anneals=R, sweeps=S, mlp=net, device=dev, tau=tau)
                 d1.set_noise(N0=f['N0'])
                 r['frame_latency'] = frame_latency(d1, f, stream, min(args.latency_frames, 1000))
                 del d1

@@ -128,16 +128,22 @@ typedef struct {
   int64_t *out_de, *out_st;
   const int8_t* m0; /* start == 2: given spin sums (B, D) */
   int warm_r;       /* start == 2: anneals r >= warm_r start from m = 0 */
+  const uint32_t* cdf; /* start == 2, or NULL: thresholds (B, D, 2) of sampled starts for anneals 0 < r < warm_r */
 } dd_ctx;
 
 /* Start spins of one anneal (arpeggio_ref59.py:44-49, arpeggio_fx.cu:48-57). s is P x D. */
 static void start_spins(int start, int P, int D, uint32_t r, uint32_t inst, uint32_t k0, uint32_t k1,
-                        const int8_t* m0, int8_t* s) {
+                        const int8_t* m0, const uint32_t* cdf, int8_t* s) {
   if (start == 2) { /* given spin sums: m = 0 takes the 'bal' pattern, m != 0 sets copies p < (m + P) / 2 */
     uint64_t C = (uint64_t)bal_count(P);
     for (int j = 0; j < D; j++) {
       uint32_t w0 = philox_word(0xFFFFFFFFu, (uint32_t)j, r, inst, k0, k1, 0);
-      int m = m0[j] < -P ? -P : (m0[j] > P ? P : m0[j]);
+      int m = m0[j];
+      if (cdf) { /* sampled start: word 1 of the same block against the coordinate's thresholds */
+        uint32_t w1 = philox_word(0xFFFFFFFFu, (uint32_t)j, r, inst, k0, k1, 1);
+        m = w1 < cdf[2 * j] ? -2 : (w1 > cdf[2 * j + 1] ? 2 : 0);
+      }
+      m = m < -P ? -P : (m > P ? P : m);
       int pat = m == 0 ? bal_pat(P, (uint32_t)(((uint64_t)w0 * C) >> 32)) : (1 << ((m + P) / 2)) - 1;
       for (int p = 0; p < P; p++) s[p * D + j] = ((pat >> p) & 1) ? 1 : -1;
     }
@@ -168,7 +174,8 @@ static void dd_job(void* vctx, long t) {
   uint8_t F[128];
   static const int8_t zeros[128] = {0};
   start_spins(x->start, P, D, r, inst, x->k0, x->k1,
-              x->m0 ? ((int)r < x->warm_r ? x->m0 + (size_t)b * D : zeros) : NULL, s);
+              x->m0 ? ((int)r < x->warm_r ? x->m0 + (size_t)b * D : zeros) : NULL,
+              (x->cdf && r > 0 && (int)r < x->warm_r) ? x->cdf + (size_t)b * D * 2 : NULL, s);
   memcpy(bs, s, (size_t)P * D);
   memset(pf, 0, sizeof pf);
   for (int i = 0; i < D; i++) { /* w_i = h_i - 2 sum_j G_ij m_j (arpeggio_ref59.py:50-51) */
@@ -247,19 +254,21 @@ int orc_anneal_dd(const int32_t* G, const int32_t* h, int B, int D, int P, int R
                   int policy, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
     return 1;
-  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL, 0};
+  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL, 0, NULL};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }
 
 /* First accept from given spin sums m0 (B, D) (start 2 of start_spins) for anneals r < warm_r, from m = 0 for
- * the others; the caller permutes the problem into scan order first (the device's flip-test order is a
- * relabelling of the coordinates). */
+ * the others; with cdf (B, D, 2) (or NULL) anneals 0 < r < warm_r draw their spin sums from those thresholds
+ * instead of taking m0.  The caller permutes the problem into scan order first (the device's flip-test order
+ * is a relabelling of the coordinates). */
 int orc_anneal_dd_warm(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T, int L,
                        int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1, const int8_t* m0, int warm_r,
-                       int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
+                       const uint32_t* cdf, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || L < 1 || R < 1 || B < 0 || !m0) return 1;
-  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0, warm_r};
+  if (cdf && P != 2) return 1;
+  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0, warm_r, cdf};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }
@@ -388,7 +397,7 @@ static void f32_job(void* vctx, long t) {
   int8_t s[6 * 128], bs[6 * 128];
   uint8_t pf[6 * 128], F[128];
   float w[128];
-  start_spins(x->start, P, D, r, inst, x->k0, x->k1, NULL, s);
+  start_spins(x->start, P, D, r, inst, x->k0, x->k1, NULL, NULL, s);
   memcpy(bs, s, (size_t)P * D);
   memset(pf, 0, sizeof pf);
   for (int i = 0; i < D; i++) {

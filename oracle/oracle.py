@@ -466,10 +466,35 @@ def warm_start(logits, G, h, xq, P, M):
     return m0, perm, np.where(keep, e0, 0), keep.astype(np.int32)
 
 
-def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=None):
+def warm_cdf(logits, xq, P, M, tau, kept):
+    """Sampling thresholds (B, D, 2) uint32 of the sampled warm start (P = 2): softmax(tau z) over the classes
+    m in {-2, 0, 2} whose level x + m stays inside the constellation; t0 = floor(2^32 p(m=-2)) (0 if -2 is out),
+    t1 = floor(2^32 (p(m=-2) + p(m=0))) (0xFFFFFFFF if +2 is out); problems with kept = 0 get (0, 0xFFFFFFFF).
+    Computed in float64: the device's single-precision exponentials agree to a few thousand units of 2^-32."""
+    assert P == 2
+    xq = np.asarray(xq, dtype=np.int64)
+    B, D = xq.shape
+    Lmax = {4: 1, 16: 3, 64: 7}[M]
+    z = np.asarray(logits, dtype=np.float32).reshape(B, D, -1)[..., :3].astype(np.float64)
+    q = np.exp(tau * (z - z.max(-1, keepdims=True)))
+    ok0 = xq - 2 >= -Lmax
+    ok2 = xq + 2 <= Lmax
+    q0 = np.where(ok0, q[..., 0], 0.0)
+    q2 = np.where(ok2, q[..., 2], 0.0)
+    qs = q0 + q[..., 1] + q2
+    t0 = np.where(ok0, np.floor(q0 / qs * 2.0 ** 32), 0)
+    t1 = np.where(ok2, np.floor((q0 + q[..., 1]) / qs * 2.0 ** 32), 0xFFFFFFFF)
+    out = np.stack([np.minimum(t0, 0xFFFFFFFF), np.minimum(t1, 0xFFFFFFFF)], -1).astype(np.uint32)
+    keep = np.asarray(kept).astype(bool)
+    out[~keep] = np.array([0, 0xFFFFFFFF], dtype=np.uint32)
+    return out
+
+
+def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=None, cdf=None):
     """First accept from the given start in the given flip-test order: the problem relabelled into scan order
     (position j' = coordinate perm[j']), annealed from spin sums m0 with the 'bal' pattern where m0 = 0, and the
-    spins relabelled back."""
+    spins relabelled back.  With cdf (B, D, 2) uint32 (warm_cdf) anneals 0 < r < warm_r draw their start spin
+    sums from the thresholds with word 1 of their start Philox block."""
     G = np.asarray(G, dtype=np.int32)
     h = np.asarray(h, dtype=np.int32)
     B, D, _ = G.shape
@@ -478,6 +503,7 @@ def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=Non
     Gp = np.ascontiguousarray(G[bi[:, :, None], pm[:, :, None], pm[:, None, :]], dtype=np.int32)
     hp = np.ascontiguousarray(h[bi, pm], dtype=np.int32)
     mp = np.ascontiguousarray(np.asarray(m0, dtype=np.int8)[bi, pm], dtype=np.int8)
+    cp = None if cdf is None else np.ascontiguousarray(np.asarray(cdf, dtype=np.uint32)[bi, pm], dtype=np.uint32)
     T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
     it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
     out_s = np.zeros((B, R, P * D), dtype=np.int8)
@@ -486,10 +512,10 @@ def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=Non
     L = lib()
     L.orc_anneal_dd_warm.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int,
                                      ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_int, _P, _P, _P,
-                                     ctypes.c_int]
+                                     _P, ctypes.c_int]
     rc = L.orc_anneal_dd_warm(_ptr(Gp), _ptr(hp), B, D, P, R, _ptr(T), len(T), int(q), _ptr(it), key & MASK,
-                              (key >> 32) & MASK, _ptr(mp), R if warm_r is None else int(warm_r), _ptr(out_s),
-                              _ptr(out_de), _ptr(out_st), nthreads)
+                              (key >> 32) & MASK, _ptr(mp), R if warm_r is None else int(warm_r),
+                              None if cp is None else _ptr(cp), _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
     if rc:
         raise ValueError('orc_anneal_dd_warm: unsupported shape')
     s = out_s.reshape(B, R, P, D)

@@ -315,3 +315,53 @@ def test_warm_start_mix_matches_oracle():
                                      99 | (1 << 32), m0, perm, nthreads=NTH, warm_r=wr)
         assert np.array_equal(so.cpu().numpy(), s) and np.array_equal(deo.cpu().numpy(), de), wr
         assert np.array_equal(sto.cpu().numpy(), st), wr
+
+
+def test_sampled_warm_starts_match_oracle():
+    """Sampled starts: the thresholds of softmax(tau z) against a float64 restatement (within 4096 / 2^32), and
+    the anneal that draws anneal r's start (0 < r < warm_r) from them bit for bit against the oracle fed the
+    device's thresholds."""
+    from arpeggio_b200 import _lib
+    B, D, R, wr, tau = 64, 64, 8, 6, 0.5
+    d, det = _problems(B, 32, 14.0, 31)
+    cls = (det.levels.long() - det.xq.long()) // 2 + 1
+    Zc = torch.randn(B * D, 16, generator=torch.Generator().manual_seed(4)).cuda()
+    Zc[torch.arange(B * D), cls.reshape(-1).clamp(0, 2)] += 3.0
+    m0 = torch.empty(B, D, dtype=torch.int8, device='cuda')
+    perm = torch.empty(B, D, dtype=torch.uint8, device='cuda')
+    e0 = torch.empty(B, dtype=torch.int64, device='cuda')
+    kept = torch.empty(B, dtype=torch.int32, device='cuda')
+    cdf = torch.empty(B, D, 2, dtype=torch.int32, device='cuda')
+    L = _lib.lib()
+    _lib.check(L.arp_warm_start_sampled(_lib.ptr(Zc), 16, _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(det.xq), B, D,
+                                        2, 16, 1, _lib.ptr(m0), _lib.ptr(perm), _lib.ptr(e0), _lib.ptr(kept), tau,
+                                        _lib.ptr(cdf), _lib.stream_ptr()), 'warm start sampled')
+    torch.cuda.synchronize()
+    G, h, xq = det.G.cpu().numpy(), det.h.cpu().numpy(), det.xq.cpu().numpy()
+    m0o, po, e0o, ko = O.warm_start(Zc.cpu().numpy(), G, h, xq, 2, 16)
+    assert ko.sum() > 16 and ko.sum() < B
+    assert np.array_equal(m0.cpu().numpy(), m0o) and np.array_equal(perm.cpu().numpy(), po)
+    assert np.array_equal(e0.cpu().numpy(), e0o) and np.array_equal(kept.cpu().numpy(), ko)
+    cd = cdf.cpu().numpy().view(np.uint32)
+    co = O.warm_cdf(Zc.cpu().numpy(), xq, 2, 16, tau, ko)
+    assert np.abs(cd.astype(np.int64) - co.astype(np.int64)).max() <= 4096
+    T = det.schedule['T']
+    Tt = torch.tensor(T, dtype=torch.int32, device='cuda')
+    inst = torch.arange(B, dtype=torch.int32, device='cuda')
+    so = torch.empty(B, R, 128, dtype=torch.int8, device='cuda')
+    deo = torch.empty(B, R, dtype=torch.int64, device='cuda')
+    sto = torch.empty(B, R, 2, dtype=torch.int64, device='cuda')
+    stat = torch.zeros(1, dtype=torch.int32, device='cuda')
+    _lib.check(L.arp_anneal_first_accept_warm_sampled(
+        _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(Tt), len(T), 0, 2, R, D, B, _lib.ptr(inst), 17, 3, _lib.ptr(m0),
+        _lib.ptr(cdf), _lib.ptr(perm), wr, _lib.ptr(so), _lib.ptr(deo), _lib.ptr(sto), _lib.ptr(stat),
+        _lib.stream_ptr()), 'warm anneal sampled')
+    torch.cuda.synchronize()
+    assert int(stat.item()) == 0
+    s, de, st = O.anneal_dd_warm(G, h, 2, R, T, 0, np.arange(B), 17 | (3 << 32), m0o, po, nthreads=NTH, warm_r=wr,
+                                 cdf=cd)
+    assert np.array_equal(so.cpu().numpy(), s) and np.array_equal(deo.cpu().numpy(), de)
+    assert np.array_equal(sto.cpu().numpy(), st)
+    # the sampled anneals explore: their results are not all anneal 0's
+    sd = so.cpu().numpy().reshape(B, R, 2, D).sum(2)
+    assert (sd[ko.astype(bool), 1:wr] != sd[ko.astype(bool), :1]).any()

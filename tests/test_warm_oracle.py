@@ -97,6 +97,35 @@ def test_oracle_warm_start_falls_back_when_worse_than_the_guess():
     assert kept.dtype == np.int32
 
 
+def test_oracle_sampled_starts():
+    """Thresholds exclude the classes that leave the constellation and fall back to m = 0 for dropped problems;
+    thresholds that always give m = 0 make the sampled anneal the warm anneal with warm_r = 1; thresholds that
+    always give m0's class make it the warm anneal with every anneal from m0."""
+    r = np.random.default_rng(8)
+    xq = r.integers(-3, 4, (5, 24)).astype(np.int8)
+    xq[0, :4] = [-3, 3, -1, 1]
+    logits = r.normal(0, 2, (5 * 24, 16)).astype(np.float32)
+    kept = np.array([1, 1, 1, 1, 0], np.int32)
+    c = O.warm_cdf(logits, xq, 2, 16, 0.5, kept)
+    assert c[0, 0, 0] == 0 and c[0, 1, 1] == 0xFFFFFFFF
+    assert (c[..., 0] <= c[..., 1]).all()
+    assert (c[4, :, 0] == 0).all() and (c[4, :, 1] == 0xFFFFFFFF).all()
+    G, h = _problem(5, 24, 6)
+    T = [300] * 10
+    m0 = (2 * r.integers(-1, 2, (5, 24))).astype(np.int8)
+    perm = np.stack([r.permutation(24) for _ in range(5)]).astype(np.uint8)
+    zero = np.zeros((5, 24, 2), np.uint32)
+    zero[..., 1] = 0xFFFFFFFF
+    a = O.anneal_dd_warm(G, h, 2, 4, T, 0, np.arange(5), 21, m0, perm, warm_r=4, cdf=zero)
+    b = O.anneal_dd_warm(G, h, 2, 4, T, 0, np.arange(5), 21, m0, perm, warm_r=1)
+    assert all(np.array_equal(u, v) for u, v in zip(a, b))
+    same = np.where(m0[..., None] < 0, [0xFFFFFFFF, 0xFFFFFFFF], np.where(m0[..., None] > 0, [0, 0],
+                                                                          [0, 0xFFFFFFFF])).astype(np.uint32)
+    a = O.anneal_dd_warm(G, h, 2, 4, T, 0, np.arange(5), 21, m0, perm, warm_r=4, cdf=same)
+    b = O.anneal_dd_warm(G, h, 2, 4, T, 0, np.arange(5), 21, m0, perm, warm_r=4)
+    assert all(np.array_equal(u, v) for u, v in zip(a, b))
+
+
 def test_serving_admission_and_mixed_classes():
     from arpeggio_b200 import mixed, serve
     cls = mixed.mixed_classes()

@@ -49,9 +49,9 @@ SIGNATURES = {
     'arp_anneal_first_accept_warm': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _P, _P, _P, _P],
     'arp_anneal_first_accept_warm_mix': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _I, _P, _P, _P, _P,
                                          _P],
-    'arp_warm_start_sampled': [_P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _F, _P, _P],
+    'arp_warm_start_sampled': [_P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _F, _P, _F, _I, _I, _P, _P],
     'arp_anneal_first_accept_warm_sampled': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _I, _P, _P,
-                                             _P, _P, _P],
+                                             _P, _P, _P, _P],
     'arp_detect_dd_static': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U,
                              _I, _P, _P, _P, _P, _P, _P],
 }

@@ -397,7 +397,23 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
     dg2[t] = j < D ? 2 * Gs[j * DP + j] : 0;
   }
 
-  for (int r = bs + split * wid; r < R; r += split * W) {
+  int Rb = R;
+  if constexpr (WARM) {
+    if (a.ra) {  // a per-problem anneal count: the skipped anneals report the guess
+      const int v = a.ra[b];
+      Rb = v < 1 ? 1 : (v > R ? R : v);
+      for (int r = Rb + bs; r < R; r += split) {
+        const size_t ar = (size_t)b * R + r;
+        for (int x = threadIdx.x; x < P * D; x += blockDim.x) a.out_s[ar * P * D + x] = 0;
+        if (threadIdx.x == 0) {
+          reinterpret_cast<long long*>(a.out_de)[ar] = LLONG_MAX;
+          a.out_st[2 * ar] = 0;
+          a.out_st[2 * ar + 1] = 0;
+        }
+      }
+    }
+  }
+  for (int r = bs + split * wid; r < Rb; r += split * W) {
     // ---- start state (arpeggio_fx.cu:48-57), packed per thread
     uint32_t sp = 0;
     if constexpr (WARM) {
@@ -759,8 +775,9 @@ extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, co
 extern "C" int arp_anneal_first_accept_warm_sampled(const int32_t* Gt, const int32_t* h, const int32_t* T, int L,
                                                     int q, int P, int R, int D, int B, const uint32_t* inst,
                                                     uint32_t k0, uint32_t k1, const int8_t* m0, const uint32_t* cdf,
-                                                    const uint8_t* perm, int warm_r, int8_t* out_s, int64_t* out_de,
-                                                    int64_t* out_st, int32_t* status, void* stream) {
+                                                    const uint8_t* perm, int warm_r, const int32_t* ra,
+                                                    int8_t* out_s, int64_t* out_de, int64_t* out_st,
+                                                    int32_t* status, void* stream) {
   int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, 1, out_s, out_de, out_st);
   if (rc || B == 0) return rc;
   if (P != 2) return ARP_ERR_SHAPE;
@@ -770,6 +787,7 @@ extern "C" int arp_anneal_first_accept_warm_sampled(const int32_t* Gt, const int
   a.perm = perm;
   a.warm_r = warm_r;
   a.cdf = cdf;
+  a.ra = ra;
   return launch_warm(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 

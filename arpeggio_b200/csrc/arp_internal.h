@@ -32,6 +32,9 @@ struct DDParams {
   // per-coordinate sampling thresholds (B, D) x (t0, t1): anneals 0 < r < warm_r draw their start spin sum from
   // word 1 of their start Philox block u: class 0 if u < t0, 2 if u > t1, else 1 (m = 2 class - P); null: m0
   const uint32_t* cdf = nullptr;
+  // per-problem anneal counts (B), or null: problem b runs anneals r < ra[b] (clamped to 1..R); the skipped
+  // anneals report all-zero spin sums (the guess), best energy INT64_MAX and no tests or flips
+  const int32_t* ra = nullptr;
 };
 
 struct MapParams {

@@ -481,13 +481,15 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
                                                     const int8_t* __restrict__ xq, int B, int D, int P, int M,
                                                     int8_t* __restrict__ m0, uint8_t* __restrict__ perm,
                                                     ET* __restrict__ e0, int32_t* __restrict__ kept, float tau,
-                                                    uint2* __restrict__ cdf) {
+                                                    uint2* __restrict__ cdf, float conf_min, int r_easy, int R,
+                                                    int32_t* __restrict__ ra) {
   const int b = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (b >= B) return;
   const int C = P + 1, Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
   int mv[4];
   float sc[4];
   uint2 th[4];
+  float lse = 0.0f;  // sum over coordinates of -log max_c p_c: minus the log-probability of the argmax start
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
     const int j = t * 32 + lane;
@@ -505,6 +507,7 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
     float se = 0.0f;
     for (int c = 0; c < C; ++c) se += __expf(z[c] - zm);
     sc[t] = 1.0f - __expf(z[P / 2] - zm) / se;
+    lse += __logf(se);
     int m = 2 * am - P;
     const int x = xq[(size_t)b * D + j];
     if (cdf && P == 2) {  // sampling thresholds of softmax(tau z) over the classes that stay in the constellation
@@ -585,6 +588,11 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
     m0[(size_t)b * D + j] = (int8_t)(keep ? mv[t] : 0);
     perm[(size_t)b * D + (keep ? rk[t] : j)] = (uint8_t)j;
     if (cdf) cdf[(size_t)b * D + j] = keep ? th[t] : make_uint2(0u, 0xFFFFFFFFu);  // fallback: always m = 0
+  }
+  if (ra) {  // confident kept starts get r_easy anneals, the others R
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lse += __shfl_xor_sync(0xffffffffu, lse, o);
+    if (lane == 0) ra[b] = (keep && -lse > conf_min) ? r_easy : R;
   }
   if (lane == 0) {
     if (e0) e0[b] = keep ? e : ET(0);
@@ -676,18 +684,22 @@ extern "C" int arp_adam(float* w, void* w_bf16, const float* grad, float* m, flo
 
 extern "C" int arp_warm_start_sampled(const float* logits, int ldl, const void* G, const void* h, const int8_t* xq,
                                       int B, int D, int P, int M, int quantized, int8_t* m0, uint8_t* perm, void* e0,
-                                      int32_t* kept, float tau, uint32_t* cdf, void* stream) {
+                                      int32_t* kept, float tau, uint32_t* cdf, float conf_min, int r_easy, int R,
+                                      int32_t* ra, void* stream) {
   if (B < 0 || D < 1 || D > 128 || P != 2 || ldl < P + 1 || !(M == 4 || M == 16 || M == 64)) return ARP_ERR_SHAPE;
   if (B == 0) return ARP_OK;
   if (!logits || !G || !h || !xq || !m0 || !perm || !cdf || !(tau > 0.0f)) return ARP_ERR_ARG;
+  if (ra && (R < 1 || r_easy < 1 || r_easy > R)) return ARP_ERR_ARG;
   const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
   cudaStream_t st = (cudaStream_t)stream;
   if (quantized)
     k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
-                                                        P, M, m0, perm, (long long*)e0, kept, tau, (uint2*)cdf);
+                                                        P, M, m0, perm, (long long*)e0, kept, tau, (uint2*)cdf,
+                                                        conf_min, r_easy, R, ra);
   else
     k_warm_start<float, float><<<nb, th, 0, st>>>(logits, ldl, (const float*)G, (const float*)h, xq, B, D, P, M, m0,
-                                                  perm, (float*)e0, kept, tau, (uint2*)cdf);
+                                                  perm, (float*)e0, kept, tau, (uint2*)cdf, conf_min, r_easy, R,
+                                                  ra);
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
@@ -702,10 +714,11 @@ extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const
   cudaStream_t st = (cudaStream_t)stream;
   if (quantized)
     k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
-                                                        P, M, m0, perm, (long long*)e0, kept, 1.0f, nullptr);
+                                                        P, M, m0, perm, (long long*)e0, kept, 1.0f, nullptr, 0.0f, 1, 1,
+                                                        nullptr);
   else
     k_warm_start<float, float><<<nb, th, 0, st>>>(logits, ldl, (const float*)G, (const float*)h, xq, B, D, P, M, m0,
-                                                  perm, (float*)e0, kept, 1.0f, nullptr);
+                                                  perm, (float*)e0, kept, 1.0f, nullptr, 0.0f, 1, 1, nullptr);
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 

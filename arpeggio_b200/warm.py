@@ -178,11 +178,13 @@ class WarmDetector(Detector):
     from the MLP's warm start in its flip-test order; problems whose warm start is worse than the MMSE guess
     anneal from the plain MMSE start ('bal') in index order.  With tau set, anneal 0 starts from the argmax and
     every other warm anneal draws its start from softmax(tau z) of the network's logits (a different start per
-    anneal, from the anneal's own Philox counters).  With mlp=None it is the plain MMSE-started detector that
-    also records the features' inputs (used to make training labels)."""
+    anneal, from the anneal's own Philox counters).  With conf_min also set, problems whose kept start has
+    confidence sum_j log max_c p_jc above conf_min run only r_easy anneals (default: one per warp of the anneal's
+    block, 8), the others all R.  With mlp=None it is the plain MMSE-started detector that also records the
+    features' inputs (used to make training labels)."""
 
     def __init__(self, B, nt, nr=None, M=16, anneals=32, sweeps=None, mlp=None, T0=None, T1=None, q=None,
-                 device='cuda', warm_anneals=None, tau=None):
+                 device='cuda', warm_anneals=None, tau=None, conf_min=None, r_easy=8):
         super().__init__(B, nt, nr, M, 'arpeggio', anneals, 1, sweeps=sweeps, T0=T0, T1=T1, q=q, start='bal',
                          precision='int', device=device)
         dev = self.device
@@ -199,6 +201,10 @@ class WarmDetector(Detector):
         self.Z = torch.empty(B * D, NO, dtype=torch.float32, device=dev) if mlp is not None else None
         self.tau = tau
         self.cdf = torch.empty(B, D, 2, dtype=torch.int32, device=dev) if tau is not None else None
+        if conf_min is not None and tau is None:
+            raise ValueError('per-problem anneal counts need the sampled start (tau)')
+        self.conf_min, self.r_easy = conf_min, min(r_easy, anneals)
+        self.ra = torch.full((B,), anneals, dtype=torch.int32, device=dev) if conf_min is not None else None
 
     def set_noise(self, snr_db=None, N0=None, n=None):
         super().set_noise(snr_db, N0, n)
@@ -255,9 +261,11 @@ class WarmDetector(Detector):
                 _lib.check(L.arp_warm_start(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P, self.M, 1,
                                             *starts, sp), 'warm_start')
             else:
+                ra = _lib.ptr(self.ra[sl]) if self.ra is not None else None
+                cm = float(self.conf_min) if self.conf_min is not None else 0.0
                 _lib.check(L.arp_warm_start_sampled(_lib.ptr(Z), NO, _lib.ptr(G), _lib.ptr(h), _lib.ptr(xq), n, D, P,
-                                                    self.M, 1, *starts, float(self.tau), _lib.ptr(self.cdf[sl]), sp),
-                           'warm_start')
+                                                    self.M, 1, *starts, float(self.tau), _lib.ptr(self.cdf[sl]), cm,
+                                                    int(self.r_easy), R, ra, sp), 'warm_start')
             ev(2 if e5 else 1)
             if self.tau is None:
                 rc = L.arp_anneal_first_accept_warm_mix(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P,
@@ -267,7 +275,9 @@ class WarmDetector(Detector):
                 rc = L.arp_anneal_first_accept_warm_sampled(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt,
                                                             int(self.q), P, R, D, n, _lib.ptr(inst), k0, k1,
                                                             _lib.ptr(self.m0[sl]), _lib.ptr(self.cdf[sl]),
-                                                            _lib.ptr(self.perm[sl]), int(self.warm_anneals), *outs)
+                                                            _lib.ptr(self.perm[sl]), int(self.warm_anneals),
+                                                            _lib.ptr(self.ra[sl]) if self.ra is not None else None,
+                                                            *outs)
         else:
             ev(2 if e5 else 1)
             rc = L.arp_anneal_first_accept(_lib.ptr(G), _lib.ptr(h), _lib.ptr(self.T), Lt, int(self.q), P, R, D, n,

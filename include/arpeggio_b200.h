@@ -264,21 +264,25 @@ int arp_anneal_first_accept_warm_mix(const int32_t* Gt, const int32_t* h, const 
  * softmax(tau z) over the classes whose spin sum keeps the level inside the constellation: with u a uniform
  * 32-bit word, class 0 (m = -2) if u < cdf[0], class 2 (m = +2) if u > cdf[1], else class 1 (m = 0).  Problems
  * that fall back to the plain start (kept = 0) get (0, 0xFFFFFFFF): always m = 0.  tau > 0 sharpens (> 1) or
- * flattens (< 1) the network's distribution.  No counterpart in the reference. */
+ * flattens (< 1) the network's distribution.  With ra non-NULL it also writes per-problem anneal counts ra (B):
+ * r_easy (1..R) where the start is kept and its confidence sum_j log max_c softmax(z_j)_c exceeds conf_min,
+ * else R.  No counterpart in the reference. */
 int arp_warm_start_sampled(const float* logits, int ldl, const void* G, const void* h, const int8_t* xq, int B, int D,
                            int P, int M, int quantized, int8_t* m0, uint8_t* perm, void* e0, int32_t* kept,
-                           float tau, uint32_t* cdf, void* stream);
+                           float tau, uint32_t* cdf, float conf_min, int r_easy, int R, int32_t* ra, void* stream);
 
 /* arp_anneal_first_accept_warm_mix with sampled starts: anneal 0 starts from m0, each anneal 0 < r < warm_r
  * draws every coordinate's start spin sum from cdf (arp_warm_start_sampled) with word 1 of the Philox block
  * (0xFFFFFFFF, j', r, inst) of the coordinate's scan position j' (word 0 still picks the 'bal' pattern of m = 0),
- * anneals r >= warm_r start from the MMSE start; all in the given flip-test order.  P = 2 only.  No counterpart
- * in the reference. */
+ * anneals r >= warm_r start from the MMSE start; all in the given flip-test order.  With ra (B) non-NULL,
+ * problem b runs only anneals r < ra[b] (clamped to 1..R; each exactly as in the full run, its counters being
+ * its own) and the skipped anneals report all-zero spin sums (a candidate equal to the guess), out_de
+ * INT64_MAX and zero statistics.  P = 2 only.  No counterpart in the reference. */
 int arp_anneal_first_accept_warm_sampled(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P,
                                          int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
                                          const int8_t* m0, const uint32_t* cdf, const uint8_t* perm, int warm_r,
-                                         int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status,
-                                         void* stream);
+                                         const int32_t* ra, int8_t* out_s, int64_t* out_de, int64_t* out_st,
+                                         int32_t* status, void* stream);
 
 /* arp_detect_dd without a workspace argument, for callers that cannot allocate device memory: a receive
  * chain with a hard per-frame latency budget cannot call cudaMalloc on the frame path (it synchronises the

@@ -129,6 +129,7 @@ typedef struct {
   const int8_t* m0; /* start == 2: given spin sums (B, D) */
   int warm_r;       /* start == 2: anneals r >= warm_r start from m = 0 */
   const uint32_t* cdf; /* start == 2, or NULL: thresholds (B, D, 2) of sampled starts for anneals 0 < r < warm_r */
+  const int32_t* ra;   /* or NULL: per-problem anneal counts (B); anneals r >= ra[b] are skipped */
 } dd_ctx;
 
 /* Start spins of one anneal (arpeggio_ref59.py:44-49, arpeggio_fx.cu:48-57). s is P x D. */
@@ -173,6 +174,16 @@ static void dd_job(void* vctx, long t) {
   int64_t w[128];
   uint8_t F[128];
   static const int8_t zeros[128] = {0};
+  if (x->ra) { /* a skipped anneal reports the guess: zero spin sums, best energy INT64_MAX, no tests */
+    int rb = x->ra[b] < 1 ? 1 : (x->ra[b] > R ? R : x->ra[b]);
+    if ((int)r >= rb) {
+      memset(x->out_s + (size_t)t * P * D, 0, (size_t)P * D);
+      x->out_de[t] = INT64_MAX;
+      x->out_st[2 * t] = 0;
+      x->out_st[2 * t + 1] = 0;
+      return;
+    }
+  }
   start_spins(x->start, P, D, r, inst, x->k0, x->k1,
               x->m0 ? ((int)r < x->warm_r ? x->m0 + (size_t)b * D : zeros) : NULL,
               (x->cdf && r > 0 && (int)r < x->warm_r) ? x->cdf + (size_t)b * D * 2 : NULL, s);
@@ -254,21 +265,22 @@ int orc_anneal_dd(const int32_t* G, const int32_t* h, int B, int D, int P, int R
                   int policy, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
     return 1;
-  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL, 0, NULL};
+  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL, 0, NULL, NULL};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }
 
 /* First accept from given spin sums m0 (B, D) (start 2 of start_spins) for anneals r < warm_r, from m = 0 for
  * the others; with cdf (B, D, 2) (or NULL) anneals 0 < r < warm_r draw their spin sums from those thresholds
- * instead of taking m0.  The caller permutes the problem into scan order first (the device's flip-test order
+ * instead of taking m0; with ra (B) (or NULL) problem b runs anneals r < ra[b] only.  The caller permutes the problem into scan order first (the device's flip-test order
  * is a relabelling of the coordinates). */
 int orc_anneal_dd_warm(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T, int L,
                        int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1, const int8_t* m0, int warm_r,
-                       const uint32_t* cdf, int8_t* out_s, int64_t* out_de, int64_t* out_st, int nthreads) {
+                       const uint32_t* cdf, const int32_t* ra, int8_t* out_s, int64_t* out_de, int64_t* out_st,
+                       int nthreads) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || L < 1 || R < 1 || B < 0 || !m0) return 1;
   if (cdf && P != 2) return 1;
-  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0, warm_r, cdf};
+  dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0, warm_r, cdf, ra};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }

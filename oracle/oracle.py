@@ -490,11 +490,24 @@ def warm_cdf(logits, xq, P, M, tau, kept):
     return out
 
 
-def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=None, cdf=None):
+def warm_counts(logits, P, kept, conf_min, r_easy, R):
+    """Per-problem anneal counts (B) and confidences (B): confidence = sum_j log max_c softmax(z_j)_c over the
+    P + 1 classes (float64; the device sums single-precision logarithms, so counts can differ only where the
+    confidence is within a few 1e-4 of conf_min); r_easy where kept and confidence > conf_min, else R."""
+    kept = np.asarray(kept).astype(bool)
+    B = kept.shape[0]
+    z = np.asarray(logits, dtype=np.float32).reshape(B, -1, np.asarray(logits).shape[-1])[..., :P + 1]
+    z = z.astype(np.float64)
+    conf = -np.log(np.exp(z - z.max(-1, keepdims=True)).sum(-1)).sum(-1)
+    return np.where(kept & (conf > conf_min), r_easy, R).astype(np.int32), conf
+
+
+def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=None, cdf=None, ra=None):
     """First accept from the given start in the given flip-test order: the problem relabelled into scan order
     (position j' = coordinate perm[j']), annealed from spin sums m0 with the 'bal' pattern where m0 = 0, and the
     spins relabelled back.  With cdf (B, D, 2) uint32 (warm_cdf) anneals 0 < r < warm_r draw their start spin
-    sums from the thresholds with word 1 of their start Philox block."""
+    sums from the thresholds with word 1 of their start Philox block.  With ra (B) int32 problem b runs anneals
+    r < ra[b] only; the others report zero spin sums, INT64_MAX and zero statistics."""
     G = np.asarray(G, dtype=np.int32)
     h = np.asarray(h, dtype=np.int32)
     B, D, _ = G.shape
@@ -504,6 +517,7 @@ def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=Non
     hp = np.ascontiguousarray(h[bi, pm], dtype=np.int32)
     mp = np.ascontiguousarray(np.asarray(m0, dtype=np.int8)[bi, pm], dtype=np.int8)
     cp = None if cdf is None else np.ascontiguousarray(np.asarray(cdf, dtype=np.uint32)[bi, pm], dtype=np.uint32)
+    rp = None if ra is None else np.ascontiguousarray(ra, dtype=np.int32)
     T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
     it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
     out_s = np.zeros((B, R, P * D), dtype=np.int8)
@@ -512,10 +526,11 @@ def anneal_dd_warm(G, h, P, R, T, q, inst, key, m0, perm, nthreads=1, warm_r=Non
     L = lib()
     L.orc_anneal_dd_warm.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int,
                                      ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_int, _P, _P, _P,
-                                     _P, ctypes.c_int]
+                                     _P, _P, ctypes.c_int]
     rc = L.orc_anneal_dd_warm(_ptr(Gp), _ptr(hp), B, D, P, R, _ptr(T), len(T), int(q), _ptr(it), key & MASK,
                               (key >> 32) & MASK, _ptr(mp), R if warm_r is None else int(warm_r),
-                              None if cp is None else _ptr(cp), _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+                              None if cp is None else _ptr(cp), None if rp is None else _ptr(rp), _ptr(out_s),
+                              _ptr(out_de), _ptr(out_st), nthreads)
     if rc:
         raise ValueError('orc_anneal_dd_warm: unsupported shape')
     s = out_s.reshape(B, R, P, D)

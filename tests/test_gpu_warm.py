@@ -335,7 +335,7 @@ def test_sampled_warm_starts_match_oracle():
     L = _lib.lib()
     _lib.check(L.arp_warm_start_sampled(_lib.ptr(Zc), 16, _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(det.xq), B, D,
                                         2, 16, 1, _lib.ptr(m0), _lib.ptr(perm), _lib.ptr(e0), _lib.ptr(kept), tau,
-                                        _lib.ptr(cdf), _lib.stream_ptr()), 'warm start sampled')
+                                        _lib.ptr(cdf), 0.0, 1, R, None, _lib.stream_ptr()), 'warm start sampled')
     torch.cuda.synchronize()
     G, h, xq = det.G.cpu().numpy(), det.h.cpu().numpy(), det.xq.cpu().numpy()
     m0o, po, e0o, ko = O.warm_start(Zc.cpu().numpy(), G, h, xq, 2, 16)
@@ -354,7 +354,7 @@ def test_sampled_warm_starts_match_oracle():
     stat = torch.zeros(1, dtype=torch.int32, device='cuda')
     _lib.check(L.arp_anneal_first_accept_warm_sampled(
         _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(Tt), len(T), 0, 2, R, D, B, _lib.ptr(inst), 17, 3, _lib.ptr(m0),
-        _lib.ptr(cdf), _lib.ptr(perm), wr, _lib.ptr(so), _lib.ptr(deo), _lib.ptr(sto), _lib.ptr(stat),
+        _lib.ptr(cdf), _lib.ptr(perm), wr, None, _lib.ptr(so), _lib.ptr(deo), _lib.ptr(sto), _lib.ptr(stat),
         _lib.stream_ptr()), 'warm anneal sampled')
     torch.cuda.synchronize()
     assert int(stat.item()) == 0
@@ -365,3 +365,58 @@ def test_sampled_warm_starts_match_oracle():
     # the sampled anneals explore: their results are not all anneal 0's
     sd = so.cpu().numpy().reshape(B, R, 2, D).sum(2)
     assert (sd[ko.astype(bool), 1:wr] != sd[ko.astype(bool), :1]).any()
+
+
+def test_per_problem_anneal_counts_match_oracle():
+    """Per-problem anneal counts from the start's confidence: counts against the float64 restatement (away from
+    the threshold), the anneal with counts bit for bit against the oracle, each kept anneal identical to the
+    full run's, skipped anneals reporting the guess (zero spin sums, INT64_MAX, no statistics)."""
+    from arpeggio_b200 import _lib
+    B, D, R, tau = 64, 64, 16, 0.5
+    d, det = _problems(B, 32, 20.0, 41)
+    cls = (det.levels.long() - det.xq.long()) // 2 + 1
+    Zc = torch.randn(B * D, 16, generator=torch.Generator().manual_seed(6)).cuda()
+    Zc[torch.arange(B * D), cls.reshape(-1).clamp(0, 2)] += 3.0 + 3.0 * torch.rand(B * D, generator=torch.Generator()
+                                                                                    .manual_seed(7)).cuda()
+    m0 = torch.empty(B, D, dtype=torch.int8, device='cuda')
+    perm = torch.empty(B, D, dtype=torch.uint8, device='cuda')
+    e0 = torch.empty(B, dtype=torch.int64, device='cuda')
+    kept = torch.empty(B, dtype=torch.int32, device='cuda')
+    cdf = torch.empty(B, D, 2, dtype=torch.int32, device='cuda')
+    ra = torch.empty(B, dtype=torch.int32, device='cuda')
+    G, h, xq = det.G.cpu().numpy(), det.h.cpu().numpy(), det.xq.cpu().numpy()
+    _, _, _, ko = O.warm_start(Zc.cpu().numpy(), G, h, xq, 2, 16)
+    _, conf = O.warm_counts(Zc.cpu().numpy(), 2, ko, 0.0, 4, R)
+    cmin = float(np.median(conf[ko.astype(bool)]))
+    L = _lib.lib()
+    _lib.check(L.arp_warm_start_sampled(_lib.ptr(Zc), 16, _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(det.xq), B, D,
+                                        2, 16, 1, _lib.ptr(m0), _lib.ptr(perm), _lib.ptr(e0), _lib.ptr(kept), tau,
+                                        _lib.ptr(cdf), cmin, 4, R, _lib.ptr(ra), _lib.stream_ptr()), 'warm start')
+    torch.cuda.synchronize()
+    rao, conf = O.warm_counts(Zc.cpu().numpy(), 2, ko, cmin, 4, R)
+    rd = ra.cpu().numpy()
+    far = np.abs(conf - cmin) > 1e-3
+    assert np.array_equal(rd[far], rao[far])
+    assert (rd == 4).sum() >= 8 and (rd == R).sum() >= 8
+    T = det.schedule['T']
+    Tt = torch.tensor(T, dtype=torch.int32, device='cuda')
+    inst = torch.arange(B, dtype=torch.int32, device='cuda')
+    outs = [(torch.empty(B, R, 128, dtype=torch.int8, device='cuda'), torch.empty(B, R, dtype=torch.int64, device='cuda'),
+             torch.empty(B, R, 2, dtype=torch.int64, device='cuda')) for _ in range(2)]
+    stat = torch.zeros(1, dtype=torch.int32, device='cuda')
+    for (so, deo, sto), counts in zip(outs, (ra, None)):
+        _lib.check(L.arp_anneal_first_accept_warm_sampled(
+            _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(Tt), len(T), 0, 2, R, D, B, _lib.ptr(inst), 5, 9, _lib.ptr(m0),
+            _lib.ptr(cdf), _lib.ptr(perm), R, _lib.ptr(counts) if counts is not None else None, _lib.ptr(so),
+            _lib.ptr(deo), _lib.ptr(sto), _lib.ptr(stat), _lib.stream_ptr()), 'warm anneal counts')
+    torch.cuda.synchronize()
+    assert int(stat.item()) == 0
+    cd = cdf.cpu().numpy().view(np.uint32)
+    s, de, st = O.anneal_dd_warm(G, h, 2, R, T, 0, np.arange(B), 5 | (9 << 32), m0.cpu().numpy(), perm.cpu().numpy(),
+                                 nthreads=NTH, cdf=cd, ra=rd)
+    (so, deo, sto), (sf, def_, stf) = [[x.cpu().numpy() for x in o] for o in outs]
+    assert np.array_equal(so, s) and np.array_equal(deo, de) and np.array_equal(sto, st)
+    for b in range(B):
+        k = int(rd[b])
+        assert np.array_equal(so[b, :k], sf[b, :k]) and np.array_equal(deo[b, :k], def_[b, :k])
+        assert (so[b, k:] == 0).all() and (deo[b, k:] == np.iinfo(np.int64).max).all() and (sto[b, k:] == 0).all()

@@ -137,3 +137,24 @@ def test_serving_admission_and_mixed_classes():
     assert serve.shared_bytes((64, 128, 16), 32) > serve.shared_bytes((64, 64, 16), 32)
     arrivals = serve.poisson_arrivals(10000, 1e5, np.random.default_rng(0))
     assert np.all(np.diff(arrivals) > 0) and abs(arrivals[-1] - 0.1) < 0.01
+
+
+def test_oracle_anneal_counts_skip_exactly_the_late_anneals():
+    """Anneal counts keep anneals r < ra[b] as in the full run and report the guess for the rest."""
+    G, h = _problem(4, 20, 9)
+    T = [300] * 8
+    r = np.random.default_rng(10)
+    m0 = (2 * r.integers(-1, 2, (4, 20))).astype(np.int8)
+    perm = np.stack([r.permutation(20) for _ in range(4)]).astype(np.uint8)
+    ra = np.array([1, 3, 6, 0], np.int32)  # 0 is clamped to 1
+    full = O.anneal_dd_warm(G, h, 2, 6, T, 0, np.arange(4), 3, m0, perm)
+    part = O.anneal_dd_warm(G, h, 2, 6, T, 0, np.arange(4), 3, m0, perm, ra=ra)
+    for b, k in enumerate(np.maximum(ra, 1)):
+        for f, p in zip(full, part):
+            assert np.array_equal(f[b, :k], p[b, :k])
+        assert (part[0][b, k:] == 0).all() and (part[1][b, k:] == np.iinfo(np.int64).max).all()
+        assert (part[2][b, k:] == 0).all()
+    logits = np.zeros((2 * 20, 16), np.float32)
+    logits[:20, 1] = 9.0  # problem 0 confident, problem 1 uniform (confidence 20 log(1/3))
+    counts, conf = O.warm_counts(logits, 2, np.array([1, 1]), -1.0, 4, 16)
+    assert list(counts) == [4, 16] and abs(conf[1] - 20 * np.log(1 / 3)) < 1e-9

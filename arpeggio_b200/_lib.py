@@ -16,6 +16,7 @@ _F = ctypes.c_float
 SIGNATURES = {
     'arp_version': [],
     'arp_status_string': [_I],
+    'arp_host_device_pointer': [_P, _P],
     'arp_philox_kat': [_P, _P, _I, _P],
     'arp_philox_rate': [_P, _I, _I, _I, _P],
     'arp_anneal_first_accept': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
@@ -90,6 +91,13 @@ def check(rc, what):
 def ptr(t):
     """Device pointer of a torch tensor (None -> NULL)."""
     return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def host_device_ptr(t):
+    """Device address of a pinned (mapped) host tensor, for kernels that write results straight into it."""
+    d = ctypes.c_void_p()
+    check(lib().arp_host_device_pointer(ctypes.c_void_p(t.data_ptr()), ctypes.byref(d)), 'host_device_pointer')
+    return d
 
 
 def stream_ptr(stream=None):

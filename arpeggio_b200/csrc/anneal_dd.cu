@@ -45,6 +45,8 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
   const int D = a.D, L = a.L, R = a.R;
   const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
+  pdl_trigger();
+  pdl_wait();
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
   {
@@ -348,6 +350,8 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
   const int D = a.D, L = a.L, R = a.R;
   const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
+  pdl_trigger();
+  pdl_wait();
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
   const int32_t* hg = reinterpret_cast<const int32_t*>(a.h) + (size_t)b * D;
@@ -365,15 +369,28 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
   {
     const int32_t* Gg = reinterpret_cast<const int32_t*>(a.Gt) + (size_t)b * D * D;
     bool bad = false;
-    for (int x = threadIdx.x; x < D * DP; x += blockDim.x) {
-      const int j = x / DP, i = x - j * DP;
-      int32_t v;
-      if constexpr (WARM)
-        v = i < D ? Gg[(size_t)s_perm[j] * D + s_perm[i]] : 0;
-      else
-        v = i < D ? Gg[(size_t)j * D + i] : 0;
-      bad |= (v > kMaxG || v < -kMaxG);
-      Gs[x] = v;
+    const int nG = D * DP, bt = blockDim.x;
+    for (int x0 = threadIdx.x; x0 < nG; x0 += 8 * bt) {  // eight loads in flight per thread
+      int32_t v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int x = x0 + u * bt, j = x / DP, i = x - j * DP;
+        v[u] = 0;
+        if (x < nG && i < D) {
+          if constexpr (WARM)
+            v[u] = Gg[(size_t)s_perm[j] * D + s_perm[i]];
+          else
+            v[u] = Gg[(size_t)j * D + i];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int x = x0 + u * bt;
+        if (x < nG) {
+          bad |= (v[u] > kMaxG || v[u] < -kMaxG);
+          Gs[x] = v[u];
+        }
+      }
     }
     for (int x = threadIdx.x; x < D; x += blockDim.x) bad |= (hg[x] > kMaxH || hg[x] < -kMaxH);
     for (int x = threadIdx.x; x < L; x += blockDim.x) {
@@ -679,8 +696,10 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
     b.split = (int)(sp < most ? sp : most);
     if (b.split < 1) b.split = 1;
   }
-  kern<<<(unsigned)((long long)a.B * b.split), warps * 32, smem, st>>>(b);
-  return cudaGetLastError();
+  // small integer batches (a frame's chain) launch with programmatic serialization: the kernel waits for its
+  // predecessor before any read
+  return launch_ex(kern, dim3((unsigned)((long long)a.B * b.split)), dim3(warps * 32), smem, st,
+                   !FLT && a.B <= kPdlMaxB, b);
 }
 
 template <bool CHORD, bool FLT>

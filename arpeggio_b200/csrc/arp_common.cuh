@@ -9,6 +9,35 @@
 
 namespace arp {
 
+// Programmatic dependent launch along a small batch's kernel chain.  Every kernel of the chain triggers its
+// dependents on entry; a dependent launched with programmatic serialization (launch_ex, pdl = true) may start
+// as soon as every block of its predecessor has triggered, runs only work that reads nothing the chain
+// produces (weights, the host inputs the chain's first kernel was ordered after), and calls pdl_wait() before
+// its first read of a predecessor's output: that returns once the predecessor grid has completed and its
+// writes are visible (so, transitively, every earlier kernel of the chain).  Without the launch attribute
+// both instructions do nothing.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Batches of at most this many problems launch their dependent kernels with programmatic serialization.
+constexpr int kPdlMaxB = 64;
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                             Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? at : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of two 32x32->64 multiplies,
 // Weyl key increments 0x9E3779B9 / 0xBB67AE85.  Counter (c0..c3) in place, key (k0, k1).
 // The counter layout each caller uses is the reference's (arpeggio_fx.cu:51,75; chord_kernel.cu:288,321).

@@ -38,6 +38,18 @@ extern "C" int arp_philox_rate(uint32_t* out, int blocks, int threads, int iters
 
 extern "C" const char* arp_version(void) { return "arpeggio_b200 0.1 (sm_100a)"; }
 
+extern "C" int arp_host_device_pointer(const void* host, void** dev) {
+  if (!host || !dev) return ARP_ERR_ARG;
+  *dev = nullptr;
+  void* d = nullptr;
+  if (cudaHostGetDevicePointer(&d, const_cast<void*>(host), 0) != cudaSuccess || !d) {
+    cudaGetLastError();  // reset the runtime's last error after the failed query
+    return ARP_ERR_ARG;
+  }
+  *dev = d;
+  return ARP_OK;
+}
+
 extern "C" const char* arp_status_string(int code) {
   switch (code) {
     case ARP_OK: return "ok";

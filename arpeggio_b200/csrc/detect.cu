@@ -19,10 +19,11 @@
 
 namespace arp {
 
-constexpr int kMapThreads = 256;
-// Rows of H staged per chunk: all of a 64 x 64 problem at once; 32-row chunks for the 128-wide tiles.
-template <int TB>
-__host__ __device__ constexpr int kChunkRows() { return TB <= 4 ? 64 : 32; }
+// Rows of H staged per chunk (Dp = padded width): all of a 64 x 64 problem at once; 32-row chunks at 128.
+template <int Dp>
+__host__ __device__ constexpr int kChunkRows() { return Dp <= 64 ? 64 : 32; }
+// Small batches of problems up to 64 wide take the 32 x 32 thread layout (1024 threads, 2 x 2 tiles).
+constexpr int kMapWideMaxB = 256;
 
 
 __device__ __forceinline__ float nearest_level(float v, int M) {
@@ -51,22 +52,52 @@ __device__ __forceinline__ float hsum16(float v) {
   return v;
 }
 
-// The D x D work is tiled over a 16 x 16 thread grid: thread (ty, tx) owns rows ty*TB .. ty*TB+TB-1 and
-// columns tx*TB .. tx*TB+TB-1 of Q and of the inverse, in registers.  Dp = 16 TB >= D; padded rows and
-// columns of H are zero and the padded diagonal of A is 1, so the inverse's D x D block is unchanged.
-template <int TB>
-__global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
-  constexpr int Dp = 16 * TB, QP = Dp + 4;
+// A row's dot product sum_j a_j b_j in the order of the 16 x 16 layout: each of 16 column groups is a fma chain
+// over its columns (from 0), then the butterfly hsum16 over the groups.  GS = 16: the thread's TB columns are its
+// group.  GS = 32 (TB = 2, a group of 4 columns split over an even and an odd lane): the even lane starts the
+// chain, the odd lane finishes it, the butterfly runs over the odd lanes (lane offsets 16, 8, 4, 2 are the group
+// offsets 8, 4, 2, 1) and every lane gets the result -- bit-identical to the 16 x 16 layout's sum.
+template <int TB, int GS>
+__device__ __forceinline__ float row_dot(const float (&x)[TB], const float (&y)[TB]) {
+  static_assert(GS == 16 || (GS == 32 && TB == 2), "layouts: 16 x 16, or 32 x 32 with 2 x 2 tiles");
+  float v = 0.0f;
+  if constexpr (GS == 16) {
+#pragma unroll
+    for (int j = 0; j < TB; ++j) v = __fmaf_rn(x[j], y[j], v);
+    return hsum16(v);
+  } else {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < TB; ++j) v = __fmaf_rn(x[j], y[j], v);
+    float c = __shfl_sync(ARP_FULL, v, lane & ~1);  // the odd lane continues the even lane's chain
+#pragma unroll
+    for (int j = 0; j < TB; ++j) c = __fmaf_rn(x[j], y[j], c);
+#pragma unroll
+    for (int o = 16; o >= 2; o >>= 1) c += __shfl_xor_sync(ARP_FULL, c, o);
+    return __shfl_sync(ARP_FULL, c, lane | 1);
+  }
+}
+
+// The D x D work is tiled over a GS x GS thread grid: thread (ty, tx) owns rows ty*TB .. ty*TB+TB-1 and
+// columns tx*TB .. tx*TB+TB-1 of Q and of the inverse, in registers.  Dp = GS TB >= D; padded rows and
+// columns of H are zero and the padded diagonal of A is 1, so the inverse's D x D block is unchanged.  Every
+// element sees the same operations in the same order in both layouts (GS = 16, or GS = 32 with TB = 2 for one
+// frame's latency), and the row sums go through row_dot, so the outputs are identical.
+template <int TB, int GS>
+__global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
+  constexpr int Dp = GS * TB, QP = Dp + 4, NT = GS * GS;
   extern __shared__ __align__(16) float sm[];
   float* Hc = sm;                            // kChunkRows x Dp
-  float* Qs = Hc + kChunkRows<TB>() * Dp;    // Dp x QP
+  float* Qs = Hc + kChunkRows<Dp>() * Dp;    // Dp x QP
   float* rk = Qs + Dp * QP;       // 2 x Dp (double-buffered row k)
   float* ck = rk + 2 * Dp;        // 2 x Dp (double-buffered column k)
   float* gv = ck + 2 * Dp;        // Dp
   float* xv = gv + Dp;            // Dp
-  float* red = xv + Dp;           // 8
+  float* red = xv + Dp;           // NT / 32
+  float* yc = red + NT / 32;      // kChunkRows: the chunk's rows of y
   const int D = a.D, NR2 = a.NR2, b = blockIdx.x;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4, lane = tid & 31;
+  const int tid = threadIdx.x, tx = tid % GS, ty = tid / GS, lane = tid & 31;
+  pdl_trigger();  // the chain's next kernel may launch and set up; it waits for this grid before reading
   const int u = a.idx ? a.idx[b] : b;
   const float* Hb = a.H + (size_t)u * NR2 * D;
   const float* yb = a.y + (size_t)u * NR2;
@@ -77,16 +108,17 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
     for (int j = 0; j < TB; ++j) A[i][j] = 0.0f;
   float gacc = 0.0f;
   // ---- Q = H^T H and g = H^T y over row chunks (every Q_ij, Q_ji is the same ordered fma chain)
-  constexpr int CH = kChunkRows<TB>();
+  constexpr int CH = kChunkRows<Dp>();
   for (int r0 = 0; r0 < NR2; r0 += CH) {
     const int nr = min(CH, NR2 - r0);
     __syncthreads();
+    for (int x = tid; x < nr; x += NT) yc[x] = yb[r0 + x];
     if (D == Dp && (D & 3) == 0) {
       const float4* src = reinterpret_cast<const float4*>(Hb + (size_t)r0 * D);
       float4* dst = reinterpret_cast<float4*>(Hc);
-      for (int x = tid; x < nr * Dp / 4; x += kMapThreads) dst[x] = src[x];
+      for (int x = tid; x < nr * Dp / 4; x += NT) dst[x] = src[x];
     } else {
-      for (int x = tid; x < nr * Dp; x += kMapThreads) {
+      for (int x = tid; x < nr * Dp; x += NT) {
         const int r = x / Dp, j = x - r * Dp;
         Hc[x] = j < D ? Hb[(size_t)(r0 + r) * D + j] : 0.0f;
       }
@@ -105,7 +137,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
         for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(ai[i], bj[j], A[i][j]);
     }
     if (tid < Dp)
-      for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * Dp + tid], yb[r0 + r], gacc);
+      for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * Dp + tid], yc[r], gacc);
   }
   float qmax = 0.0f;
   const float s2 = a.xg ? 0.0f : a.sigma2[b];  // only the MMSE solve reads sigma2 (null for a given guess)
@@ -130,7 +162,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
   } else {
     // ---- in-place Gauss-Jordan inverse of A = Q + sigma2 I (SPD, no pivoting), one barrier per step;
     //      k = kt*TB + kr with kr unrolled so the register tile is always indexed at compile time
-    for (int kt = 0; kt < 16; ++kt) {
+    for (int kt = 0; kt < GS; ++kt) {
 #pragma unroll
       for (int kr = 0; kr < TB; ++kr) {
         const int k = kt * TB + kr, buf = (k & 1) * Dp;
@@ -169,15 +201,15 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
     float zp[TB], mp[TB];
 #pragma unroll
     for (int i = 0; i < TB; ++i) {
-      zp[i] = 0.0f;
-      mp[i] = 0.0f;
+      float ar[TB], gj[TB], qj[TB];
 #pragma unroll
       for (int j = 0; j < TB; ++j) {
-        zp[i] = __fmaf_rn(A[i][j], gv[tx * TB + j], zp[i]);
-        mp[i] = __fmaf_rn(A[i][j], Qs[(ty * TB + i) * QP + tx * TB + j], mp[i]);
+        ar[j] = A[i][j];
+        gj[j] = gv[tx * TB + j];
+        qj[j] = Qs[(ty * TB + i) * QP + tx * TB + j];
       }
-      zp[i] = hsum16(zp[i]);
-      mp[i] = hsum16(mp[i]);
+      zp[i] = row_dot<TB, GS>(ar, gj);
+      mp[i] = row_dot<TB, GS>(ar, qj);
     }
     if (tx == 0) {
 #pragma unroll
@@ -219,7 +251,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
     __syncthreads();
     sc = 0.0f;
 #pragma unroll
-    for (int w = 0; w < kMapThreads / 32; ++w) sc = fmaxf(sc, red[w]);
+    for (int w = 0; w < NT / 32; ++w) sc = fmaxf(sc, red[w]);
     sc = fmaxf(sc, 1e-12f);
     if (tid == 0) a.scale[b] = sc;
     float* Jo = a.Jri + (size_t)b * N * N;
@@ -240,7 +272,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
         }
       }
     const float r2 = __fmul_rn(2.0f, a.r_reg);
-    for (int i = tid; i < D; i += kMapThreads) {
+    for (int i = tid; i < D; i += NT) {
       const float lv = ck[i];
       const float hv[2] = {qam ? __fmul_rn(4.0f, gv[i]) : __fmul_rn(2.0f, gv[i]), __fmul_rn(2.0f, gv[i])};
       const float sp[2] = {qam ? (lv > 0.0f ? 1.0f : -1.0f) : lv, (lv == 3.0f || lv == -1.0f) ? 1.0f : -1.0f};
@@ -258,10 +290,13 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
   float hp[TB];
 #pragma unroll
   for (int i = 0; i < TB; ++i) {
-    hp[i] = 0.0f;
+    float qj[TB], xj[TB];
 #pragma unroll
-    for (int j = 0; j < TB; ++j) hp[i] = __fmaf_rn(Qs[(ty * TB + i) * QP + tx * TB + j], xv[tx * TB + j], hp[i]);
-    hp[i] = hsum16(hp[i]);
+    for (int j = 0; j < TB; ++j) {
+      qj[j] = Qs[(ty * TB + i) * QP + tx * TB + j];
+      xj[j] = xv[tx * TB + j];
+    }
+    hp[i] = row_dot<TB, GS>(qj, xj);
     hp[i] = __fmul_rn(2.0f, __fsub_rn(gv[ty * TB + i], hp[i]));
     if (ty * TB + i < D) qmax = fmaxf(qmax, fabsf(hp[i]));
   }
@@ -271,7 +306,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
   __syncthreads();
   float sc = 0.0f;
 #pragma unroll
-  for (int w = 0; w < kMapThreads / 32; ++w) sc = fmaxf(sc, red[w]);
+  for (int w = 0; w < NT / 32; ++w) sc = fmaxf(sc, red[w]);
   sc = fmaxf(sc, 1e-12f);
   if (tid == 0) a.scale[b] = sc;
   // ---- outputs: G = Q / scale (x 4096, rounded half to even), h likewise
@@ -300,20 +335,20 @@ __global__ void __launch_bounds__(kMapThreads) k_map_dd(const MapParams a) {
   }
 }
 
-template <int TB>
+template <int TB, int GS>
 static size_t map_smem() {
-  constexpr int Dp = 16 * TB;
-  return sizeof(float) * ((size_t)kChunkRows<TB>() * Dp + (size_t)Dp * (Dp + 4) + 6 * (size_t)Dp + 8);
+  constexpr int Dp = GS * TB;
+  return sizeof(float) * ((size_t)kChunkRows<Dp>() * (Dp + 1) + (size_t)Dp * (Dp + 4) + 6 * (size_t)Dp + GS * GS / 32);
 }
 
-template <int TB>
+template <int TB, int GS = 16>
 static cudaError_t launch_map(const MapParams& a, cudaStream_t st) {
-  const size_t smem = map_smem<TB>();
+  const size_t smem = map_smem<TB, GS>();
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_map_dd<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_map_dd<TB, GS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_map_dd<TB><<<a.B, kMapThreads, smem, st>>>(a);
+  k_map_dd<TB, GS><<<a.B, GS * GS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -328,6 +363,7 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   extern __shared__ __align__(16) float sm[];
   const int D = a.D, NR2 = a.NR2, P = a.P, R = a.R, b = blockIdx.x;
   const int HS = NR2 + 1;
+  pdl_wait();
   float* Hs = sm;                   // D x HS (transposed)
   float* r0 = Hs + D * HS;          // NR2
   float* bd = r0 + NR2;             // 8
@@ -337,9 +373,21 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   const int lo = 1 - pam_size(a.M), hi = -lo;
   const int u = a.idx ? a.idx[b] : b;
   const float* Hb = a.H + (size_t)u * NR2 * D;
-  for (int x = tid; x < NR2 * D; x += kReadThreads) {
-    const int i = x / D, j = x - i * D;
-    Hs[j * HS + i] = Hb[x];
+  if ((D & 3) == 0 && (reinterpret_cast<uintptr_t>(Hb) & 15u) == 0) {  // 16-byte loads, four columns of a row
+    const float4* H4 = reinterpret_cast<const float4*>(Hb);
+    for (int x = tid; x < NR2 * D / 4; x += kReadThreads) {
+      const float4 v = H4[x];
+      const int i = (4 * x) / D, j = 4 * x - i * D;
+      Hs[j * HS + i] = v.x;
+      Hs[(j + 1) * HS + i] = v.y;
+      Hs[(j + 2) * HS + i] = v.z;
+      Hs[(j + 3) * HS + i] = v.w;
+    }
+  } else {
+    for (int x = tid; x < NR2 * D; x += kReadThreads) {
+      const int i = x / D, j = x - i * D;
+      Hs[j * HS + i] = Hb[x];
+    }
   }
   int8_t* xq8 = ek + R * D;
   for (int j = tid; j < D; j += kReadThreads)
@@ -582,6 +630,7 @@ namespace arp {
 
 cudaError_t map_dispatch(const MapParams& a, cudaStream_t st) {
   const int D = a.D;
+  if (D > 32 && D <= 64 && a.B <= kMapWideMaxB) return launch_map<2, 32>(a, st);  // one frame: 4x the warps
   return D <= 16 ? launch_map<1>(a, st) : D <= 32 ? launch_map<2>(a, st) : D <= 64 ? launch_map<4>(a, st)
                                                                           : launch_map<8>(a, st);
 }
@@ -598,8 +647,7 @@ cudaError_t readout_dispatch(const ReadParams& a, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_readout_dd<<<a.B, kReadThreads, smem, st>>>(a);
-  return cudaGetLastError();
+  return launch_ex(k_readout_dd, dim3(a.B), dim3(kReadThreads), smem, st, a.B <= kPdlMaxB, a);
 }
 
 // Workspace of the fused detector call: G, h, x_q, scale, spins, de, (flips, tests), 256-byte aligned.

@@ -256,6 +256,54 @@ static cudaError_t gemm_bn(const GemmParams& p, bool amn, bool bmn, cudaStream_t
 // ------------------------------------------------------------------------------------------------ features
 constexpr int kFeat = 16;
 
+// One coordinate's feature row (bf16, kFeat wide) and, with labels, its training label: the same arithmetic for
+// the warp-per-problem and block-per-problem kernels.
+template <typename GT>
+__device__ __forceinline__ void feature_row(const GT* __restrict__ h, const int8_t* __restrict__ xq,
+                                            const float* __restrict__ zs, size_t row, int Lmax, int P, float dg,
+                                            float ss, float mdg, float snr, float u1, float u2, bf16* __restrict__ X,
+                                            const int8_t* __restrict__ levels, int8_t* __restrict__ labels) {
+  const int x = xq[row];
+  float f[kFeat];
+#pragma unroll
+  for (int i = 0; i < kFeat; ++i) f[i] = 0.0f;
+  const float hj = (float)h[row];
+  f[0] = dg > 0.0f ? hj / (4.0f * dg) : 0.0f;  // best single-coordinate move, in level steps
+  f[1] = mdg > 0.0f ? dg / mdg : 0.0f;
+  f[2] = dg > 0.0f ? sqrtf(ss) / dg : 0.0f;  // coupling of this coordinate to the others
+  f[3] = snr;
+  f[4] = (float)x / (float)Lmax;
+  f[5] = x == Lmax ? 1.0f : 0.0f;
+  f[6] = x == -Lmax ? 1.0f : 0.0f;
+  f[7] = zs ? fminf(fmaxf(0.5f * (zs[row] - (float)x), -4.0f), 4.0f) : 0.0f;  // MMSE soft residual
+  f[8] = 1.0f;
+  f[0] = fminf(fmaxf(f[0], -8.0f), 8.0f);
+  f[2] = fminf(f[2], 64.0f);
+  f[9] = u1;
+  f[10] = u2;
+  uint32_t pk[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+    pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
+  }
+  uint4* o = reinterpret_cast<uint4*>(X + row * kFeat);
+  o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+  o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+  if (labels) {
+    int c = (levels[row] - x) / 2 + P / 2;
+    labels[row] = (int8_t)(c < 0 ? 0 : (c > P ? P : c));
+  }
+}
+
+// The greedy move of the Jacobi refinements: 2 clamp(rint(u), -1, 1), kept inside the constellation.
+__device__ __forceinline__ int jacobi_move(float u, int x, int Lmax) {
+  int m = 2 * (int)fminf(fmaxf(rintf(u), -1.0f), 1.0f);
+  if (x + m > Lmax) m = Lmax - x;
+  if (x + m < -Lmax) m = -Lmax - x;
+  return m;
+}
+
 template <typename GT>
 __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G, const GT* __restrict__ h,
                                                        const int8_t* __restrict__ xq, const float* __restrict__ zs,
@@ -299,12 +347,7 @@ __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G,
       hv[t] = j < D ? (float)h[(size_t)b * D + j] : 0.0f;
       xv[t] = j < D ? xq[(size_t)b * D + j] : 0;
     }
-    auto quant = [&](float u, int x) {
-      int m = 2 * (int)fminf(fmaxf(rintf(u), -1.0f), 1.0f);
-      if (x + m > Lmax) m = Lmax - x;
-      if (x + m < -Lmax) m = -Lmax - x;
-      return m;
-    };
+    auto quant = [&](float u, int x) { return jacobi_move(u, x, Lmax); };
 #pragma unroll
     for (int t = 0; t < 4; ++t) mq[t] = dg[t] > 0.0f ? quant(hv[t] / (4.0f * dg[t]), xv[t]) : 0;
 #pragma unroll
@@ -357,39 +400,8 @@ __global__ void __launch_bounds__(128) k_warm_features(const GT* __restrict__ G,
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
     const int j = t * 32 + lane;
-    if (j >= D) continue;
-    const size_t row = (size_t)b * D + j;
-    const int x = xq[row];
-    float f[kFeat];
-#pragma unroll
-    for (int i = 0; i < kFeat; ++i) f[i] = 0.0f;
-    const float hj = (float)h[row];
-    f[0] = dg[t] > 0.0f ? hj / (4.0f * dg[t]) : 0.0f;  // best single-coordinate move, in level steps
-    f[1] = mdg > 0.0f ? dg[t] / mdg : 0.0f;
-    f[2] = dg[t] > 0.0f ? sqrtf(ss[t]) / dg[t] : 0.0f;  // coupling of this coordinate to the others
-    f[3] = snr;
-    f[4] = (float)x / (float)Lmax;
-    f[5] = x == Lmax ? 1.0f : 0.0f;
-    f[6] = x == -Lmax ? 1.0f : 0.0f;
-    f[7] = zs ? fminf(fmaxf(0.5f * (zs[row] - (float)x), -4.0f), 4.0f) : 0.0f;  // MMSE soft residual
-    f[8] = 1.0f;
-    f[0] = fminf(fmaxf(f[0], -8.0f), 8.0f);
-    f[2] = fminf(f[2], 64.0f);
-    f[9] = u1[t];
-    f[10] = u2[t];
-    uint32_t pk[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
-      pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
-    }
-    uint4* o = reinterpret_cast<uint4*>(X + row * kFeat);
-    o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-    o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-    if (labels) {
-      int c = (levels[row] - x) / 2 + P / 2;
-      labels[row] = (int8_t)(c < 0 ? 0 : (c > P ? P : c));
-    }
+    if (j < D)
+      feature_row(h, xq, zs, (size_t)b * D + j, Lmax, P, dg[t], ss[t], mdg, snr, u1[t], u2[t], X, levels, labels);
   }
 }
 
@@ -475,6 +487,36 @@ __global__ void __launch_bounds__(256) k_adam(float* __restrict__ w, bf16* __res
 // 1 - p(m_j = 0), ties by index.  The start is kept only when its energy e0 = 2 (m^T G m - h^T m) (the dDI energy
 // change from the guess, in the units of the anneal's out_de) is no worse than the guess's (0); otherwise the
 // problem falls back to the plain MMSE start (m = 0) in index order.
+// One coordinate of the warm start from its logits z (C = P + 1 classes): the argmax spin sum clamped to the
+// constellation (returned), the order score 1 - p(m = 0), with_cdf: the sampling thresholds of softmax(tau z)
+// over the classes that stay in the constellation, and log sum_c exp(z_c - max z) (minus the log-probability of
+// the argmax class).  Shared by the warp-per-problem and block-per-problem kernels.
+__device__ __forceinline__ int start_coord(const float* __restrict__ z, int C, int P, int x, int Lmax, float tau,
+                                           bool with_cdf, float& sc, uint2& th, float& lg) {
+  float zm = z[0];
+  int am = 0;
+  for (int c = 1; c < C; ++c)
+    if (z[c] > zm) {
+      zm = z[c];
+      am = c;
+    }
+  float se = 0.0f;
+  for (int c = 0; c < C; ++c) se += __expf(z[c] - zm);
+  sc = 1.0f - __expf(z[P / 2] - zm) / se;
+  lg = __logf(se);
+  int m = 2 * am - P;
+  if (with_cdf && P == 2) {
+    const bool ok0 = x - 2 >= -Lmax, ok2 = x + 2 <= Lmax;
+    const float q0 = ok0 ? __expf(tau * (z[0] - zm)) : 0.0f, q1 = __expf(tau * (z[1] - zm));
+    const float q2 = ok2 ? __expf(tau * (z[2] - zm)) : 0.0f, qs = q0 + q1 + q2;
+    th.x = ok0 ? __float2uint_rz(q0 / qs * 4294967296.0f) : 0u;
+    th.y = ok2 ? __float2uint_rz((q0 + q1) / qs * 4294967296.0f) : 0xFFFFFFFFu;
+  }
+  if (x + m > Lmax) m = Lmax - x;
+  if (x + m < -Lmax) m = -Lmax - x;
+  return m;
+}
+
 template <typename GT, typename ET>
 __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ logits, int ldl,
                                                     const GT* __restrict__ G, const GT* __restrict__ h,
@@ -496,30 +538,10 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
     mv[t] = 0;
     sc[t] = -1.0f;
     if (j >= D) continue;
-    const float* z = logits + ((size_t)b * D + j) * ldl;
-    float zm = z[0];
-    int am = 0;
-    for (int c = 1; c < C; ++c)
-      if (z[c] > zm) {
-        zm = z[c];
-        am = c;
-      }
-    float se = 0.0f;
-    for (int c = 0; c < C; ++c) se += __expf(z[c] - zm);
-    sc[t] = 1.0f - __expf(z[P / 2] - zm) / se;
-    lse += __logf(se);
-    int m = 2 * am - P;
-    const int x = xq[(size_t)b * D + j];
-    if (cdf && P == 2) {  // sampling thresholds of softmax(tau z) over the classes that stay in the constellation
-      const bool ok0 = x - 2 >= -Lmax, ok2 = x + 2 <= Lmax;
-      const float q0 = ok0 ? __expf(tau * (z[0] - zm)) : 0.0f, q1 = __expf(tau * (z[1] - zm));
-      const float q2 = ok2 ? __expf(tau * (z[2] - zm)) : 0.0f, qs = q0 + q1 + q2;
-      th[t].x = ok0 ? __float2uint_rz(q0 / qs * 4294967296.0f) : 0u;
-      th[t].y = ok2 ? __float2uint_rz((q0 + q1) / qs * 4294967296.0f) : 0xFFFFFFFFu;
-    }
-    if (x + m > Lmax) m = Lmax - x;
-    if (x + m < -Lmax) m = -Lmax - x;
-    mv[t] = m;
+    float lg;
+    mv[t] = start_coord(logits + ((size_t)b * D + j) * ldl, C, P, xq[(size_t)b * D + j], Lmax, tau, cdf != nullptr,
+                        sc[t], th[t], lg);
+    lse += lg;
   }
   // start energy m^T G m - h^T m
   ET e = ET(0);
@@ -600,11 +622,201 @@ __global__ void __launch_bounds__(128) k_warm_start(const float* __restrict__ lo
   }
 }
 
+
+// ------------------------------------------------------------------------ small batches: a block per problem
+// A one-frame (or few-frame) batch leaves a warp per problem waiting on one G row after another.  These kernels
+// give each problem a block of 128 threads, stage its G (int32, D x D) into shared memory with every 16-byte
+// copy in flight at once, and give each coordinate a thread that runs the warp kernel's loops in the same order,
+// so every output is bit-identical to the warp kernel's; the warp reductions are replayed in their lane order.
+constexpr int kBlkThreads = 128;
+
+__device__ __forceinline__ void stage_g(int32_t* Gs, const int32_t* __restrict__ Gb, int D) {
+  const int n = D * D;
+  if (((n & 3) == 0) && ((reinterpret_cast<uintptr_t>(Gb) & 15u) == 0)) {
+    const uint32_t base = umma::su32(Gs);
+    for (int x = threadIdx.x; x < n / 4; x += blockDim.x) umma::cp16(base + 16u * x, Gb + 4 * x, true);
+    umma::cp_commit();
+    umma::cp_wait<0>();
+  } else {
+    for (int x = threadIdx.x; x < n; x += blockDim.x) Gs[x] = Gb[x];
+  }
+}
+
+// The warp kernels' butterfly sum of per-lane partials, lane l holding coordinates l, 32 + l, 64 + l, 96 + l
+// summed in that order (absent coordinates contribute nothing): warp 0 of the block computes it from v (128
+// entries in shared memory) and returns it in every lane of warp 0.
+template <typename T>
+__device__ __forceinline__ T lane_order_sum(const T* v, int D) {
+  const int lane = threadIdx.x & 31;
+  T a = T(0);
+#pragma unroll
+  for (int t = 0; t < 4; ++t)
+    if (t * 32 + lane < D) a += v[t * 32 + lane];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  return a;
+}
+
+__global__ void __launch_bounds__(kBlkThreads) k_warm_features_blk(const int32_t* __restrict__ G,
+                                                                   const int32_t* __restrict__ h,
+                                                                   const int8_t* __restrict__ xq,
+                                                                   const float* __restrict__ zs,
+                                                                   const float* __restrict__ snr_db, int D, int M,
+                                                                   int P, bf16* __restrict__ X,
+                                                                   const int8_t* __restrict__ levels,
+                                                                   int8_t* __restrict__ labels) {
+  extern __shared__ __align__(16) int32_t Gs[];
+  __shared__ float s_dg[128];
+  __shared__ int s_mq[128];
+  __shared__ float s_mdg;
+  const int b = blockIdx.x, j = threadIdx.x;
+  pdl_trigger();
+  pdl_wait();
+  stage_g(Gs, G + (size_t)b * D * D, D);
+  __syncthreads();
+  float dg = 0.0f, ss = 0.0f;
+  if (j < D)
+    for (int i = 0; i < D; ++i) {
+      const float g = (float)Gs[i * D + j];
+      if (i == j)
+        dg = g;
+      else
+        ss = fmaf(g, g, ss);
+    }
+  s_dg[j] = dg;
+  __syncthreads();
+  if (j < 32) {
+    const float sdg = lane_order_sum(s_dg, 128);  // the warp kernel adds the zero dg of absent coordinates too
+    if (j == 0) s_mdg = sdg / (float)D;
+  }
+  const int Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
+  const float hv = j < D ? (float)h[(size_t)b * D + j] : 0.0f;
+  const int xv = j < D ? xq[(size_t)b * D + j] : 0;
+  int mq = dg > 0.0f ? jacobi_move(hv / (4.0f * dg), xv, Lmax) : 0;
+  s_mq[j] = mq;
+  __syncthreads();
+  float u1 = 0.0f, u2 = 0.0f;
+  for (int pass = 0; pass < 2; ++pass) {
+    float acc = 0.0f;
+    if (j < D)
+      for (int i = 0; i < D; ++i) {
+        const int mi = s_mq[i];
+        if (mi != 0 && i != j) acc = fmaf((float)Gs[i * D + j], (float)mi, acc);
+      }
+    const float v = dg > 0.0f ? (hv - 2.0f * acc) / (4.0f * dg) : 0.0f;
+    const float uc = fminf(fmaxf(v, -8.0f), 8.0f);
+    if (pass == 0)
+      u1 = uc;
+    else
+      u2 = uc;
+    mq = j < D && dg > 0.0f ? jacobi_move(uc, xv, Lmax) : 0;
+    __syncthreads();
+    s_mq[j] = mq;
+    __syncthreads();
+  }
+  const float snr = snr_db ? snr_db[b] * 0.05f : 0.0f;
+  if (j < D)
+    feature_row(h, xq, zs, (size_t)b * D + j, Lmax, P, dg, ss, s_mdg, snr, u1, u2, X, levels, labels);
+}
+
+__global__ void __launch_bounds__(kBlkThreads) k_warm_start_blk(const float* __restrict__ logits, int ldl,
+                                                                const int32_t* __restrict__ G,
+                                                                const int32_t* __restrict__ h,
+                                                                const int8_t* __restrict__ xq, int D, int P, int M,
+                                                                int8_t* __restrict__ m0, uint8_t* __restrict__ perm,
+                                                                long long* __restrict__ e0,
+                                                                int32_t* __restrict__ kept, float tau,
+                                                                uint2* __restrict__ cdf, float conf_min, int r_easy,
+                                                                int R, int32_t* __restrict__ ra) {
+  extern __shared__ __align__(16) int32_t Gs[];
+  __shared__ float s_sc[128], s_lg[128];
+  __shared__ int s_m[128];
+  __shared__ long long s_e[kBlkThreads / 32];
+  __shared__ int s_keep;
+  __shared__ float s_lse;
+  const int b = blockIdx.x, j = threadIdx.x, lane = j & 31, w = j >> 5;
+  pdl_trigger();
+  pdl_wait();
+  const int32_t* Gb = G + (size_t)b * D * D;
+  // the copies of G fly while the logits are read
+  const int n = D * D;
+  const bool vec = ((n & 3) == 0) && ((reinterpret_cast<uintptr_t>(Gb) & 15u) == 0);
+  if (vec) {
+    const uint32_t base = umma::su32(Gs);
+    for (int x = j; x < n / 4; x += blockDim.x) umma::cp16(base + 16u * x, Gb + 4 * x, true);
+    umma::cp_commit();
+  } else {
+    for (int x = j; x < n; x += blockDim.x) Gs[x] = Gb[x];
+  }
+  const int C = P + 1, Lmax = M == 4 ? 1 : (M == 16 ? 3 : 7);
+  int mv = 0;
+  float sc = -1.0f, lg = 0.0f;
+  uint2 th = make_uint2(0u, 0xFFFFFFFFu);
+  if (j < D)
+    mv = start_coord(logits + ((size_t)b * D + j) * ldl, C, P, xq[(size_t)b * D + j], Lmax, tau, cdf != nullptr,
+                     sc, th, lg);
+  s_m[j] = mv;
+  s_sc[j] = sc;
+  s_lg[j] = lg;
+  if (vec) umma::cp_wait<0>();
+  __syncthreads();
+  // start energy m^T G m - h^T m, exact in 64-bit integers (any order)
+  long long e = 0;
+  if (j < D && mv != 0) {
+    for (int i = 0; i < D; ++i) {
+      const int mi = s_m[i];
+      if (mi != 0) e += (long long)Gs[i * D + j] * (long long)(mi * mv);
+    }
+  }
+  if (j < D) e -= (long long)h[(size_t)b * D + j] * (long long)mv;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if (lane == 0) s_e[w] = e;
+  // rank by descending score (ties by index)
+  int rk = 0;
+  if (j < D)
+    for (int i = 0; i < D; ++i) {
+      const float si = s_sc[i];
+      if (si > sc || (si == sc && i < j)) ++rk;
+    }
+  __syncthreads();
+  if (j == 0) {
+    long long et = 0;
+    for (int q = 0; q < kBlkThreads / 32; ++q) et += s_e[q];
+    et = et + et;  // the anneal's energy units
+    s_keep = et <= 0 ? 1 : 0;
+    if (e0) e0[b] = et <= 0 ? et : 0;
+    if (kept) kept[b] = et <= 0 ? 1 : 0;
+  }
+  if (ra && j < 32) {
+    const float lse = lane_order_sum(s_lg, D);
+    if (j == 0) s_lse = lse;
+  }
+  __syncthreads();
+  const bool keep = s_keep != 0;
+  if (j < D) {
+    m0[(size_t)b * D + j] = (int8_t)(keep ? mv : 0);
+    perm[(size_t)b * D + (keep ? rk : j)] = (uint8_t)j;
+    if (cdf) cdf[(size_t)b * D + j] = keep ? th : make_uint2(0u, 0xFFFFFFFFu);
+  }
+  if (ra && j == 0) ra[b] = (keep && -s_lse > conf_min) ? r_easy : R;
+}
 }  // namespace arp
 
 using namespace arp;
 
 static bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Batches of at most this many problems (integer fields) use the block-per-problem features and start kernels.
+constexpr int kSmallBatch = 2048;
+
+// Opts a block-per-problem kernel into D x D int32 of dynamic shared memory (64 KB at D = 128).
+template <typename K>
+static cudaError_t blk_smem_attr(K kern, int D) {
+  const int bytes = D * D * 4;
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
 
 extern "C" int arp_gemm_bf16(const void* A, int a_mn_major, int lda, const void* B, int b_mn_major, int ldb, int M,
                              int N, int K, int epilogue, const float* bias, const void* aux, int ld_aux, void* C,
@@ -641,7 +853,13 @@ extern "C" int arp_warm_features(const void* G, const void* h, const int8_t* xq,
   if (!G || !h || !xq || !X || !al16(X) || (labels && !levels)) return ARP_ERR_ARG;
   const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
   cudaStream_t st = (cudaStream_t)stream;
-  if (quantized)
+  if (quantized && B <= kSmallBatch) {
+    if (blk_smem_attr(k_warm_features_blk, D) != cudaSuccess) return ARP_ERR_LAUNCH;
+    if (launch_ex(k_warm_features_blk, dim3(B), dim3(kBlkThreads), (size_t)D * D * 4, st, B <= kPdlMaxB,
+                  (const int32_t*)G, (const int32_t*)h, xq, zs, snr_db, D, M, P, (bf16*)X, levels, labels) !=
+        cudaSuccess)
+      return ARP_ERR_LAUNCH;
+  } else if (quantized)
     k_warm_features<int32_t><<<nb, th, 0, st>>>((const int32_t*)G, (const int32_t*)h, xq, zs, snr_db, B, D, M, P,
                                                 (bf16*)X, levels, labels);
   else
@@ -692,7 +910,13 @@ extern "C" int arp_warm_start_sampled(const float* logits, int ldl, const void* 
   if (ra && (R < 1 || r_easy < 1 || r_easy > R)) return ARP_ERR_ARG;
   const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
   cudaStream_t st = (cudaStream_t)stream;
-  if (quantized)
+  if (quantized && B <= kSmallBatch) {
+    if (blk_smem_attr(k_warm_start_blk, D) != cudaSuccess) return ARP_ERR_LAUNCH;
+    if (launch_ex(k_warm_start_blk, dim3(B), dim3(kBlkThreads), (size_t)D * D * 4, st, B <= kPdlMaxB, logits, ldl,
+                  (const int32_t*)G, (const int32_t*)h, xq, D, P, M, m0, perm, (long long*)e0, kept, tau,
+                  (uint2*)cdf, conf_min, r_easy, R, ra) != cudaSuccess)
+      return ARP_ERR_LAUNCH;
+  } else if (quantized)
     k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
                                                         P, M, m0, perm, (long long*)e0, kept, tau, (uint2*)cdf,
                                                         conf_min, r_easy, R, ra);
@@ -712,7 +936,13 @@ extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const
   if (!logits || !G || !h || !xq || !m0 || !perm) return ARP_ERR_ARG;
   const int th = 128, nb = (int)(((size_t)B * 32 + th - 1) / th);
   cudaStream_t st = (cudaStream_t)stream;
-  if (quantized)
+  if (quantized && B <= kSmallBatch) {
+    if (blk_smem_attr(k_warm_start_blk, D) != cudaSuccess) return ARP_ERR_LAUNCH;
+    if (launch_ex(k_warm_start_blk, dim3(B), dim3(kBlkThreads), (size_t)D * D * 4, st, B <= kPdlMaxB, logits, ldl,
+                  (const int32_t*)G, (const int32_t*)h, xq, D, P, M, m0, perm, (long long*)e0, kept, 1.0f,
+                  (uint2*)nullptr, 0.0f, 1, 1, (int32_t*)nullptr) != cudaSuccess)
+      return ARP_ERR_LAUNCH;
+  } else if (quantized)
     k_warm_start<int32_t, long long><<<nb, th, 0, st>>>(logits, ldl, (const int32_t*)G, (const int32_t*)h, xq, B, D,
                                                         P, M, m0, perm, (long long*)e0, kept, 1.0f, nullptr, 0.0f, 1, 1,
                                                         nullptr);
@@ -750,6 +980,7 @@ struct MlpParams {
   float* logits;
   int rows;
   int32_t* status;
+  int bias16;  // b1 and b2 16-byte aligned: staged with cp.async
 };
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
@@ -816,10 +1047,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntiles = (p.rows + 127) / 128;
   if ((int)blockIdx.x >= ntiles) return;
-  for (int i = tid; i < 512; i += kMlpThreads) {
-    s_b1[i] = p.b1[i];
-    s_b2[i] = p.b2[i];
-  }
+  pdl_trigger();
   const uint32_t hs = umma::su32(smem), xs = hs + kHsBytes, ring = xs + kXsBytes;
   const uint32_t w1s = ring + 3 * kSlotBytes, w3s = ring + 2 * kSlotBytes;
   constexpr uint32_t ID_HID = umma::idesc_bf16(256, false, false), ID_OUT = umma::idesc_bf16(16, false, true);
@@ -839,6 +1067,16 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
   __syncthreads();
   umma::tc_after_sync();
   const uint32_t tmem = s_tmem;
+  pdl_wait();  // everything above touches no global memory
+  // biases: one 16-byte copy per thread (128 of b1, 128 of b2), landing with the first tile's X and W1
+  if (p.bias16)
+    umma::cp16(umma::su32(tid < 128 ? s_b1 + 4 * tid : s_b2 + 4 * (tid - 128)),
+               tid < 128 ? p.b1 + 4 * tid : p.b2 + 4 * (tid - 128), true);
+  else
+    for (int i = tid; i < 512; i += kMlpThreads) {
+      s_b1[i] = p.b1[i];
+      s_b2[i] = p.b2[i];
+    }
 
   auto load_x = [&](int tile) {  // 128 x 16: one 16-byte chunk per thread
     const int row = tid >> 1, kc = tid & 1, m = tile * 128 + row;
@@ -877,6 +1115,11 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
   int it = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
     const int g0 = it * 32;
+    // W2 chunks 0-2 go to slots 0-2 at once (free: the previous tile's L2 and L3 have completed), so they
+    // stream while X and W1 land and layer 1 runs
+    if (tid == 0)
+      for (int g = g0; g < g0 + 3; ++g)
+        if (!produce(g)) s_abort = 1;
     // ---- layer 1 (X and W1 landed; the previous tile's TMEM reads are done)
     umma::cp_wait<0>();
     umma::fence_async_smem();
@@ -890,9 +1133,6 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
       umma::mma(tmem + 256, ad, umma::sdesc(w1s + 8192, 128, 256), ID_HID, 0u);
       umma::commit(&bar_l1);
     }
-    if (tid == 0)  // chunks 0-2 go to slots 0-2 (free: the previous tile's L2 and L3 have completed)
-      for (int g = g0; g < g0 + 3; ++g)
-        if (!produce(g)) s_abort = 1;
     if (!umma::mbar_wait(&bar_l1, it & 1)) s_abort = 1;
     umma::tc_after_sync();
     mlp_epi_hidden(tmem, hs, s_b1, warp, lane);
@@ -996,9 +1236,13 @@ extern "C" int arp_mlp_forward(const void* X, int rows, const void* W1, const fl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (rows + 127) / 128;
-  MlpParams p{(const bf16*)X, (const bf16*)W1, (const bf16*)W2p, (const bf16*)W3t, b1, b2, b3, logits, rows, status};
-  k_mlp_fused<<<ntiles < sms ? ntiles : sms, kMlpThreads, kMlpSmem, (cudaStream_t)stream>>>(p);
-  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+  MlpParams p{(const bf16*)X, (const bf16*)W1, (const bf16*)W2p, (const bf16*)W3t, b1, b2, b3, logits, rows, status,
+              al16(b1) && al16(b2) ? 1 : 0};
+  const bool pdl = rows <= kPdlMaxB * 128;
+  return launch_ex(k_mlp_fused, dim3(ntiles < sms ? ntiles : sms), dim3(kMlpThreads), kMlpSmem, (cudaStream_t)stream,
+                   pdl, p) == cudaSuccess
+             ? ARP_OK
+             : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_mlp_pack_w2(const void* W2, void* W2p, void* stream) {

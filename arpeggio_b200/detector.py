@@ -121,6 +121,7 @@ class Detector:
         self._out = torch.empty(self._out_off + 4 * B, dtype=torch.uint8, device=dev)
         self.bits = self._out[:nb].view(torch.int8).view(B, D * PAM[M]['bits'])
         self.dist = self._out[self._out_off:].view(torch.float32)
+        self._frame_out = None  # (bits, dist) device addresses of mapped host outputs while a frame is captured
         self.pick = torch.empty(B, dtype=torch.int32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self._inst_base = None
@@ -179,8 +180,9 @@ class Detector:
         _lib.check(rc, 'anneal')
         ev(2)
         levels, bits, dist, pick = self.levels[sl], self.bits[sl], self.dist[sl], self.pick[sl]
+        whole = None if (off == 0 and n == self.B) else sl
         _lib.check(L.arp_readout_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(xq), _lib.ptr(spins), n, NR2, D, P,
-                                    R, self.M, _lib.ptr(levels), _lib.ptr(bits), _lib.ptr(dist),
+                                    R, self.M, _lib.ptr(levels), self._out_ptr(0, whole), self._out_ptr(1, whole),
                                     _lib.ptr(pick), sp), 'readout')
         ev(3)
         return bits, levels, dist
@@ -211,11 +213,19 @@ class Detector:
                              0 if self.policy == 'arpeggio' else 1, 1 if f32 else 0, self.P, self.R,
                              _lib.ptr(self.T), _lib.ptr(self.c), int(self.T.shape[0]), float(self.q),
                              inst0 & M32, seed & M32, (seed >> 32) & M32, 0 if self.start == 'rand' else 1,
-                             _lib.ptr(self.workspace), self.workspace.numel(), _lib.ptr(self.bits),
-                             _lib.ptr(self.levels), _lib.ptr(self.dist), _lib.ptr(self.pick), _lib.ptr(self.status),
+                             _lib.ptr(self.workspace), self.workspace.numel(), self._out_ptr(0),
+                             _lib.ptr(self.levels), self._out_ptr(1), _lib.ptr(self.pick), _lib.ptr(self.status),
                              _lib.stream_ptr(stream))
         _lib.check(rc, 'detect')
         return self.bits, self.levels, self.dist
+
+    def _out_ptr(self, i, sl=None):
+        """Readout destination: bits (i = 0) or distances (i = 1) of the whole batch, or the mapped host
+        outputs of a frame being captured."""
+        if self._frame_out is not None and sl is None:
+            return self._frame_out[i]
+        t = self.bits if i == 0 else self.dist
+        return _lib.ptr(t if sl is None else t[sl])
 
     def run_host(self, Hh, yh, seed, bits_out, dist_out, Hd, yd, chunks=8, inst0=0, stream=None):
         """End-to-end detection from pinned host buffers: the batch is cut into `chunks` pieces; the host to
@@ -269,11 +279,13 @@ class Detector:
     def _adjacent(a, b):
         return a.is_contiguous() and b.is_contiguous() and b.data_ptr() == a.data_ptr() + a.numel() * a.element_size()
 
-    def capture(self, Hh, yh, seed, bits_out, dist_out, Hd, yd):
-        """A CUDA graph of one whole-batch detection from pinned host buffers: copy H, y in, detect, copy bits
-        and distances out.  Replaying it re-runs the same seed on whatever the pinned inputs hold, with no host
-        work per frame beyond the launch of the graph (the serving path for small frames).  Warms the launch
-        configuration up first, outside the capture."""
+    def capture(self, Hh, yh, seed, bits_out, dist_out, Hd, yd, zero_copy=True):
+        """A CUDA graph of one whole-batch detection from pinned host buffers: copy H, y in, detect, bits and
+        distances out -- with zero_copy the readout writes them straight into the mapped pinned outputs (no copy
+        node; the graph's completion makes them visible to the host), else one copy back.  Replaying it re-runs
+        the same seed on whatever the pinned inputs hold, with no host work per frame beyond the launch of the
+        graph (the serving path for small frames).  Warms the launch configuration up first, outside the
+        capture."""
         import torch
         s = torch.cuda.Stream(device=self.device)
         s.wait_stream(torch.cuda.current_stream())
@@ -288,6 +300,9 @@ class Detector:
         n_out = self._out_off + 4 * self.B
         one_out = (bits_out.data_ptr() + self._out_off == dist_out.data_ptr() and bits_out.is_contiguous()
                    and dist_out.numel() == self.B)
+        direct = None
+        if zero_copy and bits_out.is_contiguous() and dist_out.is_contiguous():
+            direct = (_lib.host_device_ptr(bits_out), _lib.host_device_ptr(dist_out))
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
             if one_in:  # H and y side by side on both ends: one copy
@@ -296,10 +311,14 @@ class Detector:
             else:
                 Hd.copy_(Hh, non_blocking=True)
                 yd.copy_(yh, non_blocking=True)
-            bits, _, dist = self.run(Hd, yd, seed)
-            if one_out:
+            self._frame_out = direct
+            try:
+                bits, _, dist = self.run(Hd, yd, seed)
+            finally:
+                self._frame_out = None
+            if direct is None and one_out:
                 bits_out.view(-1).view(torch.uint8).as_strided((n_out,), (1,)).copy_(self._out, non_blocking=True)
-            else:
+            elif direct is None:
                 bits_out.copy_(bits, non_blocking=True)
                 dist_out.copy_(dist, non_blocking=True)
         return g

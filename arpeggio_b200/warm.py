@@ -285,8 +285,10 @@ class WarmDetector(Detector):
         _lib.check(rc, 'anneal')
         ev(3 if e5 else 2)
         levels, bits, dist, pick = self.levels[sl], self.bits[sl], self.dist[sl], self.pick[sl]
+        whole = None if (off == 0 and n == self.B) else sl
         _lib.check(L.arp_readout_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(xq), _lib.ptr(spins), n, NR2, D, P, R, self.M,
-                                    _lib.ptr(levels), _lib.ptr(bits), _lib.ptr(dist), _lib.ptr(pick), sp), 'readout')
+                                    _lib.ptr(levels), self._out_ptr(0, whole), self._out_ptr(1, whole), _lib.ptr(pick),
+                                    sp), 'readout')
         ev(4 if e5 else 3)
         return bits, levels, dist
 

@@ -34,6 +34,11 @@ enum arp_status_code {
 const char* arp_version(void);
 const char* arp_status_string(int code);
 
+/* The device address of page-locked host memory (cudaHostAlloc'd, mapped): kernels may write results straight
+ * into it, so a captured one-frame detection needs no copy back.  ARP_ERR_ARG if host is not mapped memory.
+ * Host only; no counterpart in the reference. */
+int arp_host_device_pointer(const void* host, void** dev);
+
 /* Philox4x32-10 known-answer check on the device: in (n x 6 words: counter c0..c3, key k0, k1),
  * out (n x 4 words).  Replaces chord_kernel.cu:26-32 `philox_kat` (launched by
  * arpeggio/mimo/chordfx.py:180-187). */

@@ -268,10 +268,11 @@ def test_trained_network_beats_the_plain_start_at_the_same_budget():
     assert res['warm'][1] <= res['plain'][1] * 1.02, res
 
 
+@pytest.mark.parametrize('zero_copy', [True, False])
 @pytest.mark.parametrize('warm_start', [False, True])
-def test_frame_graph_with_one_copy_each_way_equals_run(warm_start):
+def test_frame_graph_with_one_copy_each_way_equals_run(warm_start, zero_copy):
     """A captured frame whose H and y sit side by side (one copy in) and whose bits and distances leave in one copy
-    gives the detector's own results."""
+    (or are written by the readout straight into the mapped pinned outputs) gives the detector's own results."""
     from arpeggio_b200 import channel, warm
     mlp = warm.WarmMLP(P=2, seed=2) if warm_start else None
     f = channel.draw_device(31, 12.0, 4, 32, 16)
@@ -282,8 +283,10 @@ def test_frame_graph_with_one_copy_each_way_equals_run(warm_start):
     Hh, yh, Hd, yd, bo, do = det.frame_buffers()
     Hh.copy_(f['H'].cpu())
     yh.copy_(f['y'].cpu())
-    g = det.capture(Hh, yh, 5, bo, do, Hd, yd)
+    g = det.capture(Hh, yh, 5, bo, do, Hd, yd, zero_copy=zero_copy)
     det.bits.zero_()
+    bo.zero_()
+    do.zero_()
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(bo, ref_bits.cpu()) and torch.equal(do, ref_dist.cpu())
@@ -420,3 +423,52 @@ def test_per_problem_anneal_counts_match_oracle():
         k = int(rd[b])
         assert np.array_equal(so[b, :k], sf[b, :k]) and np.array_equal(deo[b, :k], def_[b, :k])
         assert (so[b, k:] == 0).all() and (deo[b, k:] == np.iinfo(np.int64).max).all() and (sto[b, k:] == 0).all()
+
+
+@pytest.mark.parametrize('nt', [8, 32, 64])
+def test_block_per_problem_kernels_equal_the_warp_kernels(nt):
+    """Batches of at most 2048 problems take the block-per-problem features and start kernels (G staged in
+    shared memory); their outputs are bit-identical to the warp-per-problem kernels' on the same problems."""
+    from arpeggio_b200 import _lib
+    Bb, Bs = 2100, 64
+    d, det = _problems(Bb, nt, 16.0, 50 + nt)
+    D = 2 * nt
+    L = _lib.lib()
+    snr = torch.full((Bb,), 16.0, device='cuda')
+    Xb = torch.empty(Bb * D, 16, dtype=torch.bfloat16, device='cuda')
+    Xs = torch.empty(Bs * D, 16, dtype=torch.bfloat16, device='cuda')
+    lb = torch.empty(Bb * D, dtype=torch.int8, device='cuda')
+    ls = torch.empty(Bs * D, dtype=torch.int8, device='cuda')
+    for B, X, lab in ((Bb, Xb, lb), (Bs, Xs, ls)):
+        _lib.check(L.arp_warm_features(_lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(det.xq), _lib.ptr(det.zs),
+                                       _lib.ptr(snr), B, D, 16, 2, 1, _lib.ptr(X), _lib.ptr(det.levels), _lib.ptr(lab),
+                                       _lib.stream_ptr()), 'features')
+    torch.cuda.synchronize()
+    assert torch.equal(Xb[:Bs * D].view(torch.int16), Xs.view(torch.int16))
+    assert torch.equal(lb[:Bs * D], ls)
+    cls = (det.levels.long() - det.xq.long()) // 2 + 1
+    g = torch.Generator().manual_seed(nt)
+    Zc = torch.randn(Bb * D, 16, generator=g).cuda()
+    Zc[torch.arange(Bb * D), cls.reshape(-1).clamp(0, 2)] += 2.0 + 4.0 * torch.rand(Bb * D, generator=g).cuda()
+
+    def start(B, sampled):
+        o = (torch.empty(B, D, dtype=torch.int8, device='cuda'), torch.empty(B, D, dtype=torch.uint8, device='cuda'),
+             torch.empty(B, dtype=torch.int64, device='cuda'), torch.empty(B, dtype=torch.int32, device='cuda'),
+             torch.empty(B, D, 2, dtype=torch.int32, device='cuda'), torch.empty(B, dtype=torch.int32, device='cuda'))
+        args = [_lib.ptr(Zc), 16, _lib.ptr(det.G), _lib.ptr(det.h), _lib.ptr(det.xq), B, D, 2, 16, 1] + \
+            [_lib.ptr(t) for t in o[:4]]
+        if sampled:
+            _lib.check(L.arp_warm_start_sampled(*args, 0.8, _lib.ptr(o[4]), -5.0 * D / 64, 8, 32, _lib.ptr(o[5]),
+                                                _lib.stream_ptr()), 'start')
+        else:
+            _lib.check(L.arp_warm_start(*args, _lib.stream_ptr()), 'start')
+        torch.cuda.synchronize()
+        return o if sampled else o[:4]
+
+    for sampled in (False, True):
+        big, small = start(Bb, sampled), start(Bs, sampled)
+        assert int(big[3].sum()) > 0 and int(big[3].sum()) < Bb
+        for a, b in zip(big, small):
+            assert torch.equal(a[:Bs], b)
+        if sampled:
+            assert 0 < int((big[5] == 8).sum()) < Bb

@@ -22,9 +22,6 @@ namespace arp {
 // Rows of H staged per chunk (Dp = padded width): all of a 64 x 64 problem at once; 32-row chunks at 128.
 template <int Dp>
 __host__ __device__ constexpr int kChunkRows() { return Dp <= 64 ? 64 : 32; }
-// Small batches of problems up to 64 wide take the 32 x 32 thread layout (1024 threads, 2 x 2 tiles).
-constexpr int kMapWideMaxB = 256;
-
 
 __device__ __forceinline__ float nearest_level(float v, int M) {
   if (M == 4) return fabsf(v - 1.0f) < fabsf(v + 1.0f) ? 1.0f : -1.0f;  // ties -> the first level, -1
@@ -52,37 +49,21 @@ __device__ __forceinline__ float hsum16(float v) {
   return v;
 }
 
-// A row's dot product sum_j a_j b_j in the order of the 16 x 16 layout: each of 16 column groups is a fma chain
-// over its columns (from 0), then the butterfly hsum16 over the groups.  GS = 16: the thread's TB columns are its
-// group.  GS = 32 (TB = 2, a group of 4 columns split over an even and an odd lane): the even lane starts the
-// chain, the odd lane finishes it, the butterfly runs over the odd lanes (lane offsets 16, 8, 4, 2 are the group
-// offsets 8, 4, 2, 1) and every lane gets the result -- bit-identical to the 16 x 16 layout's sum.
-template <int TB, int GS>
+// A row's dot product sum_j x_j y_j: the thread's TB columns as one fma chain (from 0), then the butterfly over
+// the 16 threads of the row.
+template <int TB>
 __device__ __forceinline__ float row_dot(const float (&x)[TB], const float (&y)[TB]) {
-  static_assert(GS == 16 || (GS == 32 && TB == 2), "layouts: 16 x 16, or 32 x 32 with 2 x 2 tiles");
   float v = 0.0f;
-  if constexpr (GS == 16) {
 #pragma unroll
-    for (int j = 0; j < TB; ++j) v = __fmaf_rn(x[j], y[j], v);
-    return hsum16(v);
-  } else {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int j = 0; j < TB; ++j) v = __fmaf_rn(x[j], y[j], v);
-    float c = __shfl_sync(ARP_FULL, v, lane & ~1);  // the odd lane continues the even lane's chain
-#pragma unroll
-    for (int j = 0; j < TB; ++j) c = __fmaf_rn(x[j], y[j], c);
-#pragma unroll
-    for (int o = 16; o >= 2; o >>= 1) c += __shfl_xor_sync(ARP_FULL, c, o);
-    return __shfl_sync(ARP_FULL, c, lane | 1);
-  }
+  for (int j = 0; j < TB; ++j) v = __fmaf_rn(x[j], y[j], v);
+  return hsum16(v);
 }
 
-// The D x D work is tiled over a GS x GS thread grid: thread (ty, tx) owns rows ty*TB .. ty*TB+TB-1 and
-// columns tx*TB .. tx*TB+TB-1 of Q and of the inverse, in registers.  Dp = GS TB >= D; padded rows and
-// columns of H are zero and the padded diagonal of A is 1, so the inverse's D x D block is unchanged.  Every
-// element sees the same operations in the same order in both layouts (GS = 16, or GS = 32 with TB = 2 for one
-// frame's latency), and the row sums go through row_dot, so the outputs are identical.
+// The D x D work is tiled over a GS x GS (16 x 16) thread grid: thread (ty, tx) owns rows ty*TB .. ty*TB+TB-1
+// and columns tx*TB .. tx*TB+TB-1 of Q and of the inverse, in registers.  Dp = GS TB >= D; padded rows and
+// columns of H are zero and the padded diagonal of A is 1, so the inverse's D x D block is unchanged.  (A 32 x 32
+// grid of 2 x 2 tiles was measured for one frame and is slower: the 64 elimination steps are latency-bound and
+// a 1024-thread barrier per step costs more than the smaller tiles save.)
 template <int TB, int GS>
 __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
   constexpr int Dp = GS * TB, QP = Dp + 4, NT = GS * GS;
@@ -208,8 +189,8 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
         gj[j] = gv[tx * TB + j];
         qj[j] = Qs[(ty * TB + i) * QP + tx * TB + j];
       }
-      zp[i] = row_dot<TB, GS>(ar, gj);
-      mp[i] = row_dot<TB, GS>(ar, qj);
+      zp[i] = row_dot<TB>(ar, gj);
+      mp[i] = row_dot<TB>(ar, qj);
     }
     if (tx == 0) {
 #pragma unroll
@@ -296,7 +277,7 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
       qj[j] = Qs[(ty * TB + i) * QP + tx * TB + j];
       xj[j] = xv[tx * TB + j];
     }
-    hp[i] = row_dot<TB, GS>(qj, xj);
+    hp[i] = row_dot<TB>(qj, xj);
     hp[i] = __fmul_rn(2.0f, __fsub_rn(gv[ty * TB + i], hp[i]));
     if (ty * TB + i < D) qmax = fmaxf(qmax, fabsf(hp[i]));
   }
@@ -359,6 +340,8 @@ constexpr int kReadThreads = 256;
 // 32 lanes of a warp, which own rows i = lane + 32 m, read consecutive words.  r0 = y - H x_q is formed once;
 // candidate c's residual is r0 - sum_j H[:, j] e_j over the few coordinates where its clipped level differs
 // from the guess (e = x - x_q), and its distance is ||r||^2.
+// MR: rows of H per lane (NR2 <= 32 MR); rows beyond NR2 add exact zeros, so every MR gives the same sums.
+template <int MR>
 __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a) {
   extern __shared__ __align__(16) float sm[];
   const int D = a.D, NR2 = a.NR2, P = a.P, R = a.R, b = blockIdx.x;
@@ -395,17 +378,39 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
   __syncthreads();
   // every candidate's clipped delta from the guess, from one coalesced pass over its spins
   const int8_t* sb = a.spins + (size_t)b * R * P * D;  // spins are per problem b (group-local)
-  for (int x = tid; x < R * D; x += kReadThreads) {
-    const int c = x / D, j = x - c * D;
-    int xv;
-    if (a.ri) {  // RI spins: l = 2 s1 + s2 (16-QAM) or s (QPSK), mimo.spins_to_levels (mimo.py:39-42)
-      xv = P == 1 ? sb[(size_t)c * D + j] : 2 * sb[(size_t)c * 2 * D + j] + sb[(size_t)c * 2 * D + D + j];
-    } else {
-      int d = 0;
-      for (int p = 0; p < P; ++p) d += sb[(size_t)c * P * D + p * D + j];
-      xv = min(max((int)xq8[j] + d, lo), hi);
+  if (!a.ri && (D & 15) == 0 && P <= 6 && (reinterpret_cast<uintptr_t>(sb) & 15u) == 0) {
+    // 16 coordinates of one candidate per thread: its P 16-byte spin loads are all in flight at once
+    const int ng = D >> 4;
+    for (int x = tid; x < R * ng; x += kReadThreads) {
+      const int c = x / ng, j0 = (x - c * ng) << 4;
+      int4 sv[6];
+#pragma unroll
+      for (int p = 0; p < 6; ++p)
+        if (p < P) sv[p] = *reinterpret_cast<const int4*>(sb + (size_t)c * P * D + p * D + j0);
+      int8_t* ec = ek + c * D + j0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        int d = 0;
+#pragma unroll
+        for (int p = 0; p < 6; ++p)
+          if (p < P) d += reinterpret_cast<const int8_t*>(&sv[p])[q];
+        const int xv = min(max((int)xq8[j0 + q] + d, lo), hi);
+        ec[q] = (int8_t)(xv - xq8[j0 + q]);
+      }
     }
-    ek[x] = (int8_t)(xv - xq8[j]);
+  } else {
+    for (int x = tid; x < R * D; x += kReadThreads) {
+      const int c = x / D, j = x - c * D;
+      int xv;
+      if (a.ri) {  // RI spins: l = 2 s1 + s2 (16-QAM) or s (QPSK), mimo.spins_to_levels (mimo.py:39-42)
+        xv = P == 1 ? sb[(size_t)c * D + j] : 2 * sb[(size_t)c * 2 * D + j] + sb[(size_t)c * 2 * D + D + j];
+      } else {
+        int d = 0;
+        for (int p = 0; p < P; ++p) d += sb[(size_t)c * P * D + p * D + j];
+        xv = min(max((int)xq8[j] + d, lo), hi);
+      }
+      ek[x] = (int8_t)(xv - xq8[j]);
+    }
   }
   for (int i = tid; i < NR2; i += kReadThreads) {
     float r = a.y[(size_t)u * NR2 + i];
@@ -433,24 +438,39 @@ __global__ void __launch_bounds__(kReadThreads) k_readout_dd(const ReadParams a)
         const int j = t * 32 + lane;
         nzm[t] = __ballot_sync(ARP_FULL, j < D && e[j] != 0);
       }
-      float rr[8];
+      constexpr int U = MR <= 2 ? 4 : (MR == 4 ? 2 : 1);  // coordinates in flight, within the registers of MR rows
+      float rr[MR];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) rr[m] = (lane + 32 * m < NR2) ? r0[lane + 32 * m] : 0.0f;
+      for (int m = 0; m < MR; ++m) rr[m] = (lane + 32 * m < NR2) ? r0[lane + 32 * m] : 0.0f;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         uint32_t mm = nzm[t];
-        while (mm) {
-          const int l = __ffs(mm) - 1;
-          mm &= mm - 1u;
-          const int j = t * 32 + l;
-          const float ev = (float)e[j];
+        while (mm) {  // U differing coordinates at a time, in ascending order, their column loads in flight
+          int jj[U];
 #pragma unroll
-          for (int m = 0; m < 8; ++m)
-            if (lane + 32 * m < NR2) rr[m] = __fmaf_rn(-Hs[j * HS + lane + 32 * m], ev, rr[m]);
+          for (int u = 0; u < U; ++u) {
+            jj[u] = mm ? t * 32 + __ffs(mm) - 1 : -1;
+            if (mm) mm &= mm - 1u;
+          }
+          float ev[U], hv[U][MR];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            ev[u] = jj[u] >= 0 ? (float)e[jj[u]] : 0.0f;
+#pragma unroll
+            for (int m = 0; m < MR; ++m)
+              hv[u][m] = (jj[u] >= 0 && lane + 32 * m < NR2) ? Hs[jj[u] * HS + lane + 32 * m] : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (jj[u] < 0) break;
+#pragma unroll
+            for (int m = 0; m < MR; ++m)
+              if (lane + 32 * m < NR2) rr[m] = __fmaf_rn(-hv[u][m], ev[u], rr[m]);
+          }
         }
       }
 #pragma unroll
-      for (int m = 0; m < 8; ++m) acc = __fmaf_rn(rr[m], rr[m], acc);
+      for (int m = 0; m < MR; ++m) acc = __fmaf_rn(rr[m], rr[m], acc);
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(ARP_FULL, acc, o);
@@ -630,7 +650,6 @@ namespace arp {
 
 cudaError_t map_dispatch(const MapParams& a, cudaStream_t st) {
   const int D = a.D;
-  if (D > 32 && D <= 64 && a.B <= kMapWideMaxB) return launch_map<2, 32>(a, st);  // one frame: 4x the warps
   return D <= 16 ? launch_map<1>(a, st) : D <= 32 ? launch_map<2>(a, st) : D <= 64 ? launch_map<4>(a, st)
                                                                           : launch_map<8>(a, st);
 }
@@ -644,10 +663,17 @@ static size_t readout_smem(int D, int NR2, int R, bool soft = false) {
 cudaError_t readout_dispatch(const ReadParams& a, cudaStream_t st) {
   const size_t smem = readout_smem(a.D, a.NR2, a.R, a.llr != nullptr);
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_readout_dd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    for (auto k : {k_readout_dd<1>, k_readout_dd<2>, k_readout_dd<4>, k_readout_dd<8>}) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
   }
-  return launch_ex(k_readout_dd, dim3(a.B), dim3(kReadThreads), smem, st, a.B <= kPdlMaxB, a);
+  const bool pdl = a.B <= kPdlMaxB;
+  const dim3 g(a.B), t(kReadThreads);
+  if (a.NR2 <= 32) return launch_ex(k_readout_dd<1>, g, t, smem, st, pdl, a);
+  if (a.NR2 <= 64) return launch_ex(k_readout_dd<2>, g, t, smem, st, pdl, a);
+  if (a.NR2 <= 128) return launch_ex(k_readout_dd<4>, g, t, smem, st, pdl, a);
+  return launch_ex(k_readout_dd<8>, g, t, smem, st, pdl, a);
 }
 
 // Workspace of the fused detector call: G, h, x_q, scale, spins, de, (flips, tests), 256-byte aligned.

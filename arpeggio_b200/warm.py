@@ -345,20 +345,28 @@ def train(mlp, nt=32, M=16, instances=2_000_000, batch=16384, snr=(8.0, 20.0), a
 
 
 def _profile_main(argv):
-    """python -m arpeggio_b200.warm profile --batch B: trains a network briefly (262144 instances), then runs
-    three warm detections of B seeded 32-user uses (32 anneals x 16 sweeps) and prints their stage times."""
+    """python -m arpeggio_b200.warm profile --batch B [--sweeps S --T T --tau TAU --conf C --snr DB]: trains a
+    network briefly (--train instances, default 262144), then runs three warm detections of B seeded 32-user
+    uses (32 anneals x S sweeps, default 16; optional temperature, sampled starts and per-problem anneal counts
+    with confidence threshold C, one SNR) and prints their stage times."""
     import argparse
     ap = argparse.ArgumentParser()
     ap.add_argument('mode', choices=['profile'])
     ap.add_argument('--batch', type=int, default=16384)
     ap.add_argument('--train', type=int, default=262144)
+    ap.add_argument('--sweeps', type=int, default=16)
+    ap.add_argument('--T', type=float, default=None)
+    ap.add_argument('--tau', type=float, default=None)
+    ap.add_argument('--conf', type=float, default=None)
+    ap.add_argument('--snr', type=float, default=None, help='one SNR (dB) for every use; default 10/14/18/22')
     a = ap.parse_args(argv)
     mlp = WarmMLP(P=2, seed=0)
     train(mlp, nt=32, instances=a.train, batch=min(a.train, 16384), anneals=32, sweeps=32, seed=11)
     B = a.batch
-    snr = torch.tensor([float(v) for v in np.repeat([10, 14, 18, 22], -(-B // 4))[:B]])
+    snr = (torch.full((B,), a.snr) if a.snr is not None else
+           torch.tensor([float(v) for v in np.repeat([10, 14, 18, 22], -(-B // 4))[:B]]))
     d = channel.draw_device(5, snr, B, 32, 16)
-    det = WarmDetector(B, 32, anneals=32, sweeps=16, mlp=mlp)
+    det = WarmDetector(B, 32, anneals=32, sweeps=a.sweeps, mlp=mlp, T0=a.T, T1=a.T, tau=a.tau, conf_min=a.conf)
     det.set_noise(N0=d['N0'])
     for i in range(2):
         det.run(d['H'], d['y'], seed=i)

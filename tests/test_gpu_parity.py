@@ -432,37 +432,3 @@ def test_64qam_detection_vs_oracle_chain():
     ber_q = (O.levels_to_bits(out['xq'], 64) != O.levels_to_bits(b['l'].numpy(), 64)).mean()
     assert ber <= ber_q
 
-
-@pytest.mark.parametrize('nt,M', [(32, 16), (32, 4), (32, 64), (24, 16), (20, 16)])
-def test_map_layouts_agree(nt, M):
-    """Batches of at most 256 problems up to 64 wide take the map's 32 x 32 thread layout (2 x 2 tiles), larger
-    batches the 16 x 16 one (4 x 4 tiles): the same operations per element and the same row-sum order, so G, h,
-    the guess, the scale, the soft estimate and the RI map are bit-identical."""
-    from arpeggio_b200 import _lib, channel
-    Bb, Bs = 300, 48
-    d = channel.draw_device(400 + nt + M, 10.0, Bb, nt, M, nr=nt + 3)
-    H, y = d['H'].contiguous(), d['y'].contiguous()
-    NR2, D = H.shape[1], H.shape[2]
-    s2 = torch.full((Bb,), 0.05, device='cuda')
-    L = _lib.lib()
-    outs = []
-    for B in (Bb, Bs):
-        G = torch.empty(B, D, D, dtype=torch.int32, device='cuda')
-        h = torch.empty(B, D, dtype=torch.int32, device='cuda')
-        xq = torch.empty(B, D, dtype=torch.int8, device='cuda')
-        sc = torch.empty(B, device='cuda')
-        zs = torch.empty(B, D, device='cuda')
-        st = torch.zeros(1, dtype=torch.int32, device='cuda')
-        _lib.check(L.arp_map_dd_soft(_lib.ptr(H), _lib.ptr(y), _lib.ptr(s2), B, NR2, D, M, 1, _lib.ptr(G), _lib.ptr(h),
-                                     _lib.ptr(xq), _lib.ptr(sc), _lib.ptr(zs), _lib.ptr(st), _lib.stream_ptr()), 'map')
-        N = 2 * D if M == 16 else D
-        ri = [torch.empty(B, N, N, device='cuda'), torch.empty(B, N, device='cuda'), torch.empty(B, N, device='cuda'),
-              torch.empty(B, N, dtype=torch.int8, device='cuda'), torch.empty(B, D, dtype=torch.int8, device='cuda'),
-              torch.empty(B, device='cuda')]
-        if M in (4, 16):
-            _lib.check(L.arp_map_ri(_lib.ptr(H), _lib.ptr(y), _lib.ptr(s2), B, NR2, D, M, 0.15,
-                                    *[_lib.ptr(t) for t in ri], _lib.stream_ptr()), 'map_ri')
-        torch.cuda.synchronize()
-        outs.append([G, h, xq, sc, zs] + (ri if M in (4, 16) else []))
-    for a, b in zip(*outs):
-        assert torch.equal(a[:Bs].view(torch.uint8), b.view(torch.uint8))

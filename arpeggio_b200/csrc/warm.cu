@@ -70,6 +70,8 @@ __device__ __forceinline__ void load_tile(uint32_t sbase, const bf16* g, int ld,
 }
 
 enum { EPI_F32 = 0, EPI_F32_ACC = 1, EPI_BIAS_RELU_BF16 = 2, EPI_BIAS_F32 = 3, EPI_MASK_BF16 = 4 };
+// Internal: split z of a split-K product stores its partial tile at C + z M ldc (summed afterwards in split order).
+constexpr int EPI_F32_PART = 5;
 
 template <int CW>
 __device__ __forceinline__ void epilogue(const GemmParams& p, int row, int n, const uint32_t (&v)[32]) {
@@ -80,11 +82,13 @@ __device__ __forceinline__ void epilogue(const GemmParams& p, int row, int n, co
     float f[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) f[i] = __uint_as_float(v[g + i]);
-    if (p.epi == EPI_F32 || p.epi == EPI_BIAS_F32) {
+    if (p.epi == EPI_F32 || p.epi == EPI_BIAS_F32 || p.epi == EPI_F32_PART) {
       if (p.epi == EPI_BIAS_F32)
 #pragma unroll
         for (int i = 0; i < 16; ++i) f[i] += p.bias[nn + i];
-      float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.C) + (size_t)row * p.ldc + nn);
+      float* base = reinterpret_cast<float*>(p.C);
+      if (p.epi == EPI_F32_PART) base += (size_t)blockIdx.z * p.M * p.ldc;
+      float4* o = reinterpret_cast<float4*>(base + (size_t)row * p.ldc + nn);
 #pragma unroll
       for (int i = 0; i < 4; ++i) o[i] = make_float4(f[4 * i], f[4 * i + 1], f[4 * i + 2], f[4 * i + 3]);
     } else if (p.epi == EPI_F32_ACC) {
@@ -221,6 +225,18 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const GemmParams p) {
   if (warp == 0) umma::tmem_free(tmem, NCOL);
 }
 
+// C (M x N, leading dimension ldc) += sum over s = 0..splits-1 of part[s] (M x N, dense), summed in s order.
+__global__ void __launch_bounds__(256) k_sum_splits(const float* __restrict__ part, int splits, int M, int N,
+                                                    float* __restrict__ C, int ldc) {
+  const size_t mn = (size_t)M * N;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < mn; x += (size_t)gridDim.x * blockDim.x) {
+    float acc = 0.0f;
+    for (int z = 0; z < splits; ++z) acc += part[(size_t)z * mn + x];
+    const size_t i = x / N, j = x - i * N;
+    C[i * ldc + j] += acc;
+  }
+}
+
 template <int BN, bool AMN, bool BMN>
 static cudaError_t launch_gemm(GemmParams p, cudaStream_t st) {
   constexpr size_t smem = (size_t)kStages * (128 * 128 + BN * 128);
@@ -241,8 +257,30 @@ static cudaError_t launch_gemm(GemmParams p, cudaStream_t st) {
   p.kt_per = (nkt + split - 1) / split;
   split = (nkt + p.kt_per - 1) / p.kt_per;
   dim3 grid(gx, gy, split);
-  k_gemm_bf16<BN, AMN, BMN><<<grid, 128, smem, st>>>(p);
-  return cudaGetLastError();
+  if (split == 1) {  // one CTA per output tile: its single add into C is already deterministic
+    k_gemm_bf16<BN, AMN, BMN><<<grid, 128, smem, st>>>(p);
+    return cudaGetLastError();
+  }
+  // split K: each split's partial tile to a stream-ordered workspace, then C += the partials in split order, so
+  // the result does not depend on which split finishes first
+  float* ws = nullptr;
+  const size_t mn = (size_t)p.M * p.N;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ws), mn * split * sizeof(float), st);
+  if (e != cudaSuccess) return e;
+  GemmParams q = p;
+  q.epi = EPI_F32_PART;
+  q.C = ws;
+  q.ldc = p.N;
+  k_gemm_bf16<BN, AMN, BMN><<<grid, 128, smem, st>>>(q);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    const int th = 256;
+    const int nb = (int)((mn + th - 1) / th);
+    k_sum_splits<<<nb < 4096 ? nb : 4096, th, 0, st>>>(ws, split, p.M, p.N, reinterpret_cast<float*>(p.C), p.ldc);
+    e = cudaGetLastError();
+  }
+  const cudaError_t ef = cudaFreeAsync(ws, st);
+  return e != cudaSuccess ? e : ef;
 }
 
 template <int BN>
@@ -460,8 +498,21 @@ __global__ void __launch_bounds__(256) k_colsum_bf16(const bf16* __restrict__ X,
     float s = 0.0f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) s += part[i][threadIdx.x & 31];
-    atomicAdd(out + c, s);
+    if (gridDim.y == 1)
+      out[c] += s;
+    else
+      out[(size_t)blockIdx.y * cols + c] = s;  // a row band's partial, summed by k_colsum_reduce
   }
+}
+
+// out[c] += sum over the gy row bands' partials, in band order.
+__global__ void __launch_bounds__(256) k_colsum_reduce(const float* __restrict__ part, int gy, int cols,
+                                                       float* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int y = 0; y < gy; ++y) s += part[(size_t)y * cols + c];
+  out[c] += s;
 }
 
 // ------------------------------------------------------------------------------------------------ Adam
@@ -885,8 +936,24 @@ extern "C" int arp_colsum_bf16(const void* X, int rows, int cols, int ld, float*
   int gy = (rows + 8 * 64 - 1) / (8 * 64);
   if (gy > 256) gy = 256;
   dim3 grid((cols + 31) / 32, gy);
-  k_colsum_bf16<<<grid, 256, 0, (cudaStream_t)stream>>>((const bf16*)X, rows, cols, ld, out);
-  return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (gy == 1) {
+    k_colsum_bf16<<<grid, 256, 0, st>>>((const bf16*)X, rows, cols, ld, out);
+    return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+  }
+  // row bands' partials to a stream-ordered workspace, then summed in band order (no float atomics: the
+  // gradients, and so the trained network, are the same on every run)
+  float* ws = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&ws), (size_t)gy * cols * sizeof(float), st) != cudaSuccess)
+    return ARP_ERR_LAUNCH;
+  k_colsum_bf16<<<grid, 256, 0, st>>>((const bf16*)X, rows, cols, ld, ws);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    k_colsum_reduce<<<(cols + 255) / 256, 256, 0, st>>>(ws, gy, cols, out);
+    e = cudaGetLastError();
+  }
+  const cudaError_t ef = cudaFreeAsync(ws, st);
+  return e == cudaSuccess && ef == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
 extern "C" int arp_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, float lr, float beta1,

@@ -200,9 +200,10 @@ int arp_map_dd_soft(const float* H, const float* y, const float* sigma2, int B, 
 /* C (M, N) = A B^T on the tensor cores (tcgen05.mma kind::f16, bf16 operands, fp32 accumulate in TMEM).
  * A is (M, K) row-major with row stride lda (a_mn_major = 0) or (K, M) row-major (a_mn_major = 1); B is (N, K)
  * (b_mn_major = 0) or (K, N) (b_mn_major = 1).  N and K multiples of 16, leading dimensions multiples of 8
- * elements, pointers 16-byte aligned.  epilogue: 0 C = acc (float), 1 C += acc (float; K is split over CTAs,
- * the caller zeroes C first), 2 C = bf16(max(acc + bias, 0)), 3 C = acc + bias (float), 4 C = bf16(acc if
- * aux > 0 else 0) with aux (M, N) bf16 of row stride ld_aux (the ReLU backward). */
+ * elements, pointers 16-byte aligned.  epilogue: 0 C = acc (float), 1 C += acc (float; K is split over CTAs
+ * whose partial products go to a stream-ordered workspace and are added in split order, so the result is the
+ * same on every run), 2 C = bf16(max(acc + bias, 0)), 3 C = acc + bias (float), 4 C = bf16(acc if aux > 0 else
+ * 0) with aux (M, N) bf16 of row stride ld_aux (the ReLU backward). */
 int arp_gemm_bf16(const void* A, int a_mn_major, int lda, const void* B, int b_mn_major, int ldb, int M, int N, int K,
                   int epilogue, const float* bias, const void* aux, int ld_aux, void* C, int ldc, int32_t* status,
                   void* stream);
@@ -219,7 +220,7 @@ int arp_warm_features(const void* G, const void* h, const int8_t* xq, const floa
 int arp_warm_loss(const float* logits, int ldl, const int8_t* labels, int rows, int classes, void* dlogits, int ldd,
                   float* loss_sum, int32_t* correct, void* stream);
 
-/* out (cols) += column sums of X (rows, cols) bf16 with row stride ld (bias gradients). */
+/* out (cols) += column sums of X (rows, cols) bf16 with row stride ld (bias gradients), in a fixed order. */
 int arp_colsum_bf16(const void* X, int rows, int cols, int ld, float* out, void* stream);
 
 /* One Adam step on n FP32 master weights w with gradient grad * grad_scale, moments m and v, bias-corrected

@@ -135,6 +135,35 @@ def test_mlp_forward_and_gradients_match_oracle():
     assert abs(float(mlp.loss.item()) - gr['loss']) <= 1e-3 * abs(gr['loss']) + 1e-2
 
 
+def test_training_is_bit_reproducible():
+    """Split-K weight gradients and bias gradients reduce in a fixed order: two backward passes give identical
+    gradients, and two short trainings from the same seed give identical weights."""
+    from arpeggio_b200 import warm
+    d, det = _problems(640, 32, 12.0, 19)
+    rows = 640 * 64
+    lab = torch.empty(rows, dtype=torch.int8, device='cuda')
+    det.labels(lab)
+    mlp = warm.WarmMLP(P=2, seed=5)
+    mlp.reserve(rows, train=True)
+    grads = []
+    for _ in range(2):
+        mlp.forward(det.X, rows)
+        mlp.backward(det.X, lab, rows)
+        torch.cuda.synchronize()
+        grads.append(mlp.grad.clone())
+    assert torch.equal(grads[0], grads[1])
+    ws = []
+    for _ in range(2):
+        m = warm.WarmMLP(P=2, seed=6)
+        m.reserve(rows // 2, train=True)
+        for r0 in (0, rows // 2):
+            m.train_step(det.X[r0:r0 + rows // 2], lab[r0:r0 + rows // 2], rows // 2, lr=1e-3)
+        torch.cuda.synchronize()
+        m.check()
+        ws.append(m.w.clone())
+    assert torch.equal(ws[0], ws[1])
+
+
 @pytest.mark.parametrize('rows', [64, 128, 1000, 4096, 40000])
 def test_fused_forward_equals_the_layer_by_layer_forward(rows):
     """One persistent launch (hidden activations on chip) against the three GEMM launches of the training path:

@@ -497,9 +497,10 @@ def run_ours(args):
         torch.cuda.synchronize()
         det1.check()
         us = sorted(1e3 * a_.elapsed_time(b_) for a_, b_ in le)
-        lat = {'frame': 'one %d-user x %d-antenna 16-QAM channel use, %d anneals, H/y from pinned host memory, bits '
-                        'and distance back to pinned host memory, one replayed CUDA graph (copy in, map, anneal, '
-                        'readout, copy out); device time per replay' % (w['nt'], w['nr'], args.anneals),
+        lat = {'frame': 'one %d-user x %d-antenna 16-QAM channel use at %g dB, %d anneals, H/y from pinned host '
+                        'memory, bits and distance into pinned host memory, one replayed CUDA graph (copy in, map, '
+                        'anneal, readout writing straight into the mapped pinned outputs); device time per replay'
+                        % (w['nt'], w['nr'], float(w['snrs'][len(w['snrs']) // 2]), args.anneals),
                'frames': n, 'p50_us': us[n // 2], 'p99_us': us[min(n - 1, int(0.99 * n))], 'max_us': us[-1]}
 
     # ---- BER of the last timed step per SNR point (the detection itself, and its MMSE guess for reference)

@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
             cw[p][t][3] = c3;
           }
       }
-#pragma unroll
+#pragma unroll(NS <= 2 ? 4 : 1)  // three and four slots: one copy of the pass body (code size)
       for (int i = 0; i < 4; ++i) {
 #pragma unroll
         for (int p = 0; p < P; ++p) {
@@ -536,7 +536,8 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
           for (int t = 0; t < NS; ++t) {
             uint32_t u;
             if constexpr (CACHE) {
-              u = cw[p][t][i];
+              // word i of the cached block, by selects (a runtime i must not index the register array)
+              u = i == 0 ? cw[p][t][0] : (i == 1 ? cw[p][t][1] : (i == 2 ? cw[p][t][2] : cw[p][t][3]));
             } else {
               uint32_t c0 = (uint32_t)q4, c1 = (uint32_t)(p * D + t * 32 + lane), c2 = (uint32_t)r, c3 = inst;
               philox10(c0, c1, c2, c3, K);
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDPar
             if (lane == l) sp ^= 1u << (p * NS + ts);
             jl = ts * 32 + l;
           };
-          if constexpr (!CHORD && NS <= 2) {
+          if constexpr (!CHORD) {
             // A round accepts the first position after the last flip whose test passes, so once the scan has
             // left slot t (positions 32 t .. 32 t + 31) no later round of this pass can accept there: finish slot
             // t, then slot t + 1 -- one ballot of one slot per round, the same flips in the same order.  (Measured

@@ -227,12 +227,15 @@ class Detector:
         t = self.bits if i == 0 else self.dist
         return _lib.ptr(t if sl is None else t[sl])
 
-    def run_host(self, Hh, yh, seed, bits_out, dist_out, Hd, yd, chunks=8, inst0=0, stream=None):
+    def run_host(self, Hh, yh, seed, bits_out, dist_out, Hd=None, yd=None, chunks=8, inst0=0, stream=None):
         """End-to-end detection from pinned host buffers: the batch is cut into `chunks` pieces; the host to
         device copy of piece c+1 (on a copy stream) overlaps the detection of piece c (on `stream`), and each
-        piece's bits and distances go back to the pinned outputs as soon as it is done.  Hd, yd: device
-        staging buffers of the batch's size.  Results equal one run() over the whole batch.  Stream-ordered:
-        synchronise `stream` before reading bits_out / dist_out."""
+        piece's bits and distances go back to the pinned outputs as soon as it is done.  Results equal one run()
+        over the whole batch.  Stream-ordered: synchronise `stream` before reading bits_out / dist_out.
+        Hd, yd: device staging buffers of the batch's size, written once the work already on `stream` is done;
+        or None: the detector's own two staging buffers, used by alternate calls, so the copy of the next
+        batch (called before this one finishes) overlaps this batch's detection -- it waits only for the last
+        reader of its own buffer, the call before this one."""
         import torch
         cs = stream if stream is not None else torch.cuda.current_stream()
         if not hasattr(self, '_copy_stream'):
@@ -243,9 +246,23 @@ class Detector:
         edges = [B * c // chunks for c in range(chunks + 1)]
         while len(self._copy_events) < chunks + 1:
             self._copy_events.append(torch.cuda.Event())
-        go = self._copy_events[chunks]
-        go.record(cs)
-        xs.wait_event(go)
+        free = None
+        if Hd is None:
+            st = getattr(self, '_staging', None)
+            if st is None or st[0][0].shape != Hh.shape or st[0][1].shape != yh.shape:
+                st = [(torch.empty(Hh.shape, dtype=Hh.dtype, device=self.device),
+                       torch.empty(yh.shape, dtype=yh.dtype, device=self.device), torch.cuda.Event(), False)
+                      for _ in range(2)]
+                self._staging, self._staging_next = st, 0
+            k = self._staging_next
+            self._staging_next = 1 - k
+            Hd, yd, free, used = st[k]
+            if used:
+                xs.wait_event(free)  # the previous batch staged here has been read by its readout
+        else:
+            go = self._copy_events[chunks]
+            go.record(cs)
+            xs.wait_event(go)
         for c in range(chunks):
             a, b = edges[c], edges[c + 1]
             with torch.cuda.stream(xs):
@@ -261,6 +278,10 @@ class Detector:
             with torch.cuda.stream(cs):
                 bits_out[a:b].copy_(bits, non_blocking=True)
                 dist_out[a:b].copy_(dist, non_blocking=True)
+        if free is not None:
+            free.record(cs)  # every reader of this staging buffer is on cs before this point
+            k = 1 - self._staging_next
+            self._staging[k] = (Hd, yd, free, True)
 
     def frame_buffers(self):
         """Buffers for captured frames: pinned host and device inputs with H and y side by side (one copy in) and a

@@ -308,6 +308,22 @@ def test_pipelined_host_path_equals_one_run():
     det.check()
     assert torch.equal(bo, bits.cpu())
     assert torch.equal(do, dist.cpu())
+    # back-to-back calls on the detector's own two staging buffers (the next batch's copy overlaps this batch's
+    # detection): every call's outputs equal its one-run outputs, also with other inputs in between
+    d2 = channel.draw_device(12, 14.0, B, 32, 16)
+    H2h, y2h = d2['H'].cpu().pin_memory(), d2['y'].cpu().pin_memory()
+    outs = [(torch.empty(bits.shape, dtype=torch.int8).pin_memory(), torch.empty(B, dtype=torch.float32).pin_memory())
+            for _ in range(4)]
+    for i, (o_b, o_d) in enumerate(outs):
+        hh, yy = (Hh, yh) if i % 2 == 0 else (H2h, y2h)
+        det.run_host(hh, yy, 5 + i, o_b, o_d, chunks=1 + i)
+    torch.cuda.synchronize()
+    det.check()
+    for i, (o_b, o_d) in enumerate(outs):
+        dd = d if i % 2 == 0 else d2
+        rb, _, rd = det.run(dd['H'], dd['y'], seed=5 + i)
+        torch.cuda.synchronize()
+        assert torch.equal(o_b, rb.cpu()) and torch.equal(o_d, rd.cpu()), i
 
 
 def test_fused_c_entry_equals_staged_calls():

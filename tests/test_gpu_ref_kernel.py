@@ -1,7 +1,9 @@
-"""The reference's own first-accept CUDA kernel (arpeggio/sim/arpeggio_fx.cu, compiled from its source into
-oracle/_ref/ by `make -C oracle ref-gpu`, one thread per anneal) and this project's kernel on the same integer
-problems, keys and instance numbers: spins, best energies and flip/test counters bit for bit, and both timed on
-the same GPU.  Skipped where the reference kernel was not built (no reference tree at build time)."""
+"""The reference's own CUDA kernels, compiled from their sources into oracle/_ref/ by `make -C oracle ref-gpu`,
+beside this project's on the same inputs, keys and instance numbers: the first-accept kernel
+(arpeggio/sim/arpeggio_fx.cu, one thread per anneal) against arp_anneal_first_accept -- spins, best energies and
+flip/test counters bit for bit -- and the Chord kernel (arpeggio/mimo/chord_kernel.cu) against arp_anneal_chord
+on the golden Chord problems -- spins, energies and counters bit for bit; both pairs timed on the same GPU.
+Skipped where the reference kernels were not built (no reference tree at build time)."""
 import ctypes
 import os
 
@@ -10,7 +12,9 @@ import pytest
 import torch
 
 pytestmark = pytest.mark.gpu
-REF_SO = os.path.join(os.path.dirname(os.path.abspath(__file__)), '..', 'oracle', '_ref', 'libref_arpeggio.so')
+REF_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), '..', 'oracle', '_ref')
+REF_SO = os.path.join(REF_DIR, 'libref_arpeggio.so')
+REF_CHORD_SO = os.path.join(REF_DIR, 'libref_chord.so')
 M32 = 0xFFFFFFFF
 
 
@@ -90,3 +94,88 @@ def test_reference_kernel_timing_x32():
     print('\nreference arpeggio_fx: %.3f ms, this project: %.3f ms for 4096 uses x 32 anneals (%.1fx)'
           % (t_ref, t_ours, t_ref / t_ours))
     assert t_ours < t_ref
+
+
+def _ref_chord():
+    if not os.path.exists(REF_CHORD_SO):
+        pytest.skip('reference Chord kernel not built (make -C oracle ref-gpu needs the reference tree)')
+    L = ctypes.CDLL(REF_CHORD_SO)
+    P_, I, U = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32
+    L.ref_chord.argtypes = [P_, P_, P_, P_, P_, I, I, I, I, I, I, U, U, I, I, I, P_, P_, P_, P_]
+    return L
+
+
+def _chord_both(F, R, P, seed, inst0, mode, reps=1):
+    from arpeggio_b200 import _lib, chordfx
+    L = _ref_chord()
+    B, N = F['h'].shape
+    dev = torch.device('cuda')
+    F = dict(F, J=F['J'].to(dev, torch.int16).contiguous(), h=F['h'].to(dev, torch.int32).contiguous(),
+             h0=F['h0'].to(dev, torch.int32).contiguous(), T=F['T'].to(dev, torch.int32).contiguous(),
+             c=F['c'].to(dev, torch.int32).contiguous())  # both kernels read device-resident inputs
+    J = F['J']
+    h, h0 = F['h'].to(dev, torch.int32).contiguous(), F['h0'].to(dev, torch.int32).contiguous()
+    T, c = F['T'].to(dev, torch.int32).contiguous(), F['c'].to(dev, torch.int32).contiguous()
+    shape_e, shape_s = ((B,), (B, N)) if mode == 'best' else ((B, R), (B, R, N))
+    re_e = torch.empty(shape_e, dtype=torch.int32, device=dev)
+    re_s = torch.empty(shape_s, dtype=torch.int8, device=dev)
+    re_st = torch.zeros(4, dtype=torch.int64, device=dev)
+    k = chordfx.Kernel()
+    our_st = torch.zeros(4, dtype=torch.int64, device=dev)
+
+    def ref_launch(st):
+        assert L.ref_chord(_lib.ptr(J), _lib.ptr(h), _lib.ptr(h0), _lib.ptr(T), _lib.ptr(c), int(F['q']), int(F['S']),
+                           P, R, N, B, seed & M32, seed >> 32, inst0, 1 if mode == 'best' else 0, 8, _lib.ptr(re_e),
+                           _lib.ptr(re_s), _lib.ptr(st), _lib.stream_ptr()) == 0
+
+    ref_launch(re_st)
+    s, e = k.chord(F, R, seed, P=P, inst0=inst0, mode=mode, stats=our_st)
+    torch.cuda.synchronize()
+    times = []
+    for fn in (lambda: ref_launch(None), lambda: k.chord(F, R, seed, P=P, inst0=inst0, mode=mode)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / reps)
+    return (re_s, re_e.to(torch.int64), re_st), (s, e, our_st), times
+
+
+def _golden_chord(golden, name):
+    z = golden('golden_chord.npz')
+    q, S, P, R, s0, s1, inst0 = [int(v) for v in z[name + '/meta']]
+    F = dict(J=torch.from_numpy(z[name + '/J']), h=torch.from_numpy(z[name + '/h']),
+             h0=torch.from_numpy(z[name + '/h0']), T=torch.from_numpy(z[name + '/T']),
+             c=torch.from_numpy(z[name + '/c']), q=q, S=S)
+    return F, P, R, s0 | (s1 << 32), inst0
+
+
+def _chord_names():
+    from conftest import GOLDEN
+    return [str(n) for n in np.load(os.path.join(GOLDEN, 'golden_chord.npz'))['names']]
+
+
+@pytest.mark.parametrize('name', _chord_names())
+@pytest.mark.parametrize('mode', ['chains', 'best'])
+def test_reference_chord_kernel_bit_exact(golden, name, mode):
+    F, P, R, seed, inst0 = _golden_chord(golden, name)
+    ref, ours, _ = _chord_both(F, R, P, seed, inst0, mode)
+    for a, b in zip(ref, ours):
+        assert torch.equal(a, b)
+
+
+def test_reference_chord_kernel_timing(golden):
+    """The largest golden Chord problem tiled to 2048 problems (distinct instance numbers): the same outputs,
+    and both kernels' device time (printed; run with -s)."""
+    names = _chord_names()
+    F, P, R, seed, inst0 = max((_golden_chord(golden, n) for n in names), key=lambda t: t[0]['h'].shape[1])
+    B0 = F['h'].shape[0]
+    rep = -(-2048 // B0)
+    F = {k: (v.repeat((rep,) + (1,) * (v.dim() - 1))[:2048] if k in ('J', 'h', 'h0') else v) for k, v in F.items()}
+    ref, ours, (t_ref, t_ours) = _chord_both(F, R, P, seed, inst0, 'chains', reps=3)
+    for a, b in zip(ref, ours):
+        assert torch.equal(a, b)
+    print('\nreference chord_m%d: %.3f ms, this project: %.3f ms for 2048 problems x %d anneals, N = %d (%.2fx)'
+          % (F['h'].shape[1] // 32, t_ref, t_ours, R, F['h'].shape[1], t_ref / t_ours))

@@ -168,8 +168,8 @@ def frame_latency(det, f, stream, n):
 # (problems whose kept start has sum_j log max_c p_jc > -CONF_PER_COORD * D run R_EASY anneals) -- chosen on
 # separate seeded draws, not on the bench's instances.
 CONF_PER_COORD = 5.0 / 64
-WARM_POINTS = {32: {'warm': dict(sweeps=24, T=0.085, tau=0.8, counts=True),
-                    'warm_fast': dict(sweeps=20, T=0.085, tau=0.8, counts=True),
+WARM_POINTS = {32: {'warm': dict(sweeps=24, T=0.085, tau=0.8, counts=True, r_easy=4),
+                    'warm_fast': dict(sweeps=20, T=0.085, tau=0.8, counts=True, r_easy=4),
                     'warm_argmax': dict(sweeps=24, T=0.085, tau=None, counts=False)},
                64: {'warm': dict(sweeps=24, T=0.07, tau=0.8, counts=True),
                     'warm_fast': dict(sweeps=32, T=0.07, tau=0.8, counts=True, per_coord=1.6 * CONF_PER_COORD,
@@ -203,8 +203,9 @@ def warm_vs_plain(args, dev, stream, rank):
            'warm': 'MLP warm start kept only where its energy is no worse than the MMSE guess, learned flip-test '
                    'order; anneal 0 from the argmax class, anneals 1..R-1 drawn per coordinate from softmax(0.8 z) '
                    '(Philox word 1 of the start block); problems whose kept start has confidence sum_j log max_c '
-                   'p_jc above -%.4f D run %d anneals (warm_fast at 64 users: above -%.4f D, 16 anneals), the others '
-                   'all R' % (CONF_PER_COORD, R_EASY, 1.6 * CONF_PER_COORD),
+                   'p_jc above -%.4f D run 4 anneals at 32 users (one per warp of the anneal block), %d at 64 users '
+                   '(warm_fast at 64 users: above -%.4f D, 16 anneals), the others all R'
+                   % (CONF_PER_COORD, R_EASY, 1.6 * CONF_PER_COORD),
            'warm_argmax': 'every anneal from the argmax class, all R anneals, at the warm budget',
            'points': {'x%d' % k: v for k, v in WARM_POINTS.items()}}
     for nt, B, snrs, full, R in ((32, args.batch, [18, 20, 22, 24], 32, 32),

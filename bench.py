@@ -611,6 +611,10 @@ def run_ours(args):
     if os.path.exists(pf):
         peaks = json.load(open(pf))
     hbm_peak = peaks.get('hbm_gbs', 6650.0)
+    smem_bytes = 4.0 * D * st[0] + 4.0 * st[1]
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    sm_mhz = (ck or {}).get('sm_mhz') or 1965.0
+    smem_peak = 128.0 * sms * sm_mhz * 1e6 / 1e9
     line = {
         'metric': METRIC, 'value': job_throughput(B, world, ms), 'unit': 'detections/s', 'n_gpus': world,
         'steps': K, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
@@ -625,13 +629,18 @@ def run_ours(args):
         'stages_ms': {'map': stage[0], 'anneal': stage[1], 'readout': stage[2]},
         'roofline': {'bound': 'int_issue', 'achieved': ops / t_anneal / 1e9, 'peak': peak_ops / 1e9,
                      'unit': 'Gop/s', 'frac': ops / t_anneal / peak_ops, 'traffic': traffic,
-                     'kernel': 'k_anneal_dd<2,2,first-accept,int32>',
+                     'kernel': 'k_anneal_int<2, 2, first accept, cached Philox>',
                      'ops_model': '100 per Philox4x32-10 block + 5 per lane decision + 3 per field update',
                      'peak_source': 'measured in this run: arp_philox_rate (chained Philox blocks, all SMs); '
                                     'MEASURED_PEAKS.json has no integer peak'},
         'roofline_hbm': {'bound': 'hbm', 'achieved': alg_bytes / t_anneal / 1e9, 'peak': hbm_peak, 'unit': 'GB/s',
                          'frac': alg_bytes / t_anneal / 1e9 / hbm_peak,
                          'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if peaks else 'fallback'},
+        'roofline_smem': {'bound': 'smem', 'achieved': smem_bytes / t_anneal / 1e9, 'peak': smem_peak, 'unit': 'GB/s',
+                          'frac': smem_bytes / t_anneal / 1e9 / smem_peak,
+                          'bytes_model': 'flips x D x 4 (a flipped coordinate\'s int32 row of G, read by the rank-1 '
+                                         'field update) + tests x 4',
+                          'peak_source': 'nominal: 128 B per clock per SM x %d SMs x the sampled median SM clock' % sms},
         'anneal_counters': {'flips': int(st[0]), 'tests': int(st[1]), 'anneals': B * R, 'philox_blocks': blocks},
         'latency': lat,
         'ber': ber,

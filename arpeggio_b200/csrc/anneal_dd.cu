@@ -341,7 +341,9 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
 #endif
 
 template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false>
-__global__ void __launch_bounds__(256, ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
+// Four slots (D > 96) are bounded at 128 registers: four 4-warp blocks per SM instead of three (no spills;
+// 64 users: 129 -> 120 ms per 32768 uses).
+__global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
   constexpr int DP = NS * 32;
   extern __shared__ __align__(16) unsigned char smem[];
   int32_t* Gs = reinterpret_cast<int32_t*>(smem);

@@ -240,46 +240,23 @@ __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
             ++flips;
           };
           if constexpr (!CHORD) {
-            uint32_t rem[NS];
-#pragma unroll
-            for (int t = 0; t < NS; ++t) rem[t] = vmask[t];
+            // the scan finishes slot t (positions 32 t .. 32 t + 31) before slot t + 1: a round accepts only after
+            // the last flip, so a slot the scan has left has no candidate left this pass
             long long tt = 1;
-            for (;;) {
-              uint32_t am[NS];
 #pragma unroll
-              for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, accept(t)) & rem[t];
-              int ts = -1;
-              uint32_t m = 0;
-#pragma unroll
-              for (int t = NS - 1; t >= 0; --t)
-                if (am[t]) {
-                  ts = t;
-                  m = am[t];
-                }
-              if (ts < 0) break;
-              const int l = __ffs(m) - 1;
-              FT wsel = w[0], dsel = dg[0];
-              uint32_t sbits = Sm[p][0];
-#pragma unroll
-              for (int t = 1; t < NS; ++t)
-                if (ts == t) {
-                  wsel = w[t];
-                  dsel = dg[t];
-                  sbits = Sm[p][t];
-                }
-              const int j = ts * 32 + l;
-              commit(wsel, dsel, sbits, j, l);
-              const uint32_t bit = 1u << l;
-#pragma unroll
-              for (int t = 0; t < NS; ++t) {
-                if (t == ts) {
-                  Sm[p][t] ^= bit;
-                  rem[t] &= ~((bit << 1) - 1u);
-                } else if (t < ts) {
-                  rem[t] = 0;
-                }
+            for (int t = 0; t < NS; ++t) {
+              uint32_t rem = vmask[t];
+              for (;;) {
+                const uint32_t m = __ballot_sync(ARP_FULL, accept(t)) & rem;
+                if (m == 0) break;
+                const int l = __ffs(m) - 1;
+                const int j = t * 32 + l;
+                commit(w[t], dg[t], Sm[p][t], j, l);
+                const uint32_t bit = 1u << l;
+                Sm[p][t] ^= bit;
+                rem &= ~((bit << 1) - 1u);
+                if (j < D - 1) ++tt;
               }
-              if (j < D - 1) ++tt;
             }
             tests += tt;
           } else {

@@ -119,25 +119,21 @@ __global__ void __launch_bounds__(256) k_anneal_full_f32(const FullParams a) {
           if (t == ts) Sm[t] ^= 1u << l;
       };
       if constexpr (!CHORD) {
+        // the scan finishes slot t before slot t + 1 (a round accepts only after the last flip, so a slot the
+        // scan has left has no candidate left this pass): one ballot of one slot per round, the same flips
         int jl = -1;
-        for (;;) {
-          uint32_t am[MPL];
+        ++ballots;  // the round that finds no further flip (ballots = flips + 1 per pass)
 #pragma unroll
-          for (int t = 0; t < MPL; ++t)
-            am[t] = (t / tpc == p) ? __ballot_sync(ARP_FULL, accept(t) && t * 32 + lane > jl) : 0u;
-          ++ballots;
-          int ts = -1;
-          uint32_t m = 0;
-#pragma unroll
-          for (int t = MPL - 1; t >= 0; --t)
-            if (am[t]) {
-              ts = t;
-              m = am[t];
-            }
-          if (ts < 0) break;
-          const int l = __ffs(m) - 1;
-          commit(ts, l);
-          jl = ts * 32 + l;
+        for (int t = 0; t < MPL; ++t) {
+          if (t / tpc != p) continue;
+          for (;;) {
+            const uint32_t m = __ballot_sync(ARP_FULL, accept(t) && t * 32 + lane > jl);
+            if (m == 0) break;
+            ++ballots;
+            const int l = __ffs(m) - 1;
+            commit(t, l);
+            jl = t * 32 + l;
+          }
         }
         if (jl == (p + 1) * D - 1) ++lastflips;
       } else {

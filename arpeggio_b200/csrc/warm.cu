@@ -1036,9 +1036,13 @@ extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const
 // update, so a chunk is one contiguous 16 KB copy (whole L2 sectors, no gather).
 namespace arp {
 
+constexpr int kNH = 256;  // hidden width of the warm-start network
 constexpr int kMlpThreads = 256;
-constexpr uint32_t kHsBytes = 128 * 512 * 2, kXsBytes = 128 * 16 * 2, kSlotBytes = 256 * 32 * 2;
-constexpr uint32_t kMlpSmem = kHsBytes + kXsBytes + 4 * kSlotBytes;
+// Shared memory of the fused forward: W2 resident for the whole launch (8 chunks of 256 rows x 32 k, 128 KB),
+// the H tile (128 rows x 256, H1 then H2), the X tile, W1 and W3t resident (8 KB each).
+constexpr uint32_t kW2Bytes = kNH * kNH * 2, kHsBytes = 128 * kNH * 2, kXsBytes = 128 * 16 * 2;
+constexpr uint32_t kW1Bytes = kNH * 16 * 2, kW3Bytes = kNH * 16 * 2, kChunkBytes = kNH * 32 * 2;
+constexpr uint32_t kMlpSmem = kW2Bytes + kHsBytes + kXsBytes + kW1Bytes + kW3Bytes;
 
 struct MlpParams {
   const bf16* X;
@@ -1062,24 +1066,24 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
                : "memory");
 }
 
-// W2 (512 x 512, row-major) -> chunk order of the fused kernel's ring: chunk t = rows [256 (t / 16), +256) and
-// k [32 (t % 16), +32), within a chunk k-group b (8 wide) then row n then element: W2p[t][b][n][e].
+// W2 (256 x 256, row-major: output n, input k) -> the fused kernel's shared-memory order: chunk t = k
+// [32 t, +32) of all 256 rows, within a chunk k-group b (8 wide) then row n then element: W2p[t][b][n][e] (the
+// canonical K-major layout of a 256 x 32 B operand, k-groups 4096 B apart, 8-row groups 128 B apart).
 __global__ void __launch_bounds__(256) k_pack_w2(const bf16* __restrict__ W2, bf16* __restrict__ W2p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // one 16-byte group of 8 elements
-  if (i >= 512 * 64) return;
+  if (i >= kNH * kNH / 8) return;
   const int t = i >> 10, b = (i >> 8) & 3, n = i & 255;  // 1024 groups per chunk, 256 per k-group
-  const int row = (t >> 4) * 256 + n, k = (t & 15) * 32 + b * 8;
-  reinterpret_cast<uint4*>(W2p)[i] = *reinterpret_cast<const uint4*>(W2 + (size_t)row * 512 + k);
+  const int k = t * 32 + b * 8;
+  reinterpret_cast<uint4*>(W2p)[i] = *reinterpret_cast<const uint4*>(W2 + (size_t)n * kNH + k);
 }
 
-// TMEM -> bias (shared memory) + ReLU -> bf16 -> H tile; warp w drains rows 32 (w % 4) .. and columns
-// [256 (w / 4), +256).
-__device__ __forceinline__ void mlp_epi_hidden(uint32_t tmem, uint32_t hs, const float* bias, int warp,
-                                               int lane) {
+// TMEM -> bias (shared memory) + ReLU -> bf16 -> H tile (K-major, 8-row groups 4096 B apart); warp w drains
+// rows 32 (w % 4) .. and columns [128 (w / 4), +128).
+__device__ __forceinline__ void mlp_epi_hidden(uint32_t tmem, uint32_t hs, const float* bias, int warp, int lane) {
   const int m = (warp & 3) * 32 + lane, half = warp >> 2;
 #pragma unroll 1
-  for (int cc = 0; cc < 8; ++cc) {
-    const int c0 = half * 256 + cc * 32;
+  for (int cc = 0; cc < 4; ++cc) {
+    const int c0 = half * 128 + cc * 32;
     uint32_t v[32];
     umma::tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0, v);
 #pragma unroll
@@ -1096,7 +1100,7 @@ __device__ __forceinline__ void mlp_epi_hidden(uint32_t tmem, uint32_t hs, const
         const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
         pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
       }
-      const uint32_t addr = hs + (uint32_t)((m >> 3) * 8192 + ((c0 >> 3) + q) * 128 + (m & 7) * 16);
+      const uint32_t addr = hs + (uint32_t)((m >> 3) * 4096 + ((c0 >> 3) + q) * 128 + (m & 7) * 16);
       asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
                    "r"(pk[3])
                    : "memory");
@@ -1104,46 +1108,38 @@ __device__ __forceinline__ void mlp_epi_hidden(uint32_t tmem, uint32_t hs, const
   }
 }
 
+// The whole network per 128-row tile, one persistent CTA per SM: the weights are loaded once per launch (W2 by
+// eight bulk copies on one mbarrier, W1, W3t and the biases by cp.async) and stay in shared memory; per tile,
+// layer 1 (one MMA, N = 256), its epilogue into the H tile, layer 2 (16 MMAs from the resident W2), its
+// epilogue over H1, layer 3 (16 MMAs, N = 16), logits + b3 to global.  The next tile's X is fetched as soon as
+// layer 1 has read the current one.  Same roundings and summation order as the layer-by-layer GEMMs.
 __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t full[4], empty[4];
-  __shared__ __align__(8) uint64_t bar_l1, bar_l2, bar_l3;
+  __shared__ __align__(8) uint64_t bar_w, bar_l1, bar_l2, bar_l3;
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
-  __shared__ __align__(16) float s_b1[512], s_b2[512];
+  __shared__ __align__(16) float s_b1[kNH], s_b2[kNH];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ntiles = (p.rows + 127) / 128;
   if ((int)blockIdx.x >= ntiles) return;
   pdl_trigger();
-  const uint32_t hs = umma::su32(smem), xs = hs + kHsBytes, ring = xs + kXsBytes;
-  const uint32_t w1s = ring + 3 * kSlotBytes, w3s = ring + 2 * kSlotBytes;
-  constexpr uint32_t ID_HID = umma::idesc_bf16(256, false, false), ID_OUT = umma::idesc_bf16(16, false, true);
+  const uint32_t w2s = umma::su32(smem), hs = w2s + kW2Bytes, xs = hs + kHsBytes, w1s = xs + kXsBytes,
+                 w3s = w1s + kW1Bytes;
+  constexpr uint32_t ID_HID = umma::idesc_bf16(kNH, false, false), ID_OUT = umma::idesc_bf16(16, false, true);
   if (tid == 0) {
-    for (int s = 0; s < 4; ++s) {
-      umma::mbar_init(&full[s], 1);
-      umma::mbar_init(&empty[s], 1);
-    }
+    umma::mbar_init(&bar_w, 1);
     umma::mbar_init(&bar_l1, 1);
     umma::mbar_init(&bar_l2, 1);
     umma::mbar_init(&bar_l3, 1);
     umma::fence_mbar_init();
     s_abort = 0;
   }
-  if (warp == 0) umma::tmem_alloc(&s_tmem, 512);
+  if (warp == 0) umma::tmem_alloc(&s_tmem, kNH);
   umma::tc_before_sync();
   __syncthreads();
   umma::tc_after_sync();
   const uint32_t tmem = s_tmem;
   pdl_wait();  // everything above touches no global memory
-  // biases: one 16-byte copy per thread (128 of b1, 128 of b2), landing with the first tile's X and W1
-  if (p.bias16)
-    umma::cp16(umma::su32(tid < 128 ? s_b1 + 4 * tid : s_b2 + 4 * (tid - 128)),
-               tid < 128 ? p.b1 + 4 * tid : p.b2 + 4 * (tid - 128), true);
-  else
-    for (int i = tid; i < 512; i += kMlpThreads) {
-      s_b1[i] = p.b1[i];
-      s_b2[i] = p.b2[i];
-    }
 
   auto load_x = [&](int tile) {  // 128 x 16: one 16-byte chunk per thread
     const int row = tid >> 1, kc = tid & 1, m = tile * 128 + row;
@@ -1151,43 +1147,35 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
     umma::cp16(xs + (uint32_t)((row >> 3) * 256 + kc * 128 + (row & 7) * 16),
                ok ? (const void*)(p.X + (size_t)m * 16 + kc * 8) : (const void*)p.X, ok);
   };
-  auto load_w1 = [&]() {  // 512 x 16, K-major, SBO 256
+  // weights, once: W2 by bulk copies (thread 0), W1 (256 x 16, K-major, SBO 256) and W3t (256 k x 16 n,
+  // MN-major: LBO 256 between k-groups, SBO 128) and the biases by cp.async
+  if (tid == 0) {
+    mbar_expect_tx(&bar_w, kW2Bytes);
+    for (int t = 0; t < kNH / 32; ++t)
+      bulk_load(w2s + (uint32_t)t * kChunkBytes, p.W2p + (size_t)t * (kChunkBytes / 2), kChunkBytes, &bar_w);
+  }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int c = tid + i * kMlpThreads, row = c >> 1, kc = c & 1;
-      umma::cp16(w1s + (uint32_t)((row >> 3) * 256 + kc * 128 + (row & 7) * 16), p.W1 + (size_t)row * 16 + kc * 8,
-                 true);
+  for (int i = 0; i < 2; ++i) {
+    const int c = tid + i * kMlpThreads, r = c >> 1, h = c & 1;
+    umma::cp16(w1s + (uint32_t)((r >> 3) * 256 + h * 128 + (r & 7) * 16), p.W1 + (size_t)r * 16 + h * 8, true);
+    umma::cp16(w3s + (uint32_t)((r >> 3) * 256 + h * 128 + (r & 7) * 16), p.W3t + (size_t)r * 16 + h * 8, true);
+  }
+  if (p.bias16) {
+    if (tid < 2 * kNH / 4)
+      umma::cp16(umma::su32(tid < kNH / 4 ? s_b1 + 4 * tid : s_b2 + 4 * (tid - kNH / 4)),
+                 tid < kNH / 4 ? p.b1 + 4 * tid : p.b2 + 4 * (tid - kNH / 4), true);
+  } else {
+    for (int i = tid; i < kNH; i += kMlpThreads) {
+      s_b1[i] = p.b1[i];
+      s_b2[i] = p.b2[i];
     }
-  };
-  auto load_w3 = [&]() {  // W3t (512 k x 16 n), MN-major: LBO 256 between k-groups, SBO 128
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int c = tid + i * kMlpThreads, kr = c >> 1, nc = c & 1;
-      umma::cp16(w3s + (uint32_t)((kr >> 3) * 256 + nc * 128 + (kr & 7) * 16), p.W3t + (size_t)kr * 16 + nc * 8,
-                 true);
-    }
-  };
-  // W2 chunk g (global count of this CTA's chunks): slot g % 4, rows 256 ((g % 32) / 16), k 32 (g % 16)
-  auto produce = [&](int g) -> bool {
-    const int s = g & 3, t = g & 31;
-    if (g >= 4 && !umma::mbar_wait(&empty[s], ((g >> 2) - 1) & 1)) return false;
-    mbar_expect_tx(&full[s], kSlotBytes);
-    bulk_load(ring + (uint32_t)s * kSlotBytes, p.W2p + (size_t)t * (kSlotBytes / 2), kSlotBytes, &full[s]);
-    return true;
-  };
-
+  }
   load_x(blockIdx.x);
-  load_w1();
   umma::cp_commit();
+  bool w2_ready = false;
   int it = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int g0 = it * 32;
-    // W2 chunks 0-2 go to slots 0-2 at once (free: the previous tile's L2 and L3 have completed), so they
-    // stream while X and W1 land and layer 1 runs
-    if (tid == 0)
-      for (int g = g0; g < g0 + 3; ++g)
-        if (!produce(g)) s_abort = 1;
-    // ---- layer 1 (X and W1 landed; the previous tile's TMEM reads are done)
+    // ---- layer 1 (X landed; the previous tile's TMEM reads are done)
     umma::cp_wait<0>();
     umma::fence_async_smem();
     umma::tc_before_sync();
@@ -1195,68 +1183,52 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
     if (s_abort) break;
     if (tid == 32) {
       umma::tc_after_sync();
-      const uint64_t ad = umma::sdesc(xs, 128, 256);
-      umma::mma(tmem, ad, umma::sdesc(w1s, 128, 256), ID_HID, 0u);
-      umma::mma(tmem + 256, ad, umma::sdesc(w1s + 8192, 128, 256), ID_HID, 0u);
+      umma::mma(tmem, umma::sdesc(xs, 128, 256), umma::sdesc(w1s, 128, 256), ID_HID, 0u);
       umma::commit(&bar_l1);
     }
     if (!umma::mbar_wait(&bar_l1, it & 1)) s_abort = 1;
+    if (tile + (int)gridDim.x < ntiles) load_x(tile + gridDim.x);  // layer 1 has read X
+    umma::cp_commit();
     umma::tc_after_sync();
     mlp_epi_hidden(tmem, hs, s_b1, warp, lane);
     umma::fence_async_smem();
     umma::tc_before_sync();
     __syncthreads();
     if (s_abort) break;
-    // ---- layer 2: producer thread 0, MMA thread 32; everyone else waits for the last commit
-    if (tid == 0) {
-      for (int g = g0 + 3; g < g0 + 32; ++g)  // slot 3 held W1: free since L1 completed
-        if (!produce(g)) {
-          s_abort = 1;
-          break;
-        }
-    } else if (tid == 32) {
+    // ---- layer 2: A = H1 (K-major, SBO 4096), B = the resident W2 chunk t (LBO 4096, SBO 128)
+    if (tid == 32) {
+      umma::tc_after_sync();
       bool ok = true;
-      for (int t = 0; t < 32; ++t) {
-        const int g = g0 + t, s = g & 3;
-        if (!umma::mbar_wait(&full[s], (g >> 2) & 1)) {
-          ok = false;
-          break;
-        }
-        umma::tc_after_sync();
-        const int c32 = t & 15;
-        const uint32_t d = tmem + (uint32_t)((t >> 4) * 256), slot = ring + (uint32_t)s * kSlotBytes;
+      if (!w2_ready) ok = umma::mbar_wait(&bar_w, 0);
+      if (ok) {
+#pragma unroll 1
+        for (int t = 0; t < kNH / 32; ++t)
 #pragma unroll
-        for (int kk = 0; kk < 2; ++kk)
-          umma::mma(d, umma::sdesc(hs + (uint32_t)((c32 * 4 + kk * 2) * 128), 128, 8192),
-                    umma::sdesc(slot + (uint32_t)(kk * 8192), 4096, 128), ID_HID, (c32 > 0 || kk > 0) ? 1u : 0u);
-        umma::commit(&empty[s]);
-      }
-      if (ok)
+          for (int kk = 0; kk < 2; ++kk)
+            umma::mma(tmem, umma::sdesc(hs + (uint32_t)((t * 4 + kk * 2) * 128), 128, 4096),
+                      umma::sdesc(w2s + (uint32_t)t * kChunkBytes + (uint32_t)(kk * 8192), 4096, 128), ID_HID,
+                      (t > 0 || kk > 0) ? 1u : 0u);
         umma::commit(&bar_l2);
-      else
+      } else {
         s_abort = 1;
+        umma::commit(&bar_l2);  // nothing issued: completes at once, so no thread waits for the full bound
+      }
     }
+    w2_ready = true;
     __syncwarp();
     if (!umma::mbar_wait(&bar_l2, it & 1)) s_abort = 1;
-    load_w3();  // slot 2 and slot 3 are free: every L2 MMA has completed
-    if (tile + (int)gridDim.x < ntiles) {
-      load_x(tile + gridDim.x);
-      load_w1();
-    }
-    umma::cp_commit();
     umma::tc_after_sync();
-    mlp_epi_hidden(tmem, hs, s_b2, warp, lane);
-    umma::cp_wait<0>();
+    mlp_epi_hidden(tmem, hs, s_b2, warp, lane);  // H2 over H1: every layer-2 MMA has completed
     umma::fence_async_smem();
     umma::tc_before_sync();
     __syncthreads();
     if (s_abort) break;
-    // ---- layer 3
+    // ---- layer 3: A = H2, B = W3t (MN-major)
     if (tid == 32) {
       umma::tc_after_sync();
 #pragma unroll 4
-      for (int kk = 0; kk < 32; ++kk)
-        umma::mma(tmem, umma::sdesc(hs + (uint32_t)(kk * 256), 128, 8192), umma::sdesc(w3s + (uint32_t)(kk * 512), 256, 128),
+      for (int kk = 0; kk < kNH / 16; ++kk)
+        umma::mma(tmem, umma::sdesc(hs + (uint32_t)(kk * 256), 128, 4096), umma::sdesc(w3s + (uint32_t)(kk * 512), 256, 128),
                   ID_OUT, kk > 0 ? 1u : 0u);
       umma::commit(&bar_l3);
     }
@@ -1281,7 +1253,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
   umma::tc_before_sync();
   __syncthreads();
   if (s_abort && tid == 0) set_status(p.status, ARP_ERR_TIMEOUT);
-  if (warp == 0) umma::tmem_free(tmem, 512);
+  if (warp == 0) umma::tmem_free(tmem, kNH);
 }
 
 }  // namespace arp
@@ -1314,6 +1286,6 @@ extern "C" int arp_mlp_forward(const void* X, int rows, const void* W1, const fl
 
 extern "C" int arp_mlp_pack_w2(const void* W2, void* W2p, void* stream) {
   if (!W2 || !W2p || !al16(W2) || !al16(W2p)) return ARP_ERR_ARG;
-  k_pack_w2<<<(512 * 64 + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const bf16*)W2, (bf16*)W2p);
+  k_pack_w2<<<(kNH * kNH / 8 + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const bf16*)W2, (bf16*)W2p);
   return cudaGetLastError() == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }

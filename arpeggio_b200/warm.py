@@ -20,7 +20,7 @@ import torch
 from . import _lib, channel
 from .detector import Detector, M32
 
-NF, NH, NO = 16, 512, 16
+NF, NH, NO = 16, 256, 16
 EPI_F32, EPI_ACC, EPI_RELU_BF16, EPI_BIAS_F32, EPI_MASK_BF16 = range(5)
 
 
@@ -32,7 +32,7 @@ def gemm(A, a_mn, lda, B, b_mn, ldb, M, N, K, epi, C, ldc, bias=None, aux=None, 
 
 
 class WarmMLP:
-    """16 features -> 512 -> 512 -> 16 logits (the first P + 1 used), ReLU, BF16 weights and activations, FP32
+    """16 features -> 256 -> 256 -> 16 logits (the first P + 1 used), ReLU, BF16 weights and activations, FP32
     accumulate and FP32 master weights with Adam.  Weights live in one flat buffer in the order of LAYOUT; W3t is
     the last layer stored as (in, out)."""
     LAYOUT = (('W1', (NH, NF)), ('b1', (NH,)), ('W2', (NH, NH)), ('b2', (NH,)), ('W3t', (NH, NO)), ('b3', (NO,)))

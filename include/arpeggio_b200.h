@@ -187,7 +187,7 @@ int arp_mdi_select(const int8_t* cur, const float* dist, int B, int D, int G, in
 int arp_anneal_tune(int D, int P, int policy, int precision, int warps);
 
 /* ---- Learned warm start for first-accept annealing.  No counterpart in the reference, which has no learned
- * component: a per-coordinate MLP (16 features -> 512 -> 512 -> P+1 logits over the coordinate's spin sum
+ * component: a per-coordinate MLP (16 features -> 256 -> 256 -> P+1 logits over the coordinate's spin sum
  * m_j = 2c - P, BF16 weights and activations, FP32 accumulate) emits the start state and the flip-test order.
  * bf16 arrays are passed as void* (2-byte IEEE bfloat16). */
 
@@ -228,15 +228,16 @@ int arp_colsum_bf16(const void* X, int rows, int cols, int ld, float* out, void*
 int arp_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, float lr, float beta1, float beta2,
              float eps, int step, float grad_scale, void* stream);
 
-/* W2 (512, 512) bf16 row-major -> W2p, the same 512 x 512 values in the order arp_mlp_forward streams them
- * (32 chunks of 256 rows x 32 k; within a chunk k-group of 8, then row, then element).  Once per weight update. */
+/* W2 (256, 256) bf16 row-major -> W2p, the same 256 x 256 values in the order arp_mlp_forward keeps them in
+ * shared memory (8 chunks of 256 rows x 32 k; within a chunk k-group of 8, then row, then element).  Once per
+ * weight update. */
 int arp_mlp_pack_w2(const void* W2, void* W2p, void* stream);
 
 /* The network's forward pass in one persistent launch (no reference counterpart): logits (rows, 16) float =
- * relu(relu(X W1^T + b1) W2^T + b2) W3t + b3 with X (rows, 16), W1 (512, 16), W2 (512, 512) given packed as W2p
- * (arp_mlp_pack_w2), W3t (512, 16) bf16 and fp32 biases; per 128-row tile the hidden activations stay in TMEM and
- * shared memory (bf16, the same roundings and summation order as the three arp_gemm_bf16 calls of the training
- * path). */
+ * relu(relu(X W1^T + b1) W2^T + b2) W3t + b3 with X (rows, 16), W1 (256, 16), W2 (256, 256) given packed as W2p
+ * (arp_mlp_pack_w2), W3t (256, 16) bf16 and fp32 biases; the weights stay in shared memory for the whole launch
+ * and per 128-row tile the hidden activations stay in TMEM and shared memory (bf16, the same roundings and
+ * summation order as the three arp_gemm_bf16 calls of the training path). */
 int arp_mlp_forward(const void* X, int rows, const void* W1, const float* b1, const void* W2p, const float* b2,
                     const void* W3t, const float* b3, float* logits, int32_t* status, void* stream);
 

@@ -343,7 +343,7 @@ def list_llr(H, y, N0, allc, d, best, M, clip=50.0):
 # The reference has no learned component, so these restate this package's own warm-start definitions (feature
 # map, bf16 MLP, warm start, warm anneal) for the GPU parity tests; parity here is self-consistency, not a pin
 # to the reference.
-NF, NH, NO = 16, 512, 16
+NF, NH, NO = 16, 256, 16
 
 
 def bf16(x):

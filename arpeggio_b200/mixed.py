@@ -23,7 +23,7 @@ CONSTELLATIONS = (4, 16, 64)
 
 
 def mixed_classes():
-    """The north-star mix: users x antenna ratio x constellation (54 classes)."""
+    """The mixed-size workload: users x antenna ratio x constellation (54 classes)."""
     return [(nt, int(round(nt * r)), M) for nt in USERS for r in ANTENNA_RATIOS for M in CONSTELLATIONS]
 
 

@@ -501,3 +501,21 @@ def test_block_per_problem_kernels_equal_the_warp_kernels(nt):
             assert torch.equal(a[:Bs], b)
         if sampled:
             assert 0 < int((big[5] == 8).sum()) < Bb
+
+
+def test_host_device_pointer_refuses_unmapped_memory():
+    """Only mapped pinned memory has a device address: pageable host memory and device memory are refused with
+    ARP_ERR_ARG (the host-side query fails; nothing runs on the device)."""
+    import ctypes
+    from arpeggio_b200 import _lib
+    L = _lib.lib()
+    pinned = torch.empty(64, dtype=torch.int8).pin_memory()
+    d = ctypes.c_void_p()
+    assert L.arp_host_device_pointer(ctypes.c_void_p(pinned.data_ptr()), ctypes.byref(d)) == 0 and d.value
+    pageable = np.zeros(64, dtype=np.int8)
+    dev = torch.empty(64, dtype=torch.int8, device='cuda')
+    for ptr in (pageable.ctypes.data, dev.data_ptr()):
+        d = ctypes.c_void_p(1)
+        assert L.arp_host_device_pointer(ctypes.c_void_p(ptr), ctypes.byref(d)) == 3  # ARP_ERR_ARG
+        assert not d.value
+    assert L.arp_host_device_pointer(None, ctypes.byref(d)) == 3

@@ -49,6 +49,41 @@ __device__ __forceinline__ float hsum16(float v) {
   return v;
 }
 
+// TB consecutive floats of shared memory in one access (16-byte aligned when TB % 4 == 0, 8-byte when TB == 2).
+template <int TB>
+__device__ __forceinline__ void lds_vec(const float* p, float (&v)[TB]) {
+  if constexpr (TB % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < TB / 4; ++q) {
+      const float4 t = reinterpret_cast<const float4*>(p)[q];
+      v[4 * q] = t.x;
+      v[4 * q + 1] = t.y;
+      v[4 * q + 2] = t.z;
+      v[4 * q + 3] = t.w;
+    }
+  } else if constexpr (TB == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+#pragma unroll
+    for (int i = 0; i < TB; ++i) v[i] = p[i];
+  }
+}
+template <int TB>
+__device__ __forceinline__ void sts_vec(float* p, const float (&v)[TB]) {
+  if constexpr (TB % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < TB / 4; ++q)
+      reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  } else if constexpr (TB == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < TB; ++i) p[i] = v[i];
+  }
+}
+
 // A row's dot product sum_j x_j y_j: the thread's TB columns as one fma chain (from 0), then the butterfly over
 // the 16 threads of the row.
 template <int TB>
@@ -107,11 +142,8 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
     __syncthreads();
     for (int r = 0; r < nr; ++r) {
       float ai[TB], bj[TB];
-#pragma unroll
-      for (int i = 0; i < TB; ++i) {
-        ai[i] = Hc[r * Dp + ty * TB + i];
-        bj[i] = Hc[r * Dp + tx * TB + i];
-      }
+      lds_vec<TB>(Hc + r * Dp + ty * TB, ai);
+      lds_vec<TB>(Hc + r * Dp + tx * TB, bj);
 #pragma unroll
       for (int i = 0; i < TB; ++i)
 #pragma unroll
@@ -148,21 +180,24 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
       for (int kr = 0; kr < TB; ++kr) {
         const int k = kt * TB + kr, buf = (k & 1) * Dp;
         if (ty == kt) {
+          float rw[TB];
 #pragma unroll
-          for (int j = 0; j < TB; ++j) rk[buf + tx * TB + j] = A[kr][j];
+          for (int j = 0; j < TB; ++j) rw[j] = A[kr][j];
+          sts_vec<TB>(rk + buf + tx * TB, rw);
         }
         if (tx == kt) {
+          float cw[TB];
 #pragma unroll
-          for (int i = 0; i < TB; ++i) ck[buf + ty * TB + i] = A[i][kr];
+          for (int i = 0; i < TB; ++i) cw[i] = A[i][kr];
+          sts_vec<TB>(ck + buf + ty * TB, cw);
         }
         __syncthreads();
         const float inv = __frcp_rn(rk[buf + k]);
         float f[TB], rj[TB];
+        lds_vec<TB>(ck + buf + ty * TB, f);
+        lds_vec<TB>(rk + buf + tx * TB, rj);
 #pragma unroll
-        for (int i = 0; i < TB; ++i) {
-          f[i] = __fmul_rn(ck[buf + ty * TB + i], inv);
-          rj[i] = rk[buf + tx * TB + i];
-        }
+        for (int i = 0; i < TB; ++i) f[i] = __fmul_rn(f[i], inv);
 #pragma unroll
         for (int i = 0; i < TB; ++i)
 #pragma unroll

@@ -125,6 +125,52 @@ def cpu_sample(args, nthreads, target_s):
         n = int(min(args.batch, max(2 * n, rate * target_s)))
 
 
+def chord_engine_baseline(det, stream, target_s):
+    """Chord's solver alone, both sides on the detector's own integer problems (G, h), schedule, instance numbers
+    and key: this library's anneal over the whole batch on the GPU (CUDA events) against the reference's C++
+    engine model (engine_model.cpp engine_solve_batch, Philox numbers, all host threads) on a bounded sample,
+    whose outputs must equal the GPU's bit for bit."""
+    import torch
+    from arpeggio_b200 import arpeggiofx
+    from oracle import ref_engine
+    if not ref_engine.available():
+        return {'unavailable': 'oracle/_ref/libape.so not built (make -C oracle ref needs the reference tree)'}
+    B, R, P, D = det.B, det.R, det.P, det.D
+    key = 12
+    args = (det.G, det.h, P, R, det.T, det.q, det.inst, key, 'rand', 'chord', det.c)
+    arpeggiofx.anneal(*args)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s, de, st, status = arpeggiofx.anneal(*args)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    arpeggiofx.check_status(status)
+    ms = e0.elapsed_time(e1)
+    T = det.schedule['T']
+    c = det.schedule['c'] if det.schedule['c'] is not None else [0] * len(T)
+    nthreads = os.cpu_count() or 1
+    n, rate, dt = 16, None, 0.0
+    while True:
+        G = det.G[:n].cpu().numpy()
+        h = det.h[:n].cpu().numpy()
+        inst = det.inst[:n].cpu().numpy().view(np.uint32)
+        t0 = time.perf_counter()
+        es, ede, cyc, est = ref_engine.solve_batch(G, h, P, R, T, c, det.q, inst, key, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        rate = n / dt
+        if dt >= 0.5 * target_s or n >= B:
+            break
+        n = int(min(B, max(2 * n, rate * target_s)))
+    equal = bool(np.array_equal(es, s[:n].cpu().numpy()) and np.array_equal(ede, de[:n].cpu().numpy()))
+    return {'gpu_anneal_only': {'value': B / (ms / 1e3), 'unit': 'detections/s', 'ms': ms, 'uses': B},
+            'cpu_baseline': {'value': rate, 'unit': 'detections/s', 'cores': nthreads, 'kind': 'reference',
+                             'sample': '%d channel uses x %d anneals x %d steps through the reference\'s C++ Chord '
+                                       'engine model (4 contexts, Philox numbers), %.1f s' % (n, R, len(T), dt)},
+            'equal_to_gpu_on_sample': equal,
+            'engine_cycles_per_use': float(cyc.mean()),
+            'engine_cycles_model': 'Engine::cycle() clock edges from the first coupling row to idle, 4 contexts'}
+
+
 # ---------------------------------------------------------------- cross-rank timing
 def max_over_ranks(values, world, device='cpu'):
     """Per-rank device times (ms) -> their maximum over all ranks (every rank takes part, same order)."""
@@ -542,6 +588,8 @@ def run_ours(args):
                            'ber': float((dtx.bits != btx).float().mean()),
                            'flips_per_anneal': float(dtx.st[..., 0].float().mean()),
                            'tests_per_anneal': float(dtx.st[..., 1].float().mean())}
+            if name == 'chord_x32' and world == 1 and not args.no_cpu:
+                extra[name]['solver_vs_reference_engine'] = chord_engine_baseline(dtx, stream, 6.0)
             del dtx
 
     # ---- the reference's full chain: multi-stage MDI at its recorded x16 point (16 x 16, 20 dB, Ns 32,

@@ -179,3 +179,29 @@ def test_reference_chord_kernel_timing(golden):
         assert torch.equal(a, b)
     print('\nreference chord_m%d: %.3f ms, this project: %.3f ms for 2048 problems x %d anneals, N = %d (%.2fx)'
           % (F['h'].shape[1] // 32, t_ref, t_ours, R, F['h'].shape[1], t_ref / t_ours))
+
+
+@pytest.mark.parametrize('nt,K,steps,kappa', [(32, 1, 256, 0.0), (16, 1, 256, 0.3), (64, 2, 64, 0.3)])
+def test_chord_round_equals_reference_engine(nt, K, steps, kappa):
+    """This project's Chord round on compressed problems (arp_anneal_chord_dd, 'rand' start) against the reference's
+    C++ engine model (arpeggio/sim/x3model/engine_model.cpp, Philox numbers, built into oracle/_ref/libape.so):
+    best spins and best energy changes bit for bit, flips per problem equal."""
+    from arpeggio_b200 import arpeggiofx
+    from arpeggio_b200.detector import chord_schedule
+    from oracle import ref_engine
+    if not ref_engine.available():
+        pytest.skip('reference engine not built (make -C oracle ref needs the reference tree)')
+    B, R, P = 48, 8, 2 * K
+    det = _problems(B, nt, 14.0, 90 + nt, R, 8)
+    T, q, c = chord_schedule(steps, 0.3, 0.3, 0.4, kappa=kappa)
+    key = 0xABCDEF0123 + nt
+    inst = torch.arange(B, dtype=torch.int32, device='cuda') * 11 + 1
+    s, de, st, status = arpeggiofx.anneal(det.G, det.h, P, R, torch.tensor(T, dtype=torch.int32, device='cuda'), q,
+                                          inst, key, 'rand', 'chord', torch.tensor(c, dtype=torch.int32, device='cuda'))
+    torch.cuda.synchronize()
+    arpeggiofx.check_status(status)
+    es, ede, _, est = ref_engine.solve_batch(det.G.cpu().numpy(), det.h.cpu().numpy(), P, R, T, c, q,
+                                             inst.cpu().numpy().view(np.uint32), key, nthreads=os.cpu_count() or 1)
+    assert np.array_equal(s.cpu().numpy(), es)
+    assert np.array_equal(de.cpu().numpy(), ede)
+    assert np.array_equal(st[..., 0].sum(dim=1).cpu().numpy(), est[:, 1])

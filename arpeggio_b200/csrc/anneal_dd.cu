@@ -386,11 +386,14 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
   }
   const uint32_t inst = a.inst ? a.inst[b] : a.inst0 + (uint32_t)b;
   const PhiloxKeys& K = *reinterpret_cast<const PhiloxKeys*>(a.rk0);
+  // 2 G_jj; a padding lane (j >= D: h_j = 0 and G's row and column j are zero, so w_j stays 0) gets 2^29, making
+  // its margin psi2 = 2^30 + s at least every threshold kap2 = 2 (ceil(u 4 T / 2^32) - B) <= 2^30 (|4 T| <= 2^28,
+  // |B| <= 2^28 by the range checks): it never accepts, with no per-pass validity select.
   int32_t dg2[NS];
 #pragma unroll
   for (int t = 0; t < NS; ++t) {
     const int j = t * 32 + lane;
-    dg2[t] = j < D ? 2 * Gs[j * DP + j] : 0;
+    dg2[t] = j < D ? 2 * Gs[j * DP + j] : (1 << 29);
   }
 
   int Rb = R;
@@ -508,7 +511,9 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
           if (k >= L) break;
           ++passes;
           const int32_t Tk = Tg[k];
-          const long long A = 4LL * Tk;
+          // ceil(u 4 T / 2^32) as one unsigned multiply-add: with A = 4 T as a 32-bit pattern (|4 T| <= 2^28),
+          // u A + 2^32 - 1 < 2^64, and for T < 0 the pattern adds u 2^32, taken back by subtracting u
+          const uint32_t A32 = 4u * (uint32_t)Tk, Aneg = Tk < 0 ? 0xFFFFFFFFu : 0u;
           const int32_t Bk = a.qi + 2 * Tk - ((CHORD && cg) ? cg[k] : 0);
           int32_t psi2[NS], kap2[NS], cp[NS];
 #pragma unroll
@@ -522,22 +527,21 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
               philox10(c0, c1, c2, c3, K);
               u = i == 0 ? c0 : (i == 1 ? c1 : (i == 2 ? c2 : c3));
             }
-            const bool valid = t * 32 + lane < D;
-            const bool up = (sp >> (p * NS + t)) & 1u;
-            const int32_t psi = (up ? w[t] : -w[t]) + dg2[t];
-            psi2[t] = 2 * psi + (up ? 1 : 0);
-            kap2[t] = valid ? 2 * ((int32_t)ceil_shift32(u, A) - Bk) : -(1 << 30);
-            cp[t] = up ? 8 : -8;
+            const int32_t upb = (int32_t)((sp >> (p * NS + t)) & 1u), sg = 2 * upb - 1;
+            psi2[t] = 2 * (sg * w[t] + dg2[t]) + upb;
+            const uint32_t hi = (uint32_t)(((uint64_t)u * A32 + 0xFFFFFFFFull) >> 32);
+            kap2[t] = 2 * ((int32_t)(hi - (u & Aneg)) - Bk);
+            cp[t] = 8 * sg;
           }
           int jl = -1;
           // commit the flip of lane l of slot ts: energy, margins, spin bit
           auto commit = [&](int ts, int l, int32_t vsel) {
             const int32_t packed = __shfl_sync(ARP_FULL, vsel, l);
             de += 4LL * (packed >> 1);
-            const bool so_up = packed & 1;
+            const int32_t so = 2 * (packed & 1) - 1;  // the flipped coordinate's old spin
             const int32_t* gr = Gs + (ts * 32 + l) * DP + lane;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) psi2[t] += (so_up ? cp[t] : -cp[t]) * gr[t * 32];
+            for (int t = 0; t < NS; ++t) psi2[t] += (so * cp[t]) * gr[t * 32];
             if (lane == l) sp ^= 1u << (p * NS + ts);
             jl = ts * 32 + l;
           };

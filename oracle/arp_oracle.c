@@ -13,6 +13,8 @@
  *                    the contract of arpeggio/sim/arpeggio_fx.cu:35-100), policy 1 = Chord's
  *                    snapshot round (arpeggio_ref59.py:72-82 mode 'par', plus the Onsager term
  *                    of arpeggio/mimo/chordfx.py:105).
+ *  orc_anneal_chord_hw the Chord round on compressed G with the random numbers of the reference's C++
+ *                    engine model without Philox (arpeggio/sim/x3model/engine_model.cpp, philox = 0).
  *  orc_anneal_chord  Chord on a full N x N int16 coupling: arpeggio/mimo/chordfx.py:80-118
  *                    (chord_fx), modes 'chains' and 'best'.
  *  orc_anneal_dd_f32 the same two policies with FP32 fields (no reference kernel exists; the
@@ -282,6 +284,111 @@ int orc_anneal_dd_warm(const int32_t* G, const int32_t* h, int B, int D, int P, 
   if (cdf && P != 2) return 1;
   dd_ctx x = {G, h, T, NULL, B, D, P, R, L, q, inst, k0, k1, 2, 0, out_s, out_de, out_st, m0, warm_r, cdf, ra};
   orc_run(dd_job, &x, (long)B * R, nthreads);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ Chord with the engine's own numbers
+ * The Chord round of orc_anneal_dd (policy 1) with the random numbers of the reference's C++ engine model when it
+ * runs without Philox (philox = 0 of arpeggio/sim/x3model/engine_model.cpp, the mode of its production scripts
+ * arpeggio/sim/x3_prod.py:105-106 and run_a516.py:135-136):
+ *  - per anneal a seed chain of three murmur-style mixing rounds over (key low ^ inst), key high and r (the
+ *    seeder's pop :185-194 and B chain :170-178), whose result + phi seeds the lanes;
+ *  - lane j: mix(seed + j phi) (lane groups :179-184, stage B :165-167), finalised, zero replaced by phi, then one
+ *    xorshift32 step (stage C :142-163): that word is the lane's generator state and its bits 31, 30, ... are the
+ *    start spins of copies 0, 1, ...;
+ *  - every step advances every lane's state by one xorshift32 step and takes its top 16 bits u (decision D1
+ *    :242-257); the test is u 4 T > (s w_j + 2 G_jj + q - c + 2 T) 2^16 (D2 :229-240);
+ *  - the best state starts at 2^35 - 1 (:46) and is taken after every step (D0 :264, the final check :128).  */
+static inline uint32_t hw_mix_a(uint32_t v) { return (v ^ (v >> 16)) * 0x85EBCA6Bu; }
+static inline uint32_t hw_mix_b(uint32_t v) { return (v ^ (v >> 13)) * 0xC2B2AE35u; }
+static inline uint32_t hw_fin(uint32_t v) { return v ^ (v >> 16); }
+static inline uint32_t hw_xs32(uint32_t x) {
+  x ^= x << 13;
+  x ^= x >> 17;
+  x ^= x << 5;
+  return x;
+}
+
+typedef struct {
+  const int32_t *G, *h, *T, *c;
+  int B, D, P, R, L;
+  int32_t q;
+  const uint32_t* inst;
+  uint64_t key;
+  int8_t* out_s;
+  int64_t *out_de, *out_st;
+} hw_ctx;
+
+static void hw_job(void* vctx, long t) {
+  const hw_ctx* x = (const hw_ctx*)vctx;
+  const int D = x->D, P = x->P, R = x->R;
+  const long b = t / R;
+  const uint32_t r = (uint32_t)(t % R), PHI = 0x9E3779B9u;
+  const int32_t* G = x->G + (size_t)b * D * D;
+  const int32_t* h = x->h + (size_t)b * D;
+  uint32_t f = hw_fin(hw_mix_b(hw_mix_a((uint32_t)x->key ^ x->inst[b])));
+  f = hw_fin(hw_mix_b(hw_mix_a(f ^ (uint32_t)(x->key >> 32))));
+  f = hw_fin(hw_mix_b(hw_mix_a(f ^ r)));
+  const uint32_t seed = f + PHI;
+  uint32_t rng[128];
+  int8_t s[6 * 128], bs[6 * 128];
+  int64_t w[128];
+  uint8_t F[128];
+  for (int j = 0; j < D; j++) {
+    uint32_t v = hw_fin(hw_mix_b(hw_mix_a(seed + (uint32_t)j * PHI)));
+    if (v == 0) v = PHI;
+    rng[j] = hw_xs32(v);
+    for (int p = 0; p < P; p++) s[p * D + j] = ((rng[j] >> (31 - p)) & 1u) ? 1 : -1;
+  }
+  memcpy(bs, s, (size_t)P * D);
+  for (int i = 0; i < D; i++) { /* w_i = h_i - 2 sum_j G_ij m_j */
+    int64_t acc = 0;
+    for (int j = 0; j < D; j++) {
+      int m = 0;
+      for (int p = 0; p < P; p++) m += s[p * D + j];
+      acc += (int64_t)G[i * D + j] * m;
+    }
+    w[i] = h[i] - 2 * acc;
+  }
+  int64_t de = 0, best = ((int64_t)1 << 35) - 1, flips = 0;
+  for (int k = 0; k < x->L; k++) {
+    const int p = k % P;
+    const __int128 A = (__int128)4 * x->T[k];
+    const int64_t Bk = (int64_t)x->q - (x->c ? (int64_t)x->c[k] : 0) + 2 * (int64_t)x->T[k];
+    int8_t* sp = s + p * D;
+    for (int j = 0; j < D; j++) {
+      rng[j] = hw_xs32(rng[j]);
+      const uint32_t u = rng[j] >> 16;
+      const __int128 rhs = ((__int128)sp[j] * w[j] + 2 * (__int128)G[j * D + j] + Bk) * ((__int128)1 << 16);
+      F[j] = (__int128)u * A > rhs;
+    }
+    for (int j = 0; j < D; j++) {
+      if (!F[j]) continue;
+      const int so = sp[j];
+      de += 4 * (int64_t)so * w[j] + 8 * (int64_t)G[j * D + j];
+      for (int i = 0; i < D; i++) w[i] += 4 * (int64_t)so * G[j * D + i];
+      sp[j] = (int8_t)(-so);
+      flips++;
+    }
+    if (de < best) {
+      best = de;
+      memcpy(bs, s, (size_t)P * D);
+    }
+  }
+  memcpy(x->out_s + (size_t)t * P * D, bs, (size_t)P * D);
+  x->out_de[t] = best;
+  x->out_st[2 * t] = flips;
+  x->out_st[2 * t + 1] = x->L;
+}
+
+/* G (B, D, D), h (B, D); T, c (L) per step (c may be NULL); q; inst (B); the 64-bit key.  Outputs as
+ * orc_anneal_dd: best spins (B, R, P*D) copy-major, best energy change (B, R), (flips, steps) per anneal. */
+int orc_anneal_chord_hw(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T,
+                        const int32_t* c, int L, int32_t q, const uint32_t* inst, uint64_t key, int8_t* out_s,
+                        int64_t* out_de, int64_t* out_st, int nthreads) {
+  if (D < 1 || D > 128 || P < 1 || P > 6 || L < 1 || R < 1 || B < 0) return 1;
+  hw_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, key, out_s, out_de, out_st};
+  orc_run(hw_job, &x, (long)B * R, nthreads);
   return 0;
 }
 

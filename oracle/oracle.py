@@ -51,6 +51,8 @@ def lib():
         L.orc_anneal_full_f32.argtypes = [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P,
                                           _P, ctypes.c_int, ctypes.c_float, _P, ctypes.c_uint32, ctypes.c_uint32,
                                           ctypes.c_int, _P, _P, _P, ctypes.c_int]
+        L.orc_anneal_chord_hw.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
+                                          ctypes.c_int, ctypes.c_int32, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -87,6 +89,27 @@ def anneal_dd(G, h, P, R, T, q, inst, key, start, policy='arpeggio', c=None, nth
                              0 if policy == 'arpeggio' else 1, _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
     if rc:
         raise ValueError('orc_anneal_dd: unsupported shape')
+    return out_s, out_de, out_st
+
+
+def anneal_chord_hw(G, h, P, R, T, c, q, inst, key, nthreads=1):
+    """Chord's round on the compressed problem with the random numbers of the reference's C++ engine model run
+    without Philox (arpeggio/sim/x3model/engine_model.cpp, philox = 0; restated in arp_oracle.c).  T and c (L,)
+    one entry per step (c may be None).  Returns spins (B, R, P*D) int8, best energy change (B, R) int64 and
+    (B, R, 2) [flips, steps]."""
+    G = np.ascontiguousarray(G, dtype=np.int32)
+    h = np.ascontiguousarray(h, dtype=np.int32)
+    B, D, _ = G.shape
+    T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
+    cc = None if c is None else np.ascontiguousarray([int(x) for x in c], dtype=np.int32)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    out_s = np.zeros((B, R, P * D), dtype=np.int8)
+    out_de = np.zeros((B, R), dtype=np.int64)
+    out_st = np.zeros((B, R, 2), dtype=np.int64)
+    rc = lib().orc_anneal_chord_hw(_ptr(G), _ptr(h), B, D, P, R, _ptr(T), _ptr(cc), len(T), int(q), _ptr(it),
+                                   key & 0xFFFFFFFFFFFFFFFF, _ptr(out_s), _ptr(out_de), _ptr(out_st), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_chord_hw: unsupported shape')
     return out_s, out_de, out_st
 
 

@@ -48,11 +48,13 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def solve_batch(G, h, P, R, T, c, q, inst, key, contexts=4, nthreads=1):
+def solve_batch(G, h, P, R, T, c, q, inst, key, contexts=4, nthreads=1, philox=1):
     """B sub-problems, one engine each.  G (B, D, D) and h (B, D) integers, T and c (S,) one entry per step
     (S <= 1024), q an integer, inst (B,) uint32, key the 64-bit Philox key.  Returns spins (B, R, P D) int8
     copy-major, best energy change (B, R) int64, cycles (B,) from the first coupling row to idle and
-    stats (B, 4) = [decision ops (steps), flips, field-init ops, R-port busy cycles] summed over the R anneals."""
+    stats (B, 4) = [decision ops (steps), flips, field-init ops, R-port busy cycles] summed over the R anneals.
+    philox = 0 runs the engine with its own numbers (hash-seeded xorshift32 per lane, 16-bit draws), the mode of
+    the reference's production scripts."""
     G = _i16(G, 'G')
     h = _i16(h, 'h')
     B, D, _ = G.shape
@@ -68,7 +70,7 @@ def solve_batch(G, h, P, R, T, c, q, inst, key, contexts=4, nthreads=1):
     de = np.zeros((B, R), np.int64)
     cyc = np.zeros(B, np.int64)
     st = np.zeros((B, 4), np.int64)
-    lib().engine_solve_batch(D, contexts, seedl, 1, B, _ptr(G), _ptr(h), P, R, S, _ptr(T16), _ptr(c16), int(q),
+    lib().engine_solve_batch(D, contexts, seedl, 1 if philox else 0, B, _ptr(G), _ptr(h), P, R, S, _ptr(T16), _ptr(c16), int(q),
                              _ptr(it), ctypes.c_uint64(key & 0xFFFFFFFFFFFFFFFF), _ptr(spins), _ptr(de), _ptr(cyc),
                              _ptr(st), int(nthreads))
     return spins, de, cyc, st

@@ -59,3 +59,30 @@ def test_engine_refuses_wide_words():
     G[0, 0, 0] = 40000
     with pytest.raises(ValueError):
         ref_engine.solve_batch(G, np.zeros((1, 32), np.int32), 2, 1, [100], [0], 0, [0], 1)
+
+
+@pytest.mark.parametrize('D,K,R,steps,kappa,snr', [
+    (64, 1, 8, 256, 0.0, 14.0),    # 32 users, Chord's default schedule
+    (32, 1, 8, 256, 0.3, 20.0),    # 16 users, Onsager term on
+    (64, 2, 4, 128, 0.3, 10.0),    # four copies
+    (128, 1, 2, 64, 0.0, 22.0),    # 64 users, shortened
+])
+def test_oracle_chord_with_engine_numbers_equals_reference_engine(D, K, R, steps, kappa, snr):
+    """The engine's own numbers (philox = 0: hash-seeded xorshift32 per lane, 16-bit draws), the mode its
+    production scripts run: the oracle's restatement gives the engine's best spins, energies and flips."""
+    _engine()
+    from arpeggio_b200.detector import chord_schedule
+    B, P = 12, 2 * K
+    G, h = _random_dd(B, D, snr, 900 + D + K)
+    T, q, c = chord_schedule(steps, 0.3, 0.3, 0.4, kappa=kappa)
+    key = 0x0DDBA11C0FFEE + D
+    inst = (np.arange(B, dtype=np.int64) * 29 + 3) & 0xFFFFFFFF
+    es, ede, _, est = ref_engine.solve_batch(G, h, P, R, T, c, q, inst, key, nthreads=NTH, philox=0)
+    os_, ode, ost = O.anneal_chord_hw(G, h, P, R, T, c, q, inst, key, nthreads=NTH)
+    assert np.array_equal(es, os_)
+    assert np.array_equal(ede, ode)
+    assert np.array_equal(est[:, 1], ost[..., 0].sum(axis=1))
+    assert (ost[..., 1] == len(T)).all()
+    # a different stream from the Philox mode on the same problems
+    ps, _, _, _ = ref_engine.solve_batch(G, h, P, R, T, c, q, inst, key, nthreads=NTH, philox=1)
+    assert not np.array_equal(ps, es)

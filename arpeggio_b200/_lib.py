@@ -21,6 +21,7 @@ SIGNATURES = {
     'arp_philox_rate': [_P, _I, _I, _I, _P],
     'arp_anneal_first_accept': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
     'arp_anneal_chord_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
+    'arp_anneal_chord_engine': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _P, _P],
     'arp_anneal_dd_f32': [_I, _P, _P, _P, _P, _I, _F, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
     'arp_anneal_chord': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _U, _U, _U, _I, _I, _P, _P, _P, _P, _P],
     'arp_map_dd': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P],

@@ -60,6 +60,29 @@ def anneal(Gt, h, P, R, T, q, inst, key, start='rand', policy='arpeggio', c=None
     return s_, de, st, status
 
 
+@torch.no_grad()
+def anneal_engine(Gt, h, P, R, T, q, inst, key, c=None, out=None, status=None, stream=None):
+    """Chord's round with the random numbers of the reference's C++ engine model run without Philox
+    (engine_model.cpp engine_solve_batch with philox = 0): per-coordinate xorshift32 generators seeded from
+    (key, inst, r), which also give the start spins.  Device tensors as in `anneal` (T and c one entry per step);
+    returns (spins, de, st, status) without synchronising."""
+    B, D, _ = Gt.shape
+    dev = Gt.device
+    if out is None:
+        out = (torch.empty(B, R, P * D, dtype=torch.int8, device=dev),
+               torch.empty(B, R, dtype=torch.int64, device=dev),
+               torch.empty(B, R, 2, dtype=torch.int64, device=dev))
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+    s_, de, st = out
+    rc = _lib.lib().arp_anneal_chord_engine(_lib.ptr(Gt), _lib.ptr(h), _lib.ptr(T), _lib.ptr(c), int(T.shape[0]),
+                                            int(q), P, R, D, B, _lib.ptr(inst), key & M32, (key >> 32) & M32,
+                                            _lib.ptr(s_), _lib.ptr(de), _lib.ptr(st), _lib.ptr(status),
+                                            _lib.stream_ptr(stream))
+    _lib.check(rc, 'anneal_engine')
+    return s_, de, st, status
+
+
 def check_status(status):
     """Raises if a device-side check failed (synchronises on the status word)."""
     v = int(status.item())

@@ -320,11 +320,26 @@ __device__ __forceinline__ long long mad_wide_s32(int32_t a, int32_t b, long lon
   return d;
 }
 
+// The random numbers of the reference's C++ engine model run without Philox (arpeggio/sim/x3model/engine_model.cpp,
+// philox = 0): murmur-style mixing steps for the per-anneal seed chain and the lane seeds, xorshift32 per lane.
+__device__ __forceinline__ uint32_t eng_mix_a(uint32_t v) { return (v ^ (v >> 16)) * 0x85EBCA6Bu; }
+__device__ __forceinline__ uint32_t eng_mix_b(uint32_t v) { return (v ^ (v >> 13)) * 0xC2B2AE35u; }
+__device__ __forceinline__ uint32_t eng_fin(uint32_t v) { return v ^ (v >> 16); }
+__device__ __forceinline__ uint32_t eng_xs32(uint32_t x) {
+  x ^= x << 13;
+  x ^= x >> 17;
+  x ^= x << 5;
+  return x;
+}
+
 #ifndef ARP_ANNEAL_MINB
 #define ARP_ANNEAL_MINB 1
 #endif
 
-template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false>
+// ENG (Chord only): the engine's own numbers instead of Philox -- lane j's xorshift32 state starts from the anneal's
+// seed chain (engine_model.cpp:185-194, 170-184, 142-163), its bits 31, 30, ... give the start spins of copies
+// 0, 1, ..., and every step advances it once and tests with its top 16 bits: u 4 T > z 2^16 (:229-257).
+template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false, bool ENG = false>
 // Four slots (D > 96) are bounded at 128 registers: four 4-warp blocks per SM instead of three (no spills;
 // 64 users: 129 -> 120 ms per 32768 uses).
 __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
@@ -422,7 +437,22 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
   for (int r = bs + split * wid; r < Rb; r += split * W) {
     // ---- start state (arpeggio_fx.cu:48-57), packed per thread
     uint32_t sp = 0;
-    if constexpr (WARM) {
+    uint32_t es[ENG ? NS : 1];  // the engine's per-lane generator states
+    if constexpr (ENG) {
+      constexpr uint32_t PHI = 0x9E3779B9u;
+      uint32_t f = eng_fin(eng_mix_b(eng_mix_a(a.k0 ^ inst)));
+      f = eng_fin(eng_mix_b(eng_mix_a(f ^ a.k1)));
+      f = eng_fin(eng_mix_b(eng_mix_a(f ^ (uint32_t)r)));
+      const uint32_t seed = f + PHI;
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        uint32_t v = eng_fin(eng_mix_b(eng_mix_a(seed + (uint32_t)(t * 32 + lane) * PHI)));
+        es[t] = eng_xs32(v == 0 ? PHI : v);
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+          if ((es[t] >> (31 - p)) & 1u) sp |= 1u << (p * NS + t);
+      }
+    } else if constexpr (WARM) {
       // given spin sums: m = 0 takes the 'bal' pattern of the position's draw, m != 0 sets copies p < (m + P)/2
 #pragma unroll
       for (int t = 0; t < NS; ++t) {
@@ -491,13 +521,13 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
         for (int t = 0; t < NS; ++t) w[t] -= m2 * gr[t * 32];
       }
     }
-    long long de = 0, best = 1LL << 62;
+    long long de = 0, best = ENG ? (1LL << 35) - 1 : 1LL << 62;  // the engine's best register starts at 2^35 - 1
     uint32_t bsp = sp;
     int32_t flips = 0, lastflips = 0;
     const int nquad = (L + 4 * P - 1) / (4 * P);
     for (int q4 = 0; q4 < nquad; ++q4) {
       uint32_t cw[CACHE ? P : 1][CACHE ? NS : 1][4];
-      if constexpr (CACHE) {
+      if constexpr (CACHE && !ENG) {
 #pragma unroll
         for (int p = 0; p < P; ++p)
 #pragma unroll
@@ -525,7 +555,10 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
 #pragma unroll
           for (int t = 0; t < NS; ++t) {
             uint32_t u;
-            if constexpr (CACHE) {
+            if constexpr (ENG) {
+              es[t] = eng_xs32(es[t]);
+              u = es[t] >> 16;
+            } else if constexpr (CACHE) {
               // word i of the cached block, by selects (a runtime i must not index the register array)
               u = i == 0 ? cw[p][t][0] : (i == 1 ? cw[p][t][1] : (i == 2 ? cw[p][t][2] : cw[p][t][3]));
             } else {
@@ -535,8 +568,14 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
             }
             const int32_t upb = (int32_t)((sp >> (p * NS + t)) & 1u), sg = 2 * upb - 1;
             psi2[t] = 2 * (sg * w[t] + dg2[t]) + upb;
-            const uint32_t hi = (uint32_t)(((uint64_t)u * A32 + 0xFFFFFFFFull) >> 32);
-            kap2[t] = 2 * ((int32_t)(hi - (u & Aneg)) - Bk);
+            int32_t thr;
+            if constexpr (ENG) {  // ceil(u 4 T / 2^16), u < 2^16: |thr| <= |4 T| <= 2^28
+              thr = (int32_t)(((long long)u * (4LL * Tk) + 0xFFFFLL) >> 16);
+            } else {
+              const uint32_t hi = (uint32_t)(((uint64_t)u * A32 + 0xFFFFFFFFull) >> 32);
+              thr = (int32_t)(hi - (u & Aneg));
+            }
+            kap2[t] = 2 * (thr - Bk);
             cp[t] = 8 * sg;
           }
           int jl = -1;
@@ -633,10 +672,10 @@ static int pick_warps(K kern, size_t smem, int R) {
 // heuristic.  Process-wide, set through arp_anneal_tune.
 static int g_tuned_warps[5][7][2][2];
 
-template <int NS, int P, bool CHORD, bool FLT, bool WARM = false>
+template <int NS, int P, bool CHORD, bool FLT, bool WARM = false, bool ENG = false>
 static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   constexpr bool CACHE = P * NS <= 8;
-  auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE, WARM>;
+  auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE, WARM, ENG>;
   const size_t smem = (size_t)a.D * NS * 32 * 4;
   static size_t attr_smem = 48 * 1024;
   if (smem > attr_smem) {
@@ -734,9 +773,32 @@ cudaError_t anneal_dispatch(int policy, bool flt, const DDParams& a0, int P, int
   return policy == 0 ? launch_dd<false, false>(a, P, warps, st) : launch_dd<true, false>(a, P, warps, st);
 }
 
+// Chord with the engine's own numbers (integer fields; no Philox keys needed).
+static cudaError_t launch_engine(const DDParams& a, int P, cudaStream_t st) {
+  const int NS = (a.D + 31) / 32;
+#define ARP_CASE(ns, pp) \
+  if (NS == ns && P == pp) return launch_ns_p<ns, pp, true, false, false, true>(a, 0, st);
+  ARP_CASE(1, 2) ARP_CASE(1, 4) ARP_CASE(1, 6)
+  ARP_CASE(2, 2) ARP_CASE(2, 4) ARP_CASE(2, 6)
+  ARP_CASE(3, 2) ARP_CASE(3, 4) ARP_CASE(3, 6)
+  ARP_CASE(4, 2) ARP_CASE(4, 4) ARP_CASE(4, 6)
+#undef ARP_CASE
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace arp
 
 using namespace arp;
+
+extern "C" int arp_anneal_chord_engine(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c,
+                                       int L, int q, int P, int R, int D, int B, const uint32_t* inst, uint32_t k0,
+                                       uint32_t k1, int8_t* out_s, int64_t* out_de, int64_t* out_st,
+                                       int32_t* status, void* stream) {
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, 0, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  DDParams a{Gt, h, T, c, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, 0, out_s, out_de, out_st, status};
+  return launch_engine(a, P, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
+}
 
 extern "C" int arp_anneal_first_accept(const int32_t* Gt, const int32_t* h, const int32_t* T, int L, int q, int P,
                                        int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,

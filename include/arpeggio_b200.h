@@ -70,6 +70,18 @@ int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const int32_t* T, c
                         int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1, int start,
                         int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);
 
+/* The same Chord round with the random numbers of the reference's C++ engine model when it runs without Philox
+ * (arpeggio/sim/x3model/engine_model.cpp, engine_solve_batch :336-379 with philox = 0, as its production
+ * scripts arpeggio/sim/x3_prod.py:105-106 and run_a516.py:135-136 call it): per anneal a seed chain over
+ * (k0 ^ inst, k1, r), one xorshift32 generator per coordinate whose bits are the start spins, advanced once per
+ * step, 16-bit draws.  T and c (L) one entry per step, c may be NULL; key (k0 low, k1 high) = the engine's
+ * 64-bit seed.  Outputs as arp_anneal_chord_dd (tests = one per step); best spins and best energy changes equal
+ * the engine's, which starts its best at 2^35 - 1.  No start argument: the engine's start comes from its
+ * generators. */
+int arp_anneal_chord_engine(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L, int q,
+                            int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                            int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);
+
 /* FP32-field anneal on compressed dDI problems: policy 0 = first accept, 1 = Chord round.  Gt, h, T, c
  * (c may be NULL), q in float; out_de (B, R) float.  The float rule is the integer rule with the
  * decision z < thr, z = (s w_j + 2 G_jj) + q, thr = ((x >> 8) 2^-24 - 1/2) 4 T, one IEEE rounding per

@@ -205,3 +205,35 @@ def test_chord_round_equals_reference_engine(nt, K, steps, kappa):
     assert np.array_equal(s.cpu().numpy(), es)
     assert np.array_equal(de.cpu().numpy(), ede)
     assert np.array_equal(st[..., 0].sum(dim=1).cpu().numpy(), est[:, 1])
+
+
+@pytest.mark.parametrize('nt,K,steps,kappa', [(32, 1, 256, 0.0), (16, 1, 256, 0.3), (64, 1, 64, 0.0),
+                                              (32, 2, 128, 0.3), (48, 3, 48, 0.0)])
+def test_chord_engine_numbers_equal_reference_engine(nt, K, steps, kappa):
+    """arp_anneal_chord_engine (Chord with the engine's own numbers, the mode of the reference's production scripts)
+    against the reference's C++ engine model run with philox = 0 and against the oracle's restatement: best spins and
+    best energy changes bit for bit, flips per problem equal."""
+    from arpeggio_b200 import arpeggiofx
+    from arpeggio_b200.detector import chord_schedule
+    from oracle import oracle as O
+    from oracle import ref_engine
+    B, R, P = 48, 8, 2 * K
+    det = _problems(B, nt, 14.0, 120 + nt, R, 8)
+    T, q, c = chord_schedule(steps, 0.3, 0.3, 0.4, kappa=kappa)
+    key = 0xFEEDFACE12345 + nt
+    inst = torch.arange(B, dtype=torch.int32, device='cuda') * 5 + 2
+    s, de, st, status = arpeggiofx.anneal_engine(det.G, det.h, P, R, torch.tensor(T, dtype=torch.int32, device='cuda'),
+                                                 q, inst, key, torch.tensor(c, dtype=torch.int32, device='cuda'))
+    torch.cuda.synchronize()
+    arpeggiofx.check_status(status)
+    G, h, it = det.G.cpu().numpy(), det.h.cpu().numpy(), inst.cpu().numpy().view(np.uint32)
+    os_, ode, ost = O.anneal_chord_hw(G, h, P, R, T, c, q, it, key, nthreads=os.cpu_count() or 1)
+    assert np.array_equal(s.cpu().numpy(), os_)
+    assert np.array_equal(de.cpu().numpy(), ode)
+    assert np.array_equal(st.cpu().numpy(), ost)
+    if ref_engine.available():
+        es, ede, _, est = ref_engine.solve_batch(G, h, P, R, T, c, q, it, key, nthreads=os.cpu_count() or 1,
+                                                 philox=0)
+        assert np.array_equal(s.cpu().numpy(), es)
+        assert np.array_equal(de.cpu().numpy(), ede)
+        assert np.array_equal(st[..., 0].sum(dim=1).cpu().numpy(), est[:, 1])

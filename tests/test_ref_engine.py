@@ -65,6 +65,7 @@ def test_engine_refuses_wide_words():
     (64, 1, 8, 256, 0.0, 14.0),    # 32 users, Chord's default schedule
     (32, 1, 8, 256, 0.3, 20.0),    # 16 users, Onsager term on
     (64, 2, 4, 128, 0.3, 10.0),    # four copies
+    (96, 3, 2, 96, 0.3, 18.0),     # six copies, 48 users
     (128, 1, 2, 64, 0.0, 22.0),    # 64 users, shortened
 ])
 def test_oracle_chord_with_engine_numbers_equals_reference_engine(D, K, R, steps, kappa, snr):

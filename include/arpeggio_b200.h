@@ -76,8 +76,9 @@ int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const int32_t* T, c
  * (k0 ^ inst, k1, r), one xorshift32 generator per coordinate whose bits are the start spins, advanced once per
  * step, 16-bit draws.  T and c (L) one entry per step, c may be NULL; key (k0 low, k1 high) = the engine's
  * 64-bit seed.  Outputs as arp_anneal_chord_dd (tests = one per step); best spins and best energy changes equal
- * the engine's, which starts its best at 2^35 - 1.  No start argument: the engine's start comes from its
- * generators. */
+ * the engine's, which starts its best at 2^35 - 1 (an anneal none of whose steps ends below that returns its
+ * start spins here, where the engine keeps whatever its best-spin register last held).  No start argument: the
+ * engine's start comes from its generators. */
 int arp_anneal_chord_engine(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L, int q,
                             int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
                             int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);

@@ -59,8 +59,10 @@ class Kernel:
         torch.cuda.synchronize()
         return out.to(torch.int64) & MASK
 
-    def chord(self, F, R, seed, P=1, inst0=0, mode='chains', warps=8, stats=None):
-        """Kernel run with the same contract as chord_fx; returns (spins int8, 2 E0 int64) on the device."""
+    def chord(self, F, R, seed, P=1, inst0=0, mode='chains', warps=0, stats=None):
+        """Kernel run with the same contract as chord_fx; returns (spins int8, 2 E0 int64) on the device.
+        warps: anneals per block in flight (0 = the width with the most resident warps per SM); the reference's
+        default is 8, and the outputs do not depend on it."""
         B, N = F['h'].shape
         assert N % 32 == 0 and (N // P) % 32 == 0, 'spins per copy must be a multiple of 32'
         assert N // 32 in self.MPLS, 'unsupported spin count %d' % N

@@ -24,6 +24,7 @@
 // s w < ceil(u*4T / 2^32) - 2 G_jj - q - 2T, a 32-bit compare; the entry points bound |G|, |h|, |T|, |q|
 // so that every field and threshold fits 32 bits (ARP_ERR_RANGE otherwise).
 #include <climits>
+#include <mutex>
 #include <type_traits>
 
 #include "arp_common.cuh"
@@ -33,6 +34,7 @@ namespace arp {
 
 
 constexpr int32_t kMaxG = 1 << 18, kMaxH = 1 << 28, kMaxT = 1 << 26;
+constexpr int kMaxDevices = 64;
 
 template <int NS, int P, bool CHORD, bool FLT, bool CACHE>
 __global__ void __launch_bounds__(256) k_anneal_dd(const DDParams a) {
@@ -677,34 +679,45 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
   constexpr bool CACHE = P * NS <= 8;
   auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE, WARM, ENG>;
   const size_t smem = (size_t)a.D * NS * 32 * 4;
-  static size_t attr_smem = 48 * 1024;
-  if (smem > attr_smem) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_smem = smem;
-  }
-  static size_t cached_smem = 0;
-  static int cached_w = 0;
-  static int cached_nb = 0, sms = 0;
-  int per_sm = cached_nb > 0 ? cached_nb : 1;
-  if (warps <= 0) {
-    if (cached_w == 0 || cached_smem != smem) {
-      cached_w = pick_warps(kern, smem, 8);
-      cached_smem = smem;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_nb, kern, 32 * cached_w, smem) != cudaSuccess)
-        cached_nb = 1;
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // Launch settings per device (the shared-memory limit raised by cudaFuncSetAttribute applies to the current
+  // device only; occupancy and SM count are per device too), behind one lock per instantiation.
+  struct Slot {
+    size_t attr_smem = 48 * 1024, cached_smem = 0;
+    int cached_w = 0, cached_nb = 0, sms = 0;
+  };
+  static Slot slots_by_dev[kMaxDevices];
+  static std::mutex mu;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  int per_sm = 1, sms = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    Slot& sl = slots_by_dev[dev];
+    if (smem > sl.attr_smem) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      sl.attr_smem = smem;
     }
-    warps = cached_w;
-    per_sm = cached_nb > 0 ? cached_nb : 1;
-    const int tw = g_tuned_warps[NS][P][CHORD ? 1 : 0][FLT ? 1 : 0];
-    if (tw > 0 && tw != warps) {  // same resident warps per SM, another width
-      per_sm = cached_nb * cached_w / tw > 0 ? cached_nb * cached_w / tw : 1;
-      warps = tw;
+    if (warps <= 0 && (sl.cached_w == 0 || sl.cached_smem != smem)) {
+      sl.cached_w = pick_warps(kern, smem, 8);
+      sl.cached_smem = smem;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sl.cached_nb, kern, 32 * sl.cached_w, smem) != cudaSuccess)
+        sl.cached_nb = 1;
+      cudaDeviceGetAttribute(&sl.sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    while (warps > 1 && warps > a.R) warps >>= 1;
+    per_sm = sl.cached_nb > 0 ? sl.cached_nb : 1;
+    sms = sl.sms;
+    if (warps <= 0) {
+      warps = sl.cached_w;
+      const int tw = g_tuned_warps[NS][P][CHORD ? 1 : 0][FLT ? 1 : 0];
+      if (tw > 0 && tw != warps) {  // same resident warps per SM, another width
+        per_sm = sl.cached_nb * sl.cached_w / tw > 0 ? sl.cached_nb * sl.cached_w / tw : 1;
+        warps = tw;
+      }
+      while (warps > 1 && warps > a.R) warps >>= 1;
+    }
   }
   // Small batches: split each problem's anneals over several blocks so the batch still fills the GPU.
   DDParams b = a;

@@ -40,7 +40,7 @@ inline cudaError_t launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of two 32x32->64 multiplies,
 // Weyl key increments 0x9E3779B9 / 0xBB67AE85.  Counter (c0..c3) in place, key (k0, k1).
-// The counter layout each caller uses is the reference's (arpeggio_fx.cu:51,75; chord_kernel.cu:288,321).
+// The counter layout each caller uses is the reference's (arpeggio_fx.cu:51,75; chord_kernel.cu:74,107).
 __device__ __forceinline__ void philox10(uint32_t& c0, uint32_t& c1, uint32_t& c2, uint32_t& c3, uint32_t k0,
                                          uint32_t k1) {
 #pragma unroll

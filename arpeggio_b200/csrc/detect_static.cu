@@ -15,7 +15,9 @@
 //    start at zero because each stage writes its part before the next stage reads it, but two calls whose
 //    work overlaps on the GPU (different streams, or different host threads without ordering) race on it;
 //  * the first call on each device looks up the array's device address (cudaGetSymbolAddress, with that
-//    device current) and caches it; make that first call before any stream capture.
+//    device current) and caches it; make that first call before any stream capture.  The cached address
+//    outlives a cudaDeviceReset (or any reset of the primary context), after which it no longer names the
+//    array: the entry point is not for use on a device across such a reset.
 #include <mutex>
 
 #include "arp_common.cuh"

@@ -1054,18 +1054,6 @@ struct MlpParams {
   int bias16;  // b1 and b2 16-byte aligned: staged with cp.async
 };
 
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::su32(bar)), "r"(bytes)
-               : "memory");
-}
-
-// One contiguous global -> shared bulk copy (no tensor map), completing `bytes` on the mbarrier.
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(umma::su32(bar))
-               : "memory");
-}
-
 // W2 (256 x 256, row-major: output n, input k) -> the fused kernel's shared-memory order: chunk t = k
 // [32 t, +32) of all 256 rows, within a chunk k-group b (8 wide) then row n then element: W2p[t][b][n][e] (the
 // canonical K-major layout of a 256 x 32 B operand, k-groups 4096 B apart, 8-row groups 128 B apart).
@@ -1150,9 +1138,9 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
   // weights, once: W2 by bulk copies (thread 0), W1 (256 x 16, K-major, SBO 256) and W3t (256 k x 16 n,
   // MN-major: LBO 256 between k-groups, SBO 128) and the biases by cp.async
   if (tid == 0) {
-    mbar_expect_tx(&bar_w, kW2Bytes);
+    umma::expect_tx(&bar_w, kW2Bytes);
     for (int t = 0; t < kNH / 32; ++t)
-      bulk_load(w2s + (uint32_t)t * kChunkBytes, p.W2p + (size_t)t * (kChunkBytes / 2), kChunkBytes, &bar_w);
+      umma::bulk_g2s(w2s + (uint32_t)t * kChunkBytes, p.W2p + (size_t)t * (kChunkBytes / 2), kChunkBytes, &bar_w);
   }
 #pragma unroll
   for (int i = 0; i < 2; ++i) {

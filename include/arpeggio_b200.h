@@ -78,7 +78,10 @@ int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const int32_t* T, c
  * 64-bit seed.  Outputs as arp_anneal_chord_dd (tests = one per step); best spins and best energy changes equal
  * the engine's, which starts its best at 2^35 - 1 (an anneal none of whose steps ends below that returns its
  * start spins here, where the engine keeps whatever its best-spin register last held).  No start argument: the
- * engine's start comes from its generators. */
+ * engine's start comes from its generators.  The engine runs only D that are a multiple of its lane-group width
+ * (engine_model.cpp:145-183; width max(1, D / 32) as this project binds it: any D < 64, even D < 96, multiples of
+ * 3 below 128, and 128); equality with the engine holds there.  Other D (up to 128) extend the same rule to
+ * coordinates the engine cannot group and are pinned by the oracle's restatement only. */
 int arp_anneal_chord_engine(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L, int q,
                             int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
                             int8_t* out_s, int64_t* out_de, int64_t* out_st, int32_t* status, void* stream);
@@ -97,7 +100,10 @@ int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, const float* 
  * arpeggio/mimo/chordfx.py:189-208 (Kernel.chord): N % 32 == 0, (N / P) % 32 == 0, N <= 256;
  * mode 0 ('chains'): out_e (B, R), out_s (B, R, N); mode 1 ('best'): out_e (B), out_s (B, N).
  * out_e is 2 E0 (int64).  stats (4 counters: flips, energy evaluations, Philox blocks, steps x anneals)
- * may be NULL.  warps = anneals per block in flight (the reference's `warps`, <= 8). */
+ * may be NULL; their totals equal the reference kernel's.  warps = anneals per block in flight: 1..16 as given
+ * (8 at most for N = 256 with P = 1), <= 0 picks the width with the most resident warps per SM (16 at N = 256,
+ * where the staged J leaves one block per SM).  The outputs do not depend on it.  J 16-byte aligned is staged
+ * by bulk copies, otherwise by plain loads. */
 int arp_anneal_chord(const int16_t* J, const int32_t* h, const int32_t* h0, const int32_t* Tq, const int32_t* Cq,
                      int q, int S, int P, int R, int N, int B, uint32_t k0, uint32_t k1, uint32_t inst0, int mode,
                      int warps, int64_t* out_e, int8_t* out_s, unsigned long long* stats, int32_t* status,
@@ -312,7 +318,9 @@ int arp_anneal_first_accept_warm_sampled(const int32_t* Gt, const int32_t* h, co
  * holds until the process exits.  A batch whose arp_detect_dd_workspace() exceeds 32 MiB is refused with
  * ARP_ERR_WORKSPACE before any launch.  All calls on a device share the array (it keeps the last call's
  * contents, and nothing in it needs to start at zero); calls whose work overlaps on the GPU race on it.  The
- * first call on each device looks up the array's address and should come before any stream capture.
+ * first call on each device looks up the array's address and should come before any stream capture.  The
+ * address is kept for the life of the process: after a cudaDeviceReset (or any reset of the device's primary
+ * context) it no longer names the array, so do not use this entry point on a device across such a reset.
  * No counterpart in the reference: it exists only for callers that cannot allocate. */
 int arp_detect_dd_static(const float* H, const float* y, const float* sigma2, int B, int NR2, int D, int M,
                          int policy, int precision, int P, int R, const void* T, const void* c, int L, double q,

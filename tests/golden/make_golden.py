@@ -2,7 +2,7 @@
 """Generates the golden fixtures in this folder by importing the reference (skethz/Arpeggio) itself.
 
 Run in a container that has the reference tree (read-only; no bytecode is written there):
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py "$ARPEGGIO_REFERENCE"
 
 Fixtures (all small, numpy .npz):
   golden_philox.npz   Random123 KATs (arpeggio/mimo/chordfx.py:53-56) and 256 further counter/key
@@ -17,11 +17,11 @@ Fixtures (all small, numpy .npz):
                       integers, spins_to_levels_delta, dist, select and list_llr (mimo.py:434-462, clip 1e4,
                       as softlib.detect_llr) on fixed spin sets.
   golden_a513_b0.npz  batch 0 of the recorded B200 runs data/results/a513_fixed/{x16,x32}: per-use bit
-                      errors, anneals per use, per-K [flips, tests, anneals] (`... /root/reference a513`).
+                      errors, anneals per use, per-K [flips, tests, anneals] (`... "$ARPEGGIO_REFERENCE" a513`).
   golden_a513_points.npz  every recorded batch's per-use bit errors at the three recorded points
-                      (x16 20 dB, x32 22 dB, x64 22 dB) for the BER-inside-CI gate (`... /root/reference a513_points`).
+                      (x16 20 dB, x32 22 dB, x64 22 dB) for the BER-inside-CI gate (`... "$ARPEGGIO_REFERENCE" a513_points`).
   golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
-                      (sim/a56an.py:74-108) on seeded per-use error vectors (`... /root/reference stats`).
+                      (sim/a56an.py:74-108) on seeded per-use error vectors (`... "$ARPEGGIO_REFERENCE" stats`).
 """
 import math
 import os
@@ -29,7 +29,7 @@ import random
 import sys
 
 sys.dont_write_bytecode = True
-REF = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+REF = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else os.environ['ARPEGGIO_REFERENCE'])
 OUT = os.path.dirname(os.path.abspath(__file__))
 for sub in ('arpeggio/mimo', 'arpeggio/sim', 'arpeggio/sim/x3model', 'arpeggio/sim/local_code_a513'):
     sys.path.insert(0, os.path.join(REF, sub))

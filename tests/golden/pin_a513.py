@@ -9,7 +9,7 @@ produced by arpeggio_fx.cu on a B200; equality pins the oracle to the reference 
 tens of thousands of real sub-problems.  Host float effects (CPU BLAS last bits, see
 arpeggio/sim/arpx.py:40-42) can move a few uses, so differing uses are reported, not hidden.
 
-    python tests/golden/pin_a513.py /root/reference x16 [x32 x64]
+    python tests/golden/pin_a513.py "$ARPEGGIO_REFERENCE" x16 [x32 x64]
 Writes tests/golden/pin_a513.json.
 """
 import json

@@ -89,6 +89,42 @@ def test_chord_full_bit_exact_vs_chord_fx(golden, name, mode):
     assert int(stats[3].item()) == S * R * F["h"].shape[0]
 
 
+@pytest.mark.parametrize('N,P,R,S,kappa,offset,warps', [
+    (256, 2, 64, 64, 0.3, 0, 0),    # 16 warps per block (one block per SM)
+    (256, 1, 24, 40, 0.3, 0, 0),    # one phase: the Onsager sign of the previous step's flips
+    (256, 8, 16, 48, 0.0, 1, 0),    # eight phases; J one element off a 16-byte boundary (plain-load staging)
+    (192, 3, 20, 30, 0.3, 0, 5),    # a given width that is not a power of two
+    (64, 2, 40, 100, 0.3, 0, 0),    # a partial last quad of sweeps
+])
+def test_chord_full_vs_oracle_wide(N, P, R, S, kappa, offset, warps):
+    """arp_anneal_chord on dDI problems expanded to a full int16 J (chord_ref.expand) against the oracle's chord_fx
+    restatement: spins, energies and counters bit for bit in both modes, at block widths and phase counts the golden
+    cases do not reach."""
+    from arpeggio_b200 import chordfx
+    B, D = 12, N // 2
+    G, h, _, _ = _random_dd(B, D, 1, 12.0, 300 + N + P)
+    J, hN = O.expand(G, h, 1)  # the phases P need not be the dDI copy count: the kernel takes any J
+    h0 = (hN // 3).astype(np.int32)
+    T, c, q = O.chord_schedule(S, 0.3, 0.05, 0.4, kappa=kappa)
+    seed, inst0 = 0x1234ABCD5678 + N, 0xFFFFFFF0
+    Jd = torch.zeros(B * N * N + offset, dtype=torch.int16, device='cuda')
+    Jd[offset:] = torch.from_numpy(J.reshape(-1))
+    F = dict(J=Jd[offset:].view(B, N, N), h=torch.from_numpy(hN).cuda(), h0=torch.from_numpy(h0).cuda(),
+             T=torch.from_numpy(T).cuda(), c=torch.from_numpy(c).cuda(), q=q, S=S)
+    if offset:
+        assert F['J'].data_ptr() % 16 != 0
+    k = chordfx.Kernel()
+    for mode in ('chains', 'best'):
+        stats = torch.zeros(4, dtype=torch.int64, device='cuda')
+        s, e = k.chord(F, R, seed, P=P, inst0=inst0, mode=mode, warps=warps, stats=stats)
+        torch.cuda.synchronize()
+        assert int(k.last_status.item()) == 0
+        os_, oe = O.chord_fx(J, hN, h0, T, c, q, S, P, R, seed, inst0=inst0, mode=mode, nthreads=NTH)
+        assert np.array_equal(s.cpu().numpy(), os_), mode
+        assert np.array_equal(e.cpu().numpy(), oe), mode
+        assert int(stats[3].item()) == S * R * B
+
+
 def _random_dd(B, D, K, snr, seed):
     """Realistic compressed integer dDI problems from this package's draws and the oracle's float64 mapping."""
     from arpeggio_b200 import channel

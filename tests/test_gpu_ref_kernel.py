@@ -179,6 +179,7 @@ def test_reference_chord_kernel_timing(golden):
         assert torch.equal(a, b)
     print('\nreference chord_m%d: %.3f ms, this project: %.3f ms for 2048 problems x %d anneals, N = %d (%.2fx)'
           % (F['h'].shape[1] // 32, t_ref, t_ours, R, F['h'].shape[1], t_ref / t_ours))
+    assert t_ours < t_ref
 
 
 @pytest.mark.parametrize('nt,K,steps,kappa', [(32, 1, 256, 0.0), (16, 1, 256, 0.3), (64, 2, 64, 0.3)])

@@ -708,7 +708,49 @@ def run_ours(args):
                                 'sample': '%d channel uses of the same workload (same SNR mix, 32 anneals), full CPU '
                                           'chain (float64 MMSE + mapping, oracle first-accept anneal on %d threads, '
                                           'select), %.1f s' % (n, nthreads, dt)}
+    line['summary'] = summary(line)
     return line
+
+
+def _r(x, n=3):
+    return None if x is None else float('%.*g' % (n, x))
+
+
+def summary(line):
+    """The metric's other halves in a few hundred bytes, as the line's last key: warm vs plain (speed-up and the
+    paired BER-ratio intervals per SNR point), frame latency p50/p99, serving p99 per class at 1e5 frames/s."""
+    out = {'det_per_s': _r(line['value'], 4), 'e2e_det_per_s': _r(line['e2e']['value'], 4),
+           'roofline_frac': _r(line['roofline']['frac']),
+           'cpu_det_per_s': _r((line.get('cpu_baseline') or {}).get('value'), 4)}
+    lat = line.get('latency') or {}
+    out['frame_us_plain_p50_p99'] = [_r(lat.get('p50_us')), _r(lat.get('p99_us'))]
+    wv = line.get('warm_vs_plain') or {}
+    for wl in ('x32', 'x64'):
+        blk = wv.get(wl)
+        if not blk:
+            continue
+        o = {}
+        for name, v in blk.items():
+            if not isinstance(v, dict) or 'value' not in v:
+                continue
+            e = {'det_per_s': _r(v['value'], 4)}
+            if 'speedup_vs_plain' in v:
+                e['x_plain'] = _r(v['speedup_vs_plain'])
+            if 'ber_ratio_vs_plain' in v and name != 'warm_argmax':  # the ablation: speed-up only
+                e['ber_ratio_ci'] = {k.replace(' ', ''): [_r(c) for c in ci] for k, ci in v['ber_ratio_vs_plain'].items()}
+            if 'frame_latency' in v:
+                e['frame_us_p50_p99'] = [_r(v['frame_latency']['p50_us']), _r(v['frame_latency']['p99_us'])]
+            o[name] = e
+        out['warm_vs_plain_' + wl] = o
+    sv = line.get('serving') or {}
+    r5 = (sv.get('rates') or {}).get('1e+05 frames/s')
+    if r5:
+        out['serving_1e5'] = {'frames_per_s': _r(r5['achieved_frames_per_s']),
+                              'p99_ms': {k: _r(v['p99_us'] / 1e3) for k, v in r5['per_class'].items()}}
+    mx = line.get('mixed') or {}
+    if mx.get('value'):
+        out['mixed_det_per_s'] = _r(mx['value'])
+    return out
 
 
 def run_reference(args):

@@ -2,8 +2,13 @@
 //
 // map (one block per channel use; mimo.py:98-109 mmse, :176-182 _mu, :86-88 quantize_levels,
 // :506-523 ising_delta_at, chordfx.py:60-76 to_fixed, chord_ref.py:47-59 compress):
-//   Q = H^T H and g = H^T y, streamed over 32-row chunks of H (every Q_ij and Q_ji is the same ordered
-//   sum, so Q is exactly symmetric, as the symmetrised J of to_fixed);
+//   Q = H^T H on the tensor cores, exactly: per use H is scaled by a power of two so that its largest entry
+//   is just below 2^30, rounded to integers x and split into four signed 8-bit digits (x = sum_a 2^(8a) d_a);
+//   tcgen05.mma kind::i8 forms the digit products d_a^T d_b with exact s32 accumulation in TMEM, grouped by
+//   weight a + b (classes 6, 5, 4, 3; the dropped lower classes move an entry by ~2^-26 of the largest |Q|, well
+//   below the FP32 rounding of the reference's own product), and the epilogue
+//   sums the classes exactly in double and rounds once to float.  Q is exactly symmetric (an exact integer
+//   sum), as the symmetrised J of to_fixed.  g = H^T y as an ordered fma chain per coordinate;
 //   A = Q + sigma2 I inverted in shared memory (Gauss-Jordan; A is SPD), z = A^-1 g, mu = diag(A^-1 Q),
 //   x_q = nearest level of z / mu (first level on ties);
 //   h = 2 (g - Q x_q) = 2 H^T (y - H x_q);  scale = max(|h|_inf, |Q|_inf) clamped at 1e-12;
@@ -16,6 +21,7 @@
 
 #include "arp_common.cuh"
 #include "arp_internal.h"
+#include "umma.cuh"
 
 namespace arp {
 
@@ -99,35 +105,96 @@ __device__ __forceinline__ float row_dot(const float (&x)[TB], const float (&y)[
 // columns of H are zero and the padded diagonal of A is 1, so the inverse's D x D block is unchanged.  (A 32 x 32
 // grid of 2 x 2 tiles was measured for one frame and is slower: the 64 elimination steps are latency-bound and
 // a 1024-thread barrier per step costs more than the smaller tiles save.)
+// Gram on the tensor cores: digit planes of one row chunk (CH rows of H) in the canonical K-major no-swizzle
+// layout of 8-bit operands -- core matrices of 8 rows (coordinates) x 16 bytes (rows of H), LBO = 128 B between
+// neighbours along K, SBO = (CH / 16) 128 B between 8-coordinate groups; one MMA consumes K = 32 (two core
+// matrices).  MP = the MMA's M: 64 for Dp <= 64 (rows Dp .. 63 zero), else 128.
+template <int Dp>
+__host__ __device__ constexpr int kMmaM() { return Dp <= 64 ? 64 : 128; }
+template <int Dp>
+__host__ __device__ constexpr int kPlaneBytes() { return kMmaM<Dp>() * kChunkRows<Dp>(); }
+template <int Dp>
+__host__ __device__ constexpr int kTmemCols() {  // four class accumulators of Dp columns, a power of two >= 32
+  return 4 * Dp <= 32 ? 32 : (4 * Dp <= 64 ? 64 : (4 * Dp <= 128 ? 128 : (4 * Dp <= 256 ? 256 : 512)));
+}
+
+// The digit pairs (a, b) of each class a + b = 6, 5, 4, 3, in issue order.
+__constant__ int8_t kPairA[10] = {3, 3, 2, 3, 1, 2, 3, 0, 2, 1};
+__constant__ int8_t kPairB[10] = {3, 2, 3, 1, 3, 2, 0, 3, 1, 2};
+__constant__ int8_t kPairC[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};  // accumulator: class 6 - c
+
+// Signed base-256 digits of x (|x| < 2^30): x = d0 + 2^8 d1 + 2^16 d2 + 2^24 d3, each in [-128, 127].
+__device__ __forceinline__ void digits4(int32_t x, int32_t (&d)[4]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int32_t lo = (int32_t)(int8_t)(x & 0xFF);
+    d[a] = lo;
+    x = (x - lo) >> 8;
+  }
+  d[3] = x;
+}
+
 template <int TB, int GS>
 __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
   constexpr int Dp = GS * TB, QP = Dp + 4, NT = GS * GS;
-  extern __shared__ __align__(16) float sm[];
-  float* Hc = sm;                            // kChunkRows x Dp
-  float* Qs = Hc + kChunkRows<Dp>() * Dp;    // Dp x QP
-  float* rk = Qs + Dp * QP;       // 2 x Dp (double-buffered row k)
+  constexpr int CH = kChunkRows<Dp>(), MP = kMmaM<Dp>(), KG = CH / 16, PB = kPlaneBytes<Dp>();
+  constexpr uint32_t NCOL = kTmemCols<Dp>();
+  extern __shared__ __align__(128) float smap[];
+  uint8_t* planes = reinterpret_cast<uint8_t*>(smap);  // 4 digit planes, PB bytes each (aliases Qs below)
+  float* Hc = smap + (PB * 4 > Dp * QP * 4 ? PB : Dp * QP);  // CH x Dp
+  float* Qs = smap;                            // Dp x QP, written once the Gram's MMAs have completed
+  float* rk = Hc + CH * Dp;       // 2 x Dp (double-buffered row k)
   float* ck = rk + 2 * Dp;        // 2 x Dp (double-buffered column k)
   float* gv = ck + 2 * Dp;        // Dp
   float* xv = gv + Dp;            // Dp
   float* red = xv + Dp;           // NT / 32
-  float* yc = red + NT / 32;      // kChunkRows: the chunk's rows of y
+  float* yc = red + NT / 32;      // CH: the chunk's rows of y
+  __shared__ __align__(8) uint64_t mma_bar;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort, s_exp;
   const int D = a.D, NR2 = a.NR2, b = blockIdx.x;
-  const int tid = threadIdx.x, tx = tid % GS, ty = tid / GS, lane = tid & 31;
+  const int tid = threadIdx.x, tx = tid % GS, ty = tid / GS, lane = tid & 31, warp = tid >> 5;
+  // TMEM before the trigger: a dependent kernel that holds TMEM while it waits for this grid can then never
+  // take the columns a block of this grid still needs
+  if (tid == 0) {
+    umma::mbar_init(&mma_bar, 1);
+    umma::fence_mbar_init();
+    s_abort = 0;
+  }
+  if (warp == 0) umma::tmem_alloc(&s_tmem, NCOL);
+  umma::tc_before_sync();
+  __syncthreads();
+  umma::tc_after_sync();
+  const uint32_t tmem = s_tmem;
   pdl_trigger();  // the chain's next kernel may launch and set up; it waits for this grid before reading
   const int u = a.idx ? a.idx[b] : b;
   const float* Hb = a.H + (size_t)u * NR2 * D;
   const float* yb = a.y + (size_t)u * NR2;
-  float A[TB][TB];
+  // ---- the use's power-of-two scale: largest |H| just below 2^30 after scaling
+  {
+    float mx = 0.0f;
+    for (int x = tid; x < NR2 * D; x += NT) mx = fmaxf(mx, fabsf(Hb[x]));
 #pragma unroll
-  for (int i = 0; i < TB; ++i)
-#pragma unroll
-    for (int j = 0; j < TB; ++j) A[i][j] = 0.0f;
-  float gacc = 0.0f;
-  // ---- Q = H^T H and g = H^T y over row chunks (every Q_ij, Q_ji is the same ordered fma chain)
-  constexpr int CH = kChunkRows<Dp>();
-  for (int r0 = 0; r0 < NR2; r0 += CH) {
-    const int nr = min(CH, NR2 - r0);
+    for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(ARP_FULL, mx, o));
+    if (lane == 0) red[warp] = mx;
     __syncthreads();
+    if (tid == 0) {
+      float m = 0.0f;
+      for (int w = 0; w < NT / 32; ++w) m = fmaxf(m, red[w]);
+      int e = 0;
+      if (m > 0.0f) frexpf(m, &e);  // m in [2^(e-1), 2^e)
+      s_exp = m > 0.0f ? 30 - e : 0;
+    }
+  }
+  float gacc = 0.0f;
+  constexpr uint32_t IDESC = umma::idesc_s8(MP, Dp);
+  const uint32_t pbase = umma::su32(planes);
+  int nchunk = 0;
+  for (int r0 = 0; r0 < NR2; r0 += CH, ++nchunk) {
+    const int nr = min(CH, NR2 - r0);
+    __syncthreads();  // the previous chunk's digits were read by MMAs that have completed (waited below)
+    if (s_abort) break;
+    const int sx = s_exp;
     for (int x = tid; x < nr; x += NT) yc[x] = yb[r0 + x];
     if (D == Dp && (D & 3) == 0) {
       const float4* src = reinterpret_cast<const float4*>(Hb + (size_t)r0 * D);
@@ -140,18 +207,88 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
       }
     }
     __syncthreads();
-    for (int r = 0; r < nr; ++r) {
-      float ai[TB], bj[TB];
-      lds_vec<TB>(Hc + r * Dp + ty * TB, ai);
-      lds_vec<TB>(Hc + r * Dp + tx * TB, bj);
-#pragma unroll
-      for (int i = 0; i < TB; ++i)
-#pragma unroll
-        for (int j = 0; j < TB; ++j) A[i][j] = __fmaf_rn(ai[i], bj[j], A[i][j]);
-    }
     if (tid < Dp)
       for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * Dp + tid], yc[r], gacc);
+    // digit planes: a warp writes one core matrix (8 coordinates x 16 rows) at a time, lane = coordinate m % 8
+    // + 8 (row quad), one 32-bit word of four rows per plane (conflict-free); rows >= nr and coordinates >= Dp
+    // are zero
+    const int ksteps = (nr + 31) >> 5;
+    for (int cm = warp; cm < (MP / 8) * KG; cm += NT / 32) {
+      const int mg = cm / KG, kg = cm - mg * KG;
+      const int m = mg * 8 + (lane & 7), k0 = kg * 16 + (lane >> 3) * 4;
+      uint32_t wd[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int k = k0 + i;
+        const float v = (m < Dp && k < nr) ? Hc[k * Dp + m] : 0.0f;
+        int32_t d[4];
+        digits4(__float2int_rn(ldexpf(v, sx)), d);
+#pragma unroll
+        for (int p = 0; p < 4; ++p) wd[p] |= ((uint32_t)d[p] & 0xFFu) << (8 * i);
+      }
+      const uint32_t off = (uint32_t)(mg * KG * 128 + kg * 128 + (lane & 7) * 16 + (lane >> 3) * 4);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) *reinterpret_cast<uint32_t*>(planes + p * PB + off) = wd[p];
+    }
+    umma::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma::tc_after_sync();
+      for (int ks = 0; ks < ksteps; ++ks) {
+#pragma unroll
+        for (int q = 0; q < 10; ++q) {
+          const uint64_t ad = umma::sdesc(pbase + kPairA[q] * PB + ks * 256, 128, KG * 128);
+          const uint64_t bd = umma::sdesc(pbase + kPairB[q] * PB + ks * 256, 128, KG * 128);
+          // the first product of each class in the first chunk starts its accumulator
+          const bool first = nchunk == 0 && ks == 0 && (q == 0 || q == 1 || q == 3 || q == 6);
+          umma::mma_s8(tmem + (uint32_t)(kPairC[q] * Dp), ad, bd, IDESC, first ? 0u : 1u);
+        }
+      }
+      umma::commit(&mma_bar);
+    }
+    if (!umma::mbar_wait(&mma_bar, (uint32_t)(nchunk & 1))) s_abort = 1;
   }
+  __syncthreads();
+  umma::tc_after_sync();
+  if (s_abort) {  // an MMA never completed: report, wait once more for it, free TMEM, leave
+    if (tid == 0) {
+      set_status(a.status, ARP_ERR_TIMEOUT);
+      umma::mbar_wait(&mma_bar, (uint32_t)((nchunk - 1) & 1));
+    }
+    __syncthreads();
+    if (warp == 0) umma::tmem_free(tmem, NCOL);
+    return;
+  }
+  // ---- epilogue: each row of Q from the four class accumulators, summed exactly in double (every class is an
+  //      exact s32 and the sum spans < 53 bits), scaled by 2^-2s and rounded once to float.  TMEM lane of row m:
+  //      m (M = 128), or m % 16 + 32 (m / 16) (M = 64); warp w reads lanes 32 w .. 32 w + 31.
+  if (warp < 4) {
+    const int m = MP == 128 ? warp * 32 + lane : warp * 16 + lane;
+    const bool valid = (MP == 128 || lane < 16) && m < Dp;
+    const int sx2 = -2 * s_exp;
+#pragma unroll 1
+    for (int c0 = 0; c0 < Dp; c0 += 8) {
+      uint32_t v6[8], v5[8], v4[8], v3[8];
+      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      umma::tmem_ld8_nowait(ta, v6);
+      umma::tmem_ld8_nowait(ta + Dp, v5);
+      umma::tmem_ld8_nowait(ta + 2 * Dp, v4);
+      umma::tmem_ld8_nowait(ta + 3 * Dp, v3);
+      umma::tmem_wait_ld();
+      if (valid) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const double q = ldexp((double)(int32_t)v6[j], 48) + ldexp((double)(int32_t)v5[j], 40) +
+                           ldexp((double)(int32_t)v4[j], 32) + ldexp((double)(int32_t)v3[j], 24);
+          Qs[m * QP + c0 + j] = __double2float_rn(ldexp(q, sx2));
+        }
+      }
+    }
+  }
+  umma::tc_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tmem, NCOL);
+  float A[TB][TB];
   float qmax = 0.0f;
   const float s2 = a.xg ? 0.0f : a.sigma2[b];  // only the MMSE solve reads sigma2 (null for a given guess)
 #pragma unroll
@@ -159,7 +296,7 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
 #pragma unroll
     for (int j = 0; j < TB; ++j) {
       const int gi = ty * TB + i, gj = tx * TB + j;
-      Qs[gi * QP + gj] = A[i][j];
+      A[i][j] = Qs[gi * QP + gj];
       qmax = fmaxf(qmax, fabsf(A[i][j]));
       if (gi == gj) A[i][j] = gi < D ? __fadd_rn(A[i][j], s2) : 1.0f;
     }
@@ -353,8 +490,9 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
 
 template <int TB, int GS>
 static size_t map_smem() {
-  constexpr int Dp = GS * TB;
-  return sizeof(float) * ((size_t)kChunkRows<Dp>() * (Dp + 1) + (size_t)Dp * (Dp + 4) + 6 * (size_t)Dp + GS * GS / 32);
+  constexpr int Dp = GS * TB, PB = kPlaneBytes<Dp>();
+  constexpr size_t front = PB * 4 > Dp * (Dp + 4) * 4 ? (size_t)PB : (size_t)Dp * (Dp + 4);  // planes | Qs, floats
+  return sizeof(float) * (front + (size_t)kChunkRows<Dp>() * (Dp + 1) + 6 * (size_t)Dp + GS * GS / 32);
 }
 
 template <int TB, int GS = 16>

@@ -261,6 +261,34 @@ def ising_delta_compressed(H, y, xg):
     return Q / scale[:, None, None], h / scale[:, None], scale
 
 
+def gram_digits(H):
+    """Q = H^T H as this project's map forms it on the tensor cores (no reference counterpart: the reference forms
+    it in FP32 with torch matmul, mimo.py:100-104): per use H scaled by 2^s (largest |H| just below 2^30), rounded
+    to integers x, split into signed base-256 digits x = sum_a 2^(8a) d_a; the products d_a^T d_b of weight
+    a + b >= 3 summed exactly (integers, then a float64 sum that is exact below 2^53 steps of 2^24), scaled by
+    2^-2s and rounded once to float32.  Returns float32 Q (B, D, D)."""
+    H = np.asarray(H, dtype=np.float32)
+    B, NR2, D = H.shape
+    out = np.zeros((B, D, D), dtype=np.float32)
+    pairs = [(a, b) for a in range(4) for b in range(4) if a + b >= 3]
+    for u in range(B):
+        m = float(np.abs(H[u]).max())
+        s = 30 - np.frexp(m)[1] if m > 0 else 0
+        x = np.rint(np.ldexp(H[u].astype(np.float64), s)).astype(np.int64)
+        d = []
+        for _ in range(3):
+            lo = ((x & 0xFF) ^ 0x80) - 0x80
+            d.append(lo)
+            x = (x - lo) >> 8
+        d.append(x)
+        cls = {w: np.zeros((D, D), dtype=np.int64) for w in (3, 4, 5, 6)}
+        for a, b in pairs:
+            cls[a + b] += d[a].T @ d[b]
+        q = sum(np.ldexp(cls[w].astype(np.float64), 8 * w) for w in (6, 5, 4, 3))
+        out[u] = np.ldexp(q, -2 * s).astype(np.float32)
+    return out
+
+
 def geom(t0, t1, S):
     """mimo.geom (mimo.py:199-201): float64 schedule rounded once to float32."""
     k = np.arange(S, dtype=np.float64)

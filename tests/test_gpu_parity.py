@@ -245,6 +245,39 @@ def test_map_vs_reference(golden):
         assert (Gg == Gr).mean() >= 0.999 and (hg == hr).mean() >= 0.99, tag
 
 
+@pytest.mark.parametrize('nt,nr,M', [(8, 8, 16), (16, 16, 16), (32, 32, 16), (24, 36, 64), (48, 72, 4), (64, 64, 16),
+                                     (64, 128, 16)])
+def test_map_gram_is_exact(nt, nr, M):
+    """The Gram formed on the tensor cores (8-bit digit products, exact integer accumulation): the float problem's
+    G = Q / scale equals the oracle's restatement of the digit scheme (oracle.gram_digits) bit for bit, is exactly
+    symmetric, and stays within two float32 roundings plus 2^-24 of the problem's largest |G| of the float64 Gram,
+    at every map width and row count."""
+    from arpeggio_b200 import _lib, channel
+    B = 64
+    b = channel.draw(900 + nt, 14.0, 0, B, nt, M, nr=nr)
+    H = b['H'].cuda().contiguous()
+    y = b['y'].cuda().contiguous()
+    _, NR2, D = H.shape
+    s2 = torch.full((B,), 0.05, dtype=torch.float32, device='cuda')
+    G = torch.empty(B, D, D, dtype=torch.float32, device='cuda')
+    h = torch.empty(B, D, dtype=torch.float32, device='cuda')
+    xq = torch.empty(B, D, dtype=torch.int8, device='cuda')
+    sc = torch.empty(B, dtype=torch.float32, device='cuda')
+    L = _lib.lib()
+    _lib.check(L.arp_map_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(s2), B, NR2, D, M, 0, _lib.ptr(G), _lib.ptr(h),
+                            _lib.ptr(xq), _lib.ptr(sc), None, _lib.stream_ptr()), 'map')
+    torch.cuda.synchronize()
+    Gg, scg = G.cpu().numpy(), sc.cpu().numpy()
+    assert np.array_equal(Gg, np.swapaxes(Gg, 1, 2))
+    Qo = O.gram_digits(b['H'].numpy())
+    assert np.array_equal(Gg, (Qo / scg[:, None, None]).astype(np.float32))
+    Hd = b['H'].numpy().astype(np.float64)
+    ref = np.einsum('bki,bkj->bij', Hd, Hd) / scg[:, None, None]
+    ulp = np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
+    tol = ulp + 2.0 ** -24 * np.abs(ref).reshape(B, -1).max(-1)[:, None, None]  # two roundings + dropped digits
+    assert (np.abs(Gg.astype(np.float64) - ref) <= tol).all()
+
+
 def test_readout_vs_reference(golden):
     """arp_readout_dd on fixed spin sets == mimo.spins_to_levels_delta + select + levels_to_bits."""
     from arpeggio_b200 import _lib

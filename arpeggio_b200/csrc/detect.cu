@@ -154,26 +154,18 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
   __shared__ int s_abort, s_exp;
   const int D = a.D, NR2 = a.NR2, b = blockIdx.x;
   const int tid = threadIdx.x, tx = tid % GS, ty = tid / GS, lane = tid & 31, warp = tid >> 5;
-  // TMEM before the trigger: a dependent kernel that holds TMEM while it waits for this grid can then never
-  // take the columns a block of this grid still needs
   if (tid == 0) {
     umma::mbar_init(&mma_bar, 1);
     umma::fence_mbar_init();
     s_abort = 0;
   }
-  if (warp == 0) umma::tmem_alloc(&s_tmem, NCOL);
-  umma::tc_before_sync();
-  __syncthreads();
-  umma::tc_after_sync();
-  const uint32_t tmem = s_tmem;
-  pdl_trigger();  // the chain's next kernel may launch and set up; it waits for this grid before reading
   const int u = a.idx ? a.idx[b] : b;
   const float* Hb = a.H + (size_t)u * NR2 * D;
   const float* yb = a.y + (size_t)u * NR2;
-  // ---- the use's power-of-two scale: largest |H| just below 2^30 after scaling
-  {
-    float mx = 0.0f;
-    for (int x = tid; x < NR2 * D; x += NT) mx = fmaxf(mx, fabsf(Hb[x]));
+  // ---- the use's power-of-two scale (largest |H| just below 2^30 after scaling): from the staged rows when they
+  //      fit one chunk, else from a pass over H first
+  const bool one_chunk = NR2 <= CH;
+  auto set_scale = [&](float mx) {  // mx: this thread's part; every thread leaves with s_exp set
 #pragma unroll
     for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(ARP_FULL, mx, o));
     if (lane == 0) red[warp] = mx;
@@ -185,6 +177,12 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
       if (m > 0.0f) frexpf(m, &e);  // m in [2^(e-1), 2^e)
       s_exp = m > 0.0f ? 30 - e : 0;
     }
+    __syncthreads();
+  };
+  if (!one_chunk) {
+    float mx = 0.0f;
+    for (int x = tid; x < NR2 * D; x += NT) mx = fmaxf(mx, fabsf(Hb[x]));
+    set_scale(mx);
   }
   float gacc = 0.0f;
   constexpr uint32_t IDESC = umma::idesc_s8(MP, Dp);
@@ -194,46 +192,69 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
     const int nr = min(CH, NR2 - r0);
     __syncthreads();  // the previous chunk's digits were read by MMAs that have completed (waited below)
     if (s_abort) break;
-    const int sx = s_exp;
     for (int x = tid; x < nr; x += NT) yc[x] = yb[r0 + x];
+    float mx = 0.0f;
     if (D == Dp && (D & 3) == 0) {
       const float4* src = reinterpret_cast<const float4*>(Hb + (size_t)r0 * D);
       float4* dst = reinterpret_cast<float4*>(Hc);
-      for (int x = tid; x < nr * Dp / 4; x += NT) dst[x] = src[x];
+      for (int x = tid; x < nr * Dp / 4; x += NT) {
+        const float4 v = src[x];
+        dst[x] = v;
+        mx = fmaxf(fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w)));
+      }
     } else {
       for (int x = tid; x < nr * Dp; x += NT) {
         const int r = x / Dp, j = x - r * Dp;
-        Hc[x] = j < D ? Hb[(size_t)(r0 + r) * D + j] : 0.0f;
+        const float v = j < D ? Hb[(size_t)(r0 + r) * D + j] : 0.0f;
+        Hc[x] = v;
+        mx = fmaxf(mx, fabsf(v));
       }
     }
-    __syncthreads();
+    if (one_chunk)
+      set_scale(mx);  // its barriers also publish the staged rows
+    else
+      __syncthreads();
+    const int sx = s_exp;
     if (tid < Dp)
       for (int r = 0; r < nr; ++r) gacc = __fmaf_rn(Hc[r * Dp + tid], yc[r], gacc);
     // digit planes: a warp writes one core matrix (8 coordinates x 16 rows) at a time, lane = coordinate m % 8
     // + 8 (row quad), one 32-bit word of four rows per plane (conflict-free); rows >= nr and coordinates >= Dp
-    // are zero
+    // are zero.  The signed digits of x (|x| < 2^30) are the bytes of (x + 0x808080) ^ 0x808080: adding 128 at each
+    // of the three low digit positions makes every low byte u_a = d_a + 128 with the borrow carried up, and the
+    // XOR turns u_a into d_a's two's-complement byte; the top byte is d3.  A 4 x 4 byte transpose (eight byte
+    // permutes) turns four rows' digit words into one word per plane.
     const int ksteps = (nr + 31) >> 5;
+    const bool fast_scale = sx >= -126 && sx <= 127;
+    const float fs = fast_scale ? __int_as_float((sx + 127) << 23) : 1.0f;
     for (int cm = warp; cm < (MP / 8) * KG; cm += NT / 32) {
       const int mg = cm / KG, kg = cm - mg * KG;
       const int m = mg * 8 + (lane & 7), k0 = kg * 16 + (lane >> 3) * 4;
-      uint32_t wd[4] = {0u, 0u, 0u, 0u};
+      uint32_t z[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int k = k0 + i;
         const float v = (m < Dp && k < nr) ? Hc[k * Dp + m] : 0.0f;
-        int32_t d[4];
-        digits4(__float2int_rn(ldexpf(v, sx)), d);
-#pragma unroll
-        for (int p = 0; p < 4; ++p) wd[p] |= ((uint32_t)d[p] & 0xFFu) << (8 * i);
+        const int32_t x = __float2int_rn(fast_scale ? __fmul_rn(v, fs) : ldexpf(v, sx));
+        z[i] = ((uint32_t)x + 0x808080u) ^ 0x808080u;
       }
+      const uint32_t t0 = __byte_perm(z[0], z[1], 0x5140), t1 = __byte_perm(z[2], z[3], 0x5140);
+      const uint32_t t2 = __byte_perm(z[0], z[1], 0x7362), t3 = __byte_perm(z[2], z[3], 0x7362);
+      const uint32_t wd[4] = {__byte_perm(t0, t1, 0x5410), __byte_perm(t0, t1, 0x7632), __byte_perm(t2, t3, 0x5410),
+                              __byte_perm(t2, t3, 0x7632)};
       const uint32_t off = (uint32_t)(mg * KG * 128 + kg * 128 + (lane & 7) * 16 + (lane >> 3) * 4);
 #pragma unroll
       for (int p = 0; p < 4; ++p) *reinterpret_cast<uint32_t*>(planes + p * PB + off) = wd[p];
     }
     umma::fence_async_smem();
+    // TMEM is held only from the first MMA to the end of the epilogue; this grid lets dependent kernels launch
+    // (pdl_trigger) only after its blocks have released it, so a dependent that holds TMEM while it waits for
+    // this grid can never take the columns a block of this grid still needs
+    if (nchunk == 0 && warp == 0) umma::tmem_alloc(&s_tmem, NCOL);
+    umma::tc_before_sync();
     __syncthreads();
+    umma::tc_after_sync();
     if (tid == 0) {
-      umma::tc_after_sync();
+      const uint32_t tmem = s_tmem;
       for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
         for (int q = 0; q < 10; ++q) {
@@ -250,6 +271,7 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
   }
   __syncthreads();
   umma::tc_after_sync();
+  const uint32_t tmem = s_tmem;
   if (s_abort) {  // an MMA never completed: report, wait once more for it, free TMEM, leave
     if (tid == 0) {
       set_status(a.status, ARP_ERR_TIMEOUT);
@@ -259,17 +281,20 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
     if (warp == 0) umma::tmem_free(tmem, NCOL);
     return;
   }
-  // ---- epilogue: each row of Q from the four class accumulators, summed exactly in double (every class is an
-  //      exact s32 and the sum spans < 53 bits), scaled by 2^-2s and rounded once to float.  TMEM lane of row m:
-  //      m (M = 128), or m % 16 + 32 (m / 16) (M = 64); warp w reads lanes 32 w .. 32 w + 31.
-  if (warp < 4) {
-    const int m = MP == 128 ? warp * 32 + lane : warp * 16 + lane;
+  // ---- epilogue: each entry of Q from the four class accumulators, summed exactly as an integer
+  //      P = ((c6 2^8 + c5) 2^8 + c4) 2^8 + c3 (|P| < 2^50), converted once with rounding to nearest and scaled by
+  //      2^(24 - 2s) (exact).  TMEM lane of row m: m (M = 128), or m % 16 + 32 (m / 16) (M = 64); warps w and w + 4
+  //      read lanes 32 (w % 4) .. + 31, the first and the second half of the columns.
+  {
+    const int wq = warp & 3, half = warp >> 2;
+    const int m = MP == 128 ? wq * 32 + lane : wq * 16 + lane;
     const bool valid = (MP == 128 || lane < 16) && m < Dp;
-    const int sx2 = -2 * s_exp;
+    const int e2 = 24 - 2 * s_exp;
+    constexpr int CW = Dp >= 16 ? Dp / 2 : Dp;
 #pragma unroll 1
-    for (int c0 = 0; c0 < Dp; c0 += 8) {
+    for (int c0 = half * CW; c0 < (half + 1) * CW && c0 < Dp; c0 += 8) {
       uint32_t v6[8], v5[8], v4[8], v3[8];
-      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      const uint32_t ta = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0;
       umma::tmem_ld8_nowait(ta, v6);
       umma::tmem_ld8_nowait(ta + Dp, v5);
       umma::tmem_ld8_nowait(ta + 2 * Dp, v4);
@@ -278,9 +303,9 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
       if (valid) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          const double q = ldexp((double)(int32_t)v6[j], 48) + ldexp((double)(int32_t)v5[j], 40) +
-                           ldexp((double)(int32_t)v4[j], 32) + ldexp((double)(int32_t)v3[j], 24);
-          Qs[m * QP + c0 + j] = __double2float_rn(ldexp(q, sx2));
+          const long long q = ((((long long)(int32_t)v6[j] * 256 + (int32_t)v5[j]) * 256 + (int32_t)v4[j]) * 256) +
+                              (int32_t)v3[j];
+          Qs[m * QP + c0 + j] = ldexpf(__ll2float_rn(q), e2);
         }
       }
     }
@@ -288,6 +313,7 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
   umma::tc_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tmem, NCOL);
+  pdl_trigger();  // the chain's next kernel may launch and set up; it waits for this grid before reading
   float A[TB][TB];
   float qmax = 0.0f;
   const float s2 = a.xg ? 0.0f : a.sigma2[b];  // only the MMSE solve reads sigma2 (null for a given guess)

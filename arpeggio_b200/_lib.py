@@ -21,6 +21,7 @@ SIGNATURES = {
     'arp_philox_rate': [_P, _I, _I, _I, _P],
     'arp_anneal_first_accept': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
     'arp_anneal_chord_dd': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
+    'arp_anneal_chord_dd_n1': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P, _P],
     'arp_anneal_chord_engine': [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _P, _P],
     'arp_anneal_dd_f32': [_I, _P, _P, _P, _P, _I, _F, _I, _I, _I, _I, _P, _U, _U, _I, _P, _P, _P, _P, _P],
     'arp_anneal_chord': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _U, _U, _U, _I, _I, _P, _P, _P, _P, _P],
@@ -39,6 +40,7 @@ SIGNATURES = {
     'arp_mdi_update': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P],
     'arp_mdi_select': [_P, _P, _I, _I, _I, _I, _P, _P, _P],
     'arp_anneal_tune': [_I, _I, _I, _I, _I],
+    'arp_anneal_first_accept_mixed': [_P, _I, _I, _U, _U, _I, _P, _P, _P],
     'arp_map_dd_soft': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P],
     'arp_gemm_bf16': [_P, _I, _I, _P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _I, _P, _P],
     'arp_warm_features': [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P],
@@ -59,6 +61,12 @@ SIGNATURES = {
 }
 
 _lib = None
+
+
+class MixedClass(ctypes.Structure):
+    """arp_mixed_class: one size class of arp_anneal_first_accept_mixed (layout of include/arpeggio_b200.h)."""
+    _fields_ = [('Gt', _P), ('h', _P), ('T', _P), ('L', _I), ('q', _I), ('R', _I), ('D', _I), ('B', _I),
+                ('inst', _P), ('start', _I), ('out_s', _P), ('out_de', _P), ('out_st', _P)]
 
 
 class ArpError(RuntimeError):

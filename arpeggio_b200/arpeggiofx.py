@@ -24,11 +24,13 @@ def _u32(x, dev):
 
 @torch.no_grad()
 def anneal(Gt, h, P, R, T, q, inst, key, start='rand', policy='arpeggio', c=None, precision='int', out=None,
-           status=None, stream=None):
+           status=None, stream=None, n1=None):
     """Device anneal.  Gt (B, D, D) transposed coupling (Gt[b, j, i] = G[b, i, j]) on the GPU, int32 for
     precision 'int' or float32 for 'f32'; h (B, D) likewise; T (L,) and c (L,) or None device tensors;
     inst (B,) int32 bit patterns of uint32 instance numbers.  Returns (spins (B, R, P D) int8,
-    de (B, R) int64 or float32, st (B, R, 2) int64, status (1,) int32) without synchronising."""
+    de (B, R) int64 or float32, st (B, R, 2) int64, status (1,) int32) without synchronising.  n1: for the integer
+    Chord round, an int64 (B, R) device tensor that receives the rounds with at least one flip per anneal (the term
+    of the Chord engine's latency 3 L + F + n1)."""
     if policy not in POLICIES:
         raise ValueError('policy must be one of %s' % (POLICIES,))
     B, D, _ = Gt.shape
@@ -53,6 +55,10 @@ def anneal(Gt, h, P, R, T, q, inst, key, start='rand', policy='arpeggio', c=None
     elif policy == 'arpeggio':
         rc = lib.arp_anneal_first_accept(_lib.ptr(Gt), _lib.ptr(h), _lib.ptr(T), L, int(q), P, R, D, B,
                                          _lib.ptr(inst), k0, k1, sv, *args)
+    elif n1 is not None:
+        rc = lib.arp_anneal_chord_dd_n1(_lib.ptr(Gt), _lib.ptr(h), _lib.ptr(T), _lib.ptr(c), L, int(q), P, R, D, B,
+                                        _lib.ptr(inst), k0, k1, sv, _lib.ptr(s_), _lib.ptr(de), _lib.ptr(st),
+                                        _lib.ptr(n1), _lib.ptr(status), _lib.stream_ptr(stream))
     else:
         rc = lib.arp_anneal_chord_dd(_lib.ptr(Gt), _lib.ptr(h), _lib.ptr(T), _lib.ptr(c), L, int(q), P, R, D, B,
                                      _lib.ptr(inst), k0, k1, sv, *args)

@@ -24,6 +24,7 @@
 // s w < ceil(u*4T / 2^32) - 2 G_jj - q - 2T, a 32-bit compare; the entry points bound |G|, |h|, |T|, |q|
 // so that every field and threshold fits 32 bits (ARP_ERR_RANGE otherwise).
 #include <climits>
+#include <cstring>
 #include <mutex>
 #include <type_traits>
 
@@ -342,19 +343,18 @@ __device__ __forceinline__ uint32_t eng_xs32(uint32_t x) {
 // seed chain (engine_model.cpp:185-194, 170-184, 142-163), its bits 31, 30, ... give the start spins of copies
 // 0, 1, ..., and every step advances it once and tests with its top 16 bits: u 4 T > z 2^16 (:229-257).
 template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false, bool ENG = false>
-// Four slots (D > 96) are bounded at 128 registers: four 4-warp blocks per SM instead of three (no spills;
-// 64 users: 129 -> 120 ms per 32768 uses).
-__global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
+// One problem b of a block: its G staged in shared memory, anneals r = bs + split w, + split W, ... by the block's
+// warps.  Called by the per-launch kernel below (one problem per block) and by the persistent mixed-size kernel
+// (problems taken from a work counter, one after another).  Returns with every thread done reading shared memory.
+__device__ __forceinline__ void anneal_int_problem(const DDParams& a, const PhiloxKeys& K, const int b, const int bs) {
   constexpr int DP = NS * 32;
   extern __shared__ __align__(16) unsigned char smem[];
   int32_t* Gs = reinterpret_cast<int32_t*>(smem);
   __shared__ int s_bad;
   __shared__ uint8_t s_perm[WARM ? 128 : 1];
   const int D = a.D, L = a.L, R = a.R;
-  const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
+  const int split = a.split;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, W = blockDim.x >> 5;
-  pdl_trigger();
-  pdl_wait();
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
   const int32_t* hg = reinterpret_cast<const int32_t*>(a.h) + (size_t)b * D;
@@ -409,7 +409,6 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
     return;
   }
   const uint32_t inst = a.inst ? a.inst[b] : a.inst0 + (uint32_t)b;
-  const PhiloxKeys& K = *reinterpret_cast<const PhiloxKeys*>(a.rk0);
   // 2 G_jj; a padding lane (j >= D: h_j = 0 and G's row and column j are zero, so w_j stays 0) gets 2^29, making
   // its margin psi2 = 2^30 + s at least every threshold kap2 = 2 (ceil(u 4 T / 2^32) - B) <= 2^30 (|4 T| <= 2^28,
   // |B| <= 2^28 by the range checks): it never accepts, with no per-pass validity select.
@@ -525,7 +524,7 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
     }
     long long de = 0, best = ENG ? (1LL << 35) - 1 : 1LL << 62;  // the engine's best register starts at 2^35 - 1
     uint32_t bsp = sp;
-    int32_t flips = 0, lastflips = 0;
+    int32_t flips = 0, lastflips = 0, n1 = 0;
     const int nquad = (L + 4 * P - 1) / (4 * P);
     for (int q4 = 0; q4 < nquad; ++q4) {
       uint32_t cw[CACHE ? P : 1][CACHE ? NS : 1][4];
@@ -607,9 +606,13 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
               }
             }
           } else {
-            uint32_t am[NS];
+            uint32_t am[NS], anyf = 0;
 #pragma unroll
-            for (int t = 0; t < NS; ++t) am[t] = __ballot_sync(ARP_FULL, psi2[t] < kap2[t]);
+            for (int t = 0; t < NS; ++t) {
+              am[t] = __ballot_sync(ARP_FULL, psi2[t] < kap2[t]);
+              anyf |= am[t];
+            }
+            n1 += anyf != 0u;
 #pragma unroll
             for (int t = 0; t < NS; ++t) {
               uint32_t m = am[t];
@@ -647,8 +650,19 @@ __global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_i
       reinterpret_cast<long long*>(a.out_de)[ar] = best;
       a.out_st[2 * ar] = flips;
       a.out_st[2 * ar + 1] = CHORD ? L : L + flips - lastflips;
+      if (CHORD && a.out_n1) a.out_n1[ar] = n1;
     }
   }
+}
+
+template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false, bool ENG = false>
+// Four slots (D > 96) are bounded at 128 registers: four 4-warp blocks per SM instead of three (no spills;
+// 64 users: 129 -> 120 ms per 32768 uses).
+__global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
+  const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
+  pdl_trigger();
+  pdl_wait();
+  anneal_int_problem<NS, P, CHORD, CACHE, WARM, ENG>(a, *reinterpret_cast<const PhiloxKeys*>(a.rk0), b, bs);
 }
 
 // Warps per block: a block holds one problem and its warps share the anneals, so fewer warps per block let
@@ -835,6 +849,19 @@ extern "C" int arp_anneal_chord_dd(const int32_t* Gt, const int32_t* h, const in
                                                                                                 : ARP_ERR_LAUNCH;
 }
 
+extern "C" int arp_anneal_chord_dd_n1(const int32_t* Gt, const int32_t* h, const int32_t* T, const int32_t* c, int L,
+                                      int q, int P, int R, int D, int B, const uint32_t* inst, uint32_t k0,
+                                      uint32_t k1, int start, int8_t* out_s, int64_t* out_de, int64_t* out_st,
+                                      int64_t* out_n1, int32_t* status, void* stream) {
+  int rc = check_dd(Gt, h, T, L, P, R, D, B, inst, start, out_s, out_de, out_st);
+  if (rc || B == 0) return rc;
+  if (!out_n1) return ARP_ERR_ARG;
+  DDParams a{Gt, h, T, c, L, q, 0.0f, R, D, B, inst, 0u, k0, k1, start, out_s, out_de, out_st, status};
+  a.out_n1 = out_n1;
+  return anneal_dispatch(1, false, a, P, default_warps(R), (cudaStream_t)stream) == cudaSuccess ? ARP_OK
+                                                                                                : ARP_ERR_LAUNCH;
+}
+
 extern "C" int arp_anneal_dd_f32(int policy, const float* Gt, const float* h, const float* T, const float* c, int L,
                                  float q, int P, int R, int D, int B, const uint32_t* inst, uint32_t k0, uint32_t k1,
                                  int start, int8_t* out_s, float* out_de, int64_t* out_st, int32_t* status,
@@ -896,11 +923,158 @@ extern "C" int arp_anneal_first_accept_warm(const int32_t* Gt, const int32_t* h,
   return launch_warm(a, (cudaStream_t)stream) == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 
+// ---------------------------------------------------------------- persistent mixed-size first accept
+// Every problem of every size class of a mixed batch in one grid per coordinate-slot count NS (at most four
+// launches): the grid is sized to the SMs' resident blocks, and each block takes problems from a work counter in
+// global memory (one atomicAdd per problem, no waiting on other blocks) until the batch is done, running the
+// per-size body compiled for its NS.  Problems are numbered class by class, the classes in decreasing cost per
+// problem (L R D), so the costly problems start first and the short ones fill the tail.  Each problem's anneals are
+// exactly those of the per-class launch (same body, same counters), so the outputs do not depend on the schedule.
+constexpr int kMaxMixed = 64;
+
+struct MixedArgs {
+  PhiloxKeys K;  // one key for the whole batch (kernel parameter: the rounds read it as constant operands)
+  int total;
+  int* counter;
+  int first[kMaxMixed + 1];  // problems of class c: first[c] .. first[c + 1] - 1
+  DDParams cls[kMaxMixed];
+};
+
+template <int NS>
+__global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_mixed(const __grid_constant__ MixedArgs g) {
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();  // the previous problem's shared memory is no longer read
+    if (threadIdx.x == 0) s_item = atomicAdd(g.counter, 1);
+    __syncthreads();
+    const int i = s_item;
+    if (i >= g.total) break;
+    int c = 0;
+    while (c + 1 < kMaxMixed && g.first[c + 1] <= i) ++c;
+    anneal_int_problem<NS, 2, false, (2 * NS <= 8)>(g.cls[c], g.K, i - g.first[c], 0);
+  }
+}
+
+template <int NS>
+static cudaError_t launch_mixed(MixedArgs& g, int Dmax, int warps, int* counter, cudaStream_t st) {
+  auto kern = k_anneal_mixed<NS>;
+  const size_t smem = (size_t)Dmax * NS * 32 * 4;
+  struct Slot {
+    size_t attr_smem = 48 * 1024;
+    int sms = 0;
+  };
+  static Slot slots_by_dev[kMaxDevices];
+  static std::mutex mu;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  int sms = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    Slot& sl = slots_by_dev[dev];
+    if (smem > sl.attr_smem) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      sl.attr_smem = smem;
+    }
+    if (sl.sms == 0) cudaDeviceGetAttribute(&sl.sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = sl.sms;
+  }
+  int W = warps;
+  if (W <= 0) W = g_tuned_warps[NS][2][0][0];
+  if (W <= 0) W = pick_warps(kern, smem, 8);
+  int nb = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * W, smem);
+  if (e != cudaSuccess) return e;
+  if (nb < 1) return cudaErrorInvalidConfiguration;
+  long long grid = (long long)nb * (sms > 0 ? sms : 148);
+  if (grid > g.total) grid = g.total;
+  g.counter = counter;
+  e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)grid, 32 * W, smem, st>>>(g);
+  return cudaGetLastError();
+}
+
 extern "C" int arp_anneal_tune(int D, int P, int policy, int precision, int warps) {
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || (policy != 0 && policy != 1) ||
       (precision != 0 && precision != 1))
     return ARP_ERR_SHAPE;
   if (!(warps == 0 || warps == 1 || warps == 2 || warps == 4 || warps == 8)) return ARP_ERR_ARG;
   g_tuned_warps[(D + 31) / 32][P][policy][precision] = warps;
+  return ARP_OK;
+}
+
+/* Persistent mixed-size first accept: see the header.  Classes are grouped by slot count and ordered by cost. */
+extern "C" int arp_anneal_first_accept_mixed(const arp_mixed_class* cls, int ncls, int P, uint32_t k0, uint32_t k1,
+                                             int warps, int* counters, int32_t* status, void* stream) {
+  if (ncls < 0 || ncls > kMaxMixed || P != 2) return ARP_ERR_SHAPE;
+  if (ncls == 0) return ARP_OK;
+  if (!cls || !counters) return ARP_ERR_ARG;
+  if (!(warps == 0 || warps == 1 || warps == 2 || warps == 4 || warps == 8)) return ARP_ERR_ARG;
+  for (int c = 0; c < ncls; ++c) {
+    const arp_mixed_class& m = cls[c];
+    const int rc = check_dd(m.Gt, m.h, m.T, m.L, 2, m.R, m.D, m.B, m.inst, m.start, m.out_s, m.out_de, m.out_st);
+    if (rc != ARP_OK) return rc;
+  }
+  const PhiloxKeys K = philox_keys(k0, k1);
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int ns = 4; ns >= 1; --ns) {
+    // this group's classes, in decreasing cost per problem
+    int idx[kMaxMixed], n = 0, Dmax = 0;
+    for (int c = 0; c < ncls; ++c)
+      if ((cls[c].D + 31) / 32 == ns && cls[c].B > 0) idx[n++] = c;
+    if (n == 0) continue;
+    auto cost = [&](int c) { return (double)cls[c].L * cls[c].R * cls[c].D; };
+    for (int i = 1; i < n; ++i)
+      for (int j = i; j > 0 && cost(idx[j]) > cost(idx[j - 1]); --j) {
+        const int t = idx[j];
+        idx[j] = idx[j - 1];
+        idx[j - 1] = t;
+      }
+    MixedArgs g;
+    memset(&g, 0, sizeof(g));
+    g.K = K;
+    int total = 0;
+    for (int i = 0; i < n; ++i) {
+      const arp_mixed_class& m = cls[idx[i]];
+      DDParams& a = g.cls[i];
+      a.Gt = m.Gt;
+      a.h = m.h;
+      a.T = m.T;
+      a.c = nullptr;
+      a.L = m.L;
+      a.qi = m.q;
+      a.R = m.R;
+      a.D = m.D;
+      a.B = m.B;
+      a.inst = m.inst;
+      a.start = m.start;
+      a.out_s = m.out_s;
+      a.out_de = m.out_de;
+      a.out_st = m.out_st;
+      a.status = status;
+      a.split = 1;
+      a.m0 = nullptr;
+      a.perm = nullptr;
+      a.warm_r = 1 << 30;
+      a.cdf = nullptr;
+      a.ra = nullptr;
+      g.first[i] = total;
+      total += m.B;
+      if (m.D > Dmax) Dmax = m.D;
+    }
+    for (int i = n; i <= kMaxMixed; ++i) g.first[i] = total;
+    g.total = total;
+    cudaError_t e;
+    switch (ns) {
+      case 1: e = launch_mixed<1>(g, Dmax, warps, counters + 0, st); break;
+      case 2: e = launch_mixed<2>(g, Dmax, warps, counters + 1, st); break;
+      case 3: e = launch_mixed<3>(g, Dmax, warps, counters + 2, st); break;
+      default: e = launch_mixed<4>(g, Dmax, warps, counters + 3, st); break;
+    }
+    if (e != cudaSuccess) return ARP_ERR_LAUNCH;
+  }
   return ARP_OK;
 }

@@ -35,6 +35,8 @@ struct DDParams {
   // per-problem anneal counts (B), or null: problem b runs anneals r < ra[b] (clamped to 1..R); the skipped
   // anneals report all-zero spin sums (the guess), best energy INT64_MAX and no tests or flips
   const int32_t* ra = nullptr;
+  // Chord round (integer fields), or null: per anneal the rounds with at least one flip (B, R)
+  int64_t* out_n1 = nullptr;
 };
 
 struct MapParams {

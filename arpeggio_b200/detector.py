@@ -219,6 +219,35 @@ class Detector:
         _lib.check(rc, 'detect')
         return self.bits, self.levels, self.dist
 
+    # ---- the three stages of a whole-batch detection, for callers that schedule the anneal themselves (the mixed
+    #      batch's persistent anneal): map, then the anneal described by mixed_class(), then readout
+    def stage_map(self, H, y, stream=None, inst0=0):
+        if self.precision != 'int' or self.policy != 'arpeggio':
+            raise ValueError('the staged path serves integer first-accept detectors')
+        key = (inst0, 0, self.B)
+        if self._inst_base != key:
+            iv = (np.arange(inst0, inst0 + self.B, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
+            self.inst.copy_(torch.from_numpy(iv))
+            self._inst_base = key
+        L = _lib.lib()
+        _lib.check(L.arp_map_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.sigma2), self.B, self.NR2, self.D, self.M, 1,
+                                _lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.xq), _lib.ptr(self.scale),
+                                _lib.ptr(self.status), _lib.stream_ptr(stream)), 'map')
+
+    def mixed_class(self):
+        """This detector's anneal as one class of arp_anneal_first_accept_mixed (after stage_map)."""
+        return _lib.MixedClass(_lib.ptr(self.G), _lib.ptr(self.h), _lib.ptr(self.T), int(self.T.shape[0]),
+                               int(self.q), self.R, self.D, self.B, _lib.ptr(self.inst),
+                               0 if self.start == 'rand' else 1, _lib.ptr(self.spins), _lib.ptr(self.de),
+                               _lib.ptr(self.st))
+
+    def stage_readout(self, H, y, stream=None):
+        L = _lib.lib()
+        _lib.check(L.arp_readout_dd(_lib.ptr(H), _lib.ptr(y), _lib.ptr(self.xq), _lib.ptr(self.spins), self.B,
+                                    self.NR2, self.D, self.P, self.R, self.M, _lib.ptr(self.levels), self._out_ptr(0),
+                                    self._out_ptr(1), _lib.ptr(self.pick), _lib.stream_ptr(stream)), 'readout')
+        return self.bits, self.levels, self.dist
+
     def _out_ptr(self, i, sl=None):
         """Readout destination: bits (i = 0) or distances (i = 1) of the whole batch, or the mapped host
         outputs of a frame being captured."""

@@ -42,7 +42,8 @@ def detect(H, y, N0, M, seed, pick, Rmax=None, stages=None, policy='arpeggio', p
     """H (B, 2Nr, 2Nt), y (B, 2Nr) float32 (device or host), N0 scalar, M in {4, 16}; seed = the batch's draw
     seed (run_a513 passes arpx.draw_seed(seed, snr, bi)); pick: dict or abl_far_* string.
     Returns (levels (B, D) int8 on the device, anneals per use (B,) float64 numpy, per-K counters
-    {K: [flips, tests, anneals]})."""
+    {K: [flips, tests, anneals]}, for the integer Chord round {K: [flips, steps, anneals, n1]} with n1 the rounds
+    that flipped)."""
     pk = parse_pick(pick) if isinstance(pick, str) else dict(pick)
     dev = torch.device('cuda')
     H = torch.as_tensor(H, dtype=torch.float32).to(dev).contiguous()
@@ -109,16 +110,20 @@ def detect(H, y, N0, M, seed, pick, Rmax=None, stages=None, policy='arpeggio', p
                     key = (seed_base + calls * KEY_STEP + KEY_TAG) & M64
                     calls += 1
                     T, q, c = sched[K]
+                    n1 = (torch.empty(n, na, dtype=torch.int64, device=dev)
+                          if policy == 'chord' and precision == 'int' else None)
                     spins, de, stt, _ = anneal(Gm, hm, P, na, T, q, idx, key, pk['start'], policy, c, precision,
-                                               status=status)
+                                               status=status, n1=n1)
                     _lib.check(L.arp_mdi_update(_lib.ptr(H), _lib.ptr(y), _lib.ptr(idx), n, NR2, D, P, na, M,
                                                 _lib.ptr(cur), G, gi, _lib.ptr(spins), _lib.ptr(nxt), _lib.ptr(bd),
                                                 sp), 'mdi_update')
-                    v = cnt.setdefault(str(K), [0, 0, 0])
+                    v = cnt.setdefault(str(K), [0, 0, 0] if n1 is None else [0, 0, 0, 0])
                     s_ = stt.sum((0, 1)).tolist()
                     v[0] += int(s_[0])
                     v[1] += int(s_[1])
                     v[2] += int(na * n)
+                    if n1 is not None:
+                        v[3] += int(n1.sum())
                     ann[idx_np] += na
         cur = nxt
     _lib.check(L.arp_mdi_radius(_lib.ptr(H), _lib.ptr(y), _lib.ptr(cur), B, NR2, D, G, M, Rmax, _lib.ptr(Rd),

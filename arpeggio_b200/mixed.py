@@ -28,35 +28,56 @@ def mixed_classes():
 
 
 class Autotuner:
-    """Per size class, the anneal launch width with the shortest device time on a sample of the class's uses."""
+    """Per size class (coordinates D, copies P): the anneal launch width (warps per block = anneals per CTA in flight)
+    with the shortest device time on a sample of the class's uses, installed through arp_anneal_tune, and, when asked,
+    the field precision (int32 fixed point or FP32) whose anneal is faster.  The width never changes results; the
+    precision does (the FP32 rule is a different, equally valid detector), so it is chosen only when the caller
+    offers both."""
 
     WIDTHS = (1, 2, 4, 8)
 
     def __init__(self):
         self.table = {}
 
-    def tune(self, det, H, y, seed=1, reps=3):
+    def _time(self, det, H, y, seed, reps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        det.run(H, y, seed, events=ev)
+        ms = 0.0
+        for _ in range(reps):
+            det.run(H, y, seed, events=ev)
+            torch.cuda.synchronize()
+            ms += ev[1].elapsed_time(ev[2])
+        return ms / reps
+
+    def tune(self, det, H, y, seed=1, reps=3, precisions=('int',)):
         D, P = det.D, det.P
         key = (D, P, 0, 0)
         if key in self.table:
             return self.table[key]
         L = _lib.lib()
-        best, best_ms, times = 0, float('inf'), {}
-        for w in self.WIDTHS:
-            _lib.check(L.arp_anneal_tune(D, P, 0, 0, w), 'anneal_tune')
-            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-            det.run(H, y, seed, events=ev)
-            ms = 0.0
-            for _ in range(reps):
-                det.run(H, y, seed, events=ev)
-                torch.cuda.synchronize()
-                ms += ev[1].elapsed_time(ev[2])
-            times[w] = ms / reps
-            if times[w] < best_ms:
-                best, best_ms = w, times[w]
-        _lib.check(L.arp_anneal_tune(D, P, 0, 0, best), 'anneal_tune')
-        self.table[key] = {'warps': best, 'anneal_ms': times}
-        return self.table[key]
+        entry = {'precision_ms': {}}
+        for prec in precisions:
+            pc = 0 if prec == 'int' else 1
+            d = det if prec == det.precision else Detector(det.B, det.nt, det.nr, det.M, 'arpeggio', det.R, det.K,
+                                                             start=det.start, precision=prec, device=det.device)
+            if d is not det:
+                d.sigma2.copy_(det.sigma2)
+            best, best_ms, times = 0, float('inf'), {}
+            for w in self.WIDTHS:
+                _lib.check(L.arp_anneal_tune(D, P, 0, pc, w), 'anneal_tune')
+                times[w] = self._time(d, H, y, seed, reps)
+                if times[w] < best_ms:
+                    best, best_ms = w, times[w]
+            _lib.check(L.arp_anneal_tune(D, P, 0, pc, best), 'anneal_tune')
+            self.table.setdefault((D, P, 0, pc), {})
+            entry['precision_ms'][prec] = best_ms
+            if prec == det.precision:
+                entry.update(warps=best, anneal_ms=times)
+            else:
+                self.table[(D, P, 0, pc)] = {'warps': best, 'anneal_ms': times}
+        entry['precision'] = min(entry['precision_ms'], key=entry['precision_ms'].get)
+        self.table[key] = entry
+        return entry
 
     def reset(self):
         L = _lib.lib()
@@ -70,9 +91,16 @@ class Autotuner:
 
 class MixedBatch:
     """Preallocated detectors for `counts` {(nt, nr, M): uses}; plain MMSE-started Arpeggio (warm-started with an
-    MLP) at the Arpeggio picks' budgets, `anneals` anneals per use."""
+    MLP) at the Arpeggio picks' budgets, `anneals` anneals per use.  persistent=True (plain detectors only): the
+    maps and readouts stay per class on forked streams, and every class's anneals run in the persistent grids of
+    arp_anneal_first_accept_mixed (one launch per slot count, blocks pulling problems from a device work counter);
+    the outputs equal the per-class path's."""
 
-    def __init__(self, counts, anneals=32, mlp=None, streams=8, device='cuda'):
+    def __init__(self, counts, anneals=32, mlp=None, streams=8, device='cuda', persistent=False):
+        if persistent and mlp is not None:
+            raise ValueError('the persistent anneal serves the plain MMSE-started detectors')
+        self.persistent = persistent
+        self.counters = torch.zeros(16, dtype=torch.int32, device=device)  # 4 per slot-count group
         self.device = torch.device(device)
         self.classes = [tuple(c) for c in counts]
         self.counts = {tuple(c): int(n) for c, n in counts.items()}
@@ -105,6 +133,8 @@ class MixedBatch:
 
     def run(self, seed):
         """Every class on a stream forked from the current stream, joined back at the end (graph-capturable)."""
+        if self.persistent:
+            return self._run_persistent(seed)
         cur = torch.cuda.current_stream()
         for i, cls in enumerate(self.classes):
             s = self.streams[i % len(self.streams)]
@@ -112,6 +142,35 @@ class MixedBatch:
             with torch.cuda.stream(s):
                 self.dets[cls].run(self.H[cls], self.y[cls], seed, stream=s)
         for s in self.streams:
+            cur.wait_stream(s)
+
+    def _run_persistent(self, seed):
+        """Classes grouped by slot count (ceil(D / 32)); each group on its own stream: its maps, one persistent anneal
+        launch for all of its classes, its readouts, so one group's anneal overlaps another's maps, readouts and
+        drain."""
+        cur = torch.cuda.current_stream()
+        groups = {}
+        for cls in self.classes:
+            groups.setdefault((2 * cls[0] + 31) // 32, []).append(cls)
+        L = _lib.lib()
+        used = []
+        for gi, ns in enumerate(sorted(groups, reverse=True)):
+            s = self.streams[gi % len(self.streams)]
+            s.wait_stream(cur)
+            used.append(s)
+            members = groups[ns]
+            with torch.cuda.stream(s):
+                for cls in members:
+                    self.dets[cls].stage_map(self.H[cls], self.y[cls], stream=s)
+                table = (_lib.MixedClass * len(members))(*[self.dets[c].mixed_class() for c in members])
+                st = self.dets[members[0]].status
+                _lib.check(L.arp_anneal_first_accept_mixed(table, len(members), 2, seed & 0xFFFFFFFF,
+                                                           (seed >> 32) & 0xFFFFFFFF, 0,
+                                                           _lib.ptr(self.counters[4 * gi:4 * gi + 4]), _lib.ptr(st),
+                                                           _lib.stream_ptr(s)), 'anneal_mixed')
+                for cls in members:
+                    self.dets[cls].stage_readout(self.H[cls], self.y[cls], stream=s)
+        for s in used:  # only the streams this call forked (joining an unforked one breaks a capture)
             cur.wait_stream(s)
 
     def capture(self, seed):
@@ -128,17 +187,35 @@ class MixedBatch:
         self.graph = g
         return g
 
-    def tune(self, tuner):
-        """Tunes the anneal width once per problem size (coordinates D), on the largest class of that size with its
-        drawn uses (call draw() first)."""
+    def tune(self, tuner, precisions=('int',)):
+        """Tunes the anneal width (and, with precisions=('int', 'f32'), the field precision) once per problem size
+        (coordinates D), on the largest class of that size with its drawn uses (call draw() first)."""
         by_d = {}
         for cls in self.classes:
             D = 2 * cls[0]
             if D not in by_d or self.counts[cls] > self.counts[by_d[D]]:
                 by_d[D] = cls
         for D, cls in sorted(by_d.items()):
-            tuner.tune(self.dets[cls], self.H[cls], self.y[cls])
+            tuner.tune(self.dets[cls], self.H[cls], self.y[cls], precisions=precisions)
         return tuner.table
+
+    def apply_precision(self, tuner):
+        """Rebuilds, for the per-class graph path, the detectors of every size whose tuned precision differs from
+        theirs (the persistent anneal serves integer fields only).  Returns the classes rebuilt."""
+        if self.persistent:
+            return []
+        done = []
+        for cls in self.classes:
+            det = self.dets[cls]
+            e = tuner.table.get((det.D, det.P, 0, 0))
+            if e is None or e.get('precision', det.precision) == det.precision:
+                continue
+            nd = Detector(det.B, det.nt, det.nr, det.M, 'arpeggio', det.R, det.K, start=det.start,
+                          precision=e['precision'], device=det.device)
+            nd.sigma2.copy_(det.sigma2)
+            self.dets[cls] = nd
+            done.append(cls)
+        return done
 
     def check(self):
         for det in self.dets.values():

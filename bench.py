@@ -216,6 +216,8 @@ def frame_latency(det, f, stream, n):
 CONF_PER_COORD = 5.0 / 64
 WARM_POINTS = {32: {'warm': dict(sweeps=24, T=0.085, tau=0.8, counts=True, r_easy=4),
                     'warm_fast': dict(sweeps=20, T=0.085, tau=0.8, counts=True, r_easy=4),
+                    # the configuration's own comparison: warm at half the plain cycle budget (16 of 32 sweeps)
+                    'warm_half': dict(sweeps=16, T=0.085, tau=0.6, counts=True, r_easy=4),
                     'warm_argmax': dict(sweeps=24, T=0.085, tau=None, counts=False)},
                64: {'warm': dict(sweeps=24, T=0.07, tau=0.8, counts=True),
                     'warm_fast': dict(sweeps=32, T=0.07, tau=0.8, counts=True, per_coord=1.6 * CONF_PER_COORD,
@@ -252,6 +254,8 @@ def warm_vs_plain(args, dev, stream, rank):
                    'p_jc above -%.4f D run 4 anneals at 32 users (one per warp of the anneal block), %d at 64 users '
                    '(warm_fast at 64 users: above -%.4f D, 16 anneals), the others all R'
                    % (CONF_PER_COORD, R_EASY, 1.6 * CONF_PER_COORD),
+           'warm_half': 'the warm detector at half the plain budget (16 of 32 sweeps, softmax(0.6 z) starts), the '
+                        'configuration\'s own comparison (32 users)',
            'warm_argmax': 'every anneal from the argmax class, all R anneals, at the warm budget',
            'points': {'x%d' % k: v for k, v in WARM_POINTS.items()}}
     for nt, B, snrs, full, R in ((32, args.batch, [18, 20, 22, 24], 32, 32),
@@ -329,14 +333,42 @@ def mixed_batch(args, dev, rank):
     mb.draw(7 + rank)
     tuner = mixed.Autotuner()
     t0 = time.time()
-    mb.tune(tuner)
+    mb.tune(tuner, precisions=('int', 'f32'))
     tune_s = time.time() - t0
     g = mb.capture(seed=3)
     ms = mixed.timed_replay(g, reps=3)
     mb.check()
+    ber = mb.ber()
+    bits = {c: d.bits.clone() for c, d in mb.dets.items()}
+    del g
+    # the same batch with every class's anneals in the persistent grids (blocks pulling problems from a device work
+    # counter): same outputs, one anneal launch per slot count instead of one per class
+    mb.persistent = True
+    g = mb.capture(seed=3)
+    ms_p = mixed.timed_replay(g, reps=3)
+    mb.check()
+    same = all(torch.equal(bits[c], d.bits) for c, d in mb.dets.items())
+    g = None
+    mb.persistent = False
+    rebuilt = mb.apply_precision(tuner)  # sizes whose FP32-field anneal was faster, if any
+    ms_t = None
+    if rebuilt:
+        g = mb.capture(seed=3)
+        ms_t = mixed.timed_replay(g, reps=3)
+        mb.check()
     out = {'value': total / (ms / 1e3), 'unit': 'detections/s', 'detections': total, 'classes': len(counts),
-           'ms_per_replay': ms, 'ber': mb.ber(), 'tune_seconds': tune_s,
-           'tuned_warps_per_block': {'D=%d' % k[0]: v['warps'] for k, v in tuner.table.items()},
+           'ms_per_replay': ms, 'ber': ber, 'tune_seconds': tune_s,
+           'tuned_warps_per_block': {'D=%d' % k[0]: v['warps'] for k, v in tuner.table.items() if k[3] == 0},
+           'tuned_precision': {'D=%d' % k[0]: {'pick': v['precision'],
+                                               'anneal_ms': {p: round(t, 3) for p, t in v['precision_ms'].items()}}
+                               for k, v in tuner.table.items() if k[3] == 0},
+           'classes_rebuilt_for_precision': len(rebuilt),
+           'value_with_tuned_precision': None if ms_t is None else total / (ms_t / 1e3),
+           'persistent': {'value': total / (ms_p / 1e3), 'unit': 'detections/s', 'ms_per_replay': ms_p,
+                          'bits_equal_to_per_class_graph': same,
+                          'path': 'classes grouped by slot count, one stream per group: its maps, one persistent '
+                                  'anneal grid for all its classes (arp_anneal_first_accept_mixed, blocks pulling '
+                                  'problems from a device work counter), its readouts'},
            'config': 'users {8,16,24,32,48,64} x antennas {1,1.5,2}x users x {QPSK,16-QAM,64-QAM}, SNR U[5,25] dB, '
                      'MMSE-started Arpeggio first accept, 32 anneals, one CUDA graph (8 streams)'}
     tuner.reset()
@@ -750,6 +782,8 @@ def summary(line):
     mx = line.get('mixed') or {}
     if mx.get('value'):
         out['mixed_det_per_s'] = _r(mx['value'])
+        if mx.get('persistent'):
+            out['mixed_persistent_det_per_s'] = _r(mx['persistent']['value'])
     return out
 
 

@@ -132,6 +132,7 @@ typedef struct {
   int warm_r;       /* start == 2: anneals r >= warm_r start from m = 0 */
   const uint32_t* cdf; /* start == 2, or NULL: thresholds (B, D, 2) of sampled starts for anneals 0 < r < warm_r */
   const int32_t* ra;   /* or NULL: per-problem anneal counts (B); anneals r >= ra[b] are skipped */
+  int64_t* out_n1;     /* or NULL: Chord rounds with at least one flip per anneal (B, R) */
 } dd_ctx;
 
 /* Start spins of one anneal (arpeggio_ref59.py:44-49, arpeggio_fx.cu:48-57). s is P x D. */
@@ -200,7 +201,7 @@ static void dd_job(void* vctx, long t) {
     }
     w[i] = h[i] - 2 * acc;
   }
-  int64_t de = 0, best = (int64_t)1 << 62, flips = 0, tests = 0;
+  int64_t de = 0, best = (int64_t)1 << 62, flips = 0, tests = 0, n1 = 0;
   for (int k = 0; k < x->L; k++) {
     const int p = k % P;
     const uint32_t n = (uint32_t)(k / P);
@@ -235,6 +236,11 @@ static void dd_job(void* vctx, long t) {
         F[j] = lhs > rhs;
       }
       memset(pf, 0, (size_t)P * D);
+      for (int j = 0; j < D; j++)
+        if (F[j]) { /* n1: the round flips (arpeggio_ref59.py:74) */
+          n1++;
+          break;
+        }
       for (int j = 0; j < D; j++) {
         if (!F[j]) continue;
         int so = sp[j];
@@ -256,6 +262,7 @@ static void dd_job(void* vctx, long t) {
   x->out_de[t] = best;
   x->out_st[2 * t] = flips;
   x->out_st[2 * t + 1] = tests;
+  if (x->out_n1) x->out_n1[t] = n1;
 }
 
 /* G (B, D, D) row-major G[b][i][j]; h (B, D); T (L) one temperature per pass (pass k tests copy k % P);
@@ -268,6 +275,19 @@ int orc_anneal_dd(const int32_t* G, const int32_t* h, int B, int D, int P, int R
   if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6 || (P == 1 && start == 0)) || L < 1 || R < 1 || B < 0)
     return 1;
   dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, policy, out_s, out_de, out_st, NULL, 0, NULL, NULL};
+  orc_run(dd_job, &x, (long)B * R, nthreads);
+  return 0;
+}
+
+/* orc_anneal_dd's Chord round (policy 1) that also counts, per anneal, the rounds with at least one flip (n1 of
+ * arpeggio_ref59.anneal, rtl_a59/src/arpeggio_ref59.py:74): out_n1 (B, R). */
+int orc_anneal_chord_dd_n1(const int32_t* G, const int32_t* h, int B, int D, int P, int R, const int32_t* T,
+                           const int32_t* c, int L, int32_t q, const uint32_t* inst, uint32_t k0, uint32_t k1,
+                           int start, int8_t* out_s, int64_t* out_de, int64_t* out_st, int64_t* out_n1,
+                           int nthreads) {
+  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || L < 1 || R < 1 || B < 0) return 1;
+  dd_ctx x = {G, h, T, c, B, D, P, R, L, q, inst, k0, k1, start, 1, out_s, out_de, out_st, NULL, 0, NULL, NULL,
+              out_n1};
   orc_run(dd_job, &x, (long)B * R, nthreads);
   return 0;
 }

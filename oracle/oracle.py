@@ -53,6 +53,9 @@ def lib():
                                           ctypes.c_int, _P, _P, _P, ctypes.c_int]
         L.orc_anneal_chord_hw.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
                                           ctypes.c_int, ctypes.c_int32, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]
+        L.orc_anneal_chord_dd_n1.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
+                                             ctypes.c_int, ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_int, _P, _P, _P, _P, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -90,6 +93,28 @@ def anneal_dd(G, h, P, R, T, q, inst, key, start, policy='arpeggio', c=None, nth
     if rc:
         raise ValueError('orc_anneal_dd: unsupported shape')
     return out_s, out_de, out_st
+
+
+def anneal_chord_n1(G, h, P, R, T, c, q, inst, key, start, nthreads=1):
+    """anneal_dd's Chord round plus the rounds with at least one flip per anneal (n1 of arpeggio_ref59.anneal,
+    rtl_a59/src/arpeggio_ref59.py:74), the term of the Chord engine's latency 3 L + F + n1.  Returns spins, best
+    energy change, (flips, tests) and n1 (B, R) int64."""
+    G = np.ascontiguousarray(G, dtype=np.int32)
+    h = np.ascontiguousarray(h, dtype=np.int32)
+    B, D, _ = G.shape
+    T = np.ascontiguousarray([int(x) for x in T], dtype=np.int32)
+    cc = None if c is None else np.ascontiguousarray([int(x) for x in c], dtype=np.int32)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    out_s = np.zeros((B, R, P * D), dtype=np.int8)
+    out_de = np.zeros((B, R), dtype=np.int64)
+    out_st = np.zeros((B, R, 2), dtype=np.int64)
+    out_n1 = np.zeros((B, R), dtype=np.int64)
+    rc = lib().orc_anneal_chord_dd_n1(_ptr(G), _ptr(h), B, D, P, R, _ptr(T), _ptr(cc), len(T), int(q), _ptr(it),
+                                      key & MASK, (key >> 32) & MASK, 0 if start == 'rand' else 1, _ptr(out_s),
+                                      _ptr(out_de), _ptr(out_st), _ptr(out_n1), nthreads)
+    if rc:
+        raise ValueError('orc_anneal_chord_dd_n1: unsupported shape')
+    return out_s, out_de, out_st, out_n1
 
 
 def anneal_chord_hw(G, h, P, R, T, c, q, inst, key, nthreads=1):

@@ -22,6 +22,9 @@ Fixtures (all small, numpy .npz):
                       (x16 20 dB, x32 22 dB, x64 22 dB) for the BER-inside-CI gate (`... "$ARPEGGIO_REFERENCE" a513_points`).
   golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
                       (sim/a56an.py:74-108) on seeded per-use error vectors (`... "$ARPEGGIO_REFERENCE" stats`).
+  golden_cycles.json  the recorded single-lane engine latencies per K (data/results/a59/A59.json) and the x16 MDI
+                      point's model-F cost with its counters (data/results/a513/analysis.json P1)
+                      (`... "$ARPEGGIO_REFERENCE" cycles`).
 """
 import math
 import os
@@ -263,10 +266,25 @@ def stats_fixture():
     print('stats', lo, hi, r0, rlo, rhi, p)
 
 
+def cycles_fixture():
+    """The reference's recorded engine latencies and counters behind the cost models: data/results/a59/A59.json
+    (per K, RTL runs of both single-lane engines at A = 1: first-accept tests, flips and latency; Chord steps L,
+    flips, n1 and latency) and the model-F cost per anneal of its x16 MDI point P1 with the counters it was computed
+    from (data/results/a513/analysis.json: counters_fx, cost_per_anneal.fx)."""
+    import json
+    a59 = json.load(open(os.path.join(REF, 'data/results/a59/A59.json')))
+    keep = ('arpeggio_tests', 'arpeggio_F', 'arpeggio_lat', 'chord_L', 'chord_F', 'chord_n1', 'chord_lat')
+    out = {'a59': {pt: {K: {k: v[k] for k in keep} for K, v in a59[pt]['A1']['per_K'].items()} for pt in ('p1', 'p2')}}
+    a513 = json.load(open(os.path.join(REF, 'data/results/a513/analysis.json')))['points']['P1']
+    out['a513_P1'] = {'counters_fx': a513['counters_fx'], 'cost_per_anneal_fx': a513['cost_per_anneal']['fx']}
+    json.dump(out, open(os.path.join(OUT, 'golden_cycles.json'), 'w'), indent=1, sort_keys=True)
+    print('cycles', out['a513_P1']['cost_per_anneal_fx'])
+
+
 if __name__ == '__main__':
     if len(sys.argv) > 2:
         {'stats': stats_fixture, 'a513': a513_fixture, 'mapping': mapping_fixture,
-         'a513_points': a513_points_fixture}[sys.argv[2]]()
+         'a513_points': a513_points_fixture, 'cycles': cycles_fixture}[sys.argv[2]]()
         sys.exit(0)
     a513_fixture()
     a513_points_fixture()

@@ -39,6 +39,7 @@ SIGNATURES = {
     'arp_mdi_map': [_P, _P, _P, _I, _I, _I, _I, _P, _I, _I, _I, _P, _P, _P, _P, _P, _P],
     'arp_mdi_update': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P],
     'arp_mdi_select': [_P, _P, _I, _I, _I, _I, _P, _P, _P],
+    'arp_soft_trajectory': [_P, _P, _P, _P, _P, _P, _P, _F, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _P, _P],
     'arp_anneal_tune': [_I, _I, _I, _I, _I],
     'arp_anneal_first_accept_mixed': [_P, _I, _I, _U, _U, _I, _P, _P, _P],
     'arp_map_dd_soft': [_P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P],

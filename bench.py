@@ -259,7 +259,7 @@ def warm_vs_plain(args, dev, stream, rank):
            'warm_argmax': 'every anneal from the argmax class, all R anneals, at the warm budget',
            'points': {'x%d' % k: v for k, v in WARM_POINTS.items()}}
     for nt, B, snrs, full, R in ((32, args.batch, [18, 20, 22, 24], 32, 32),
-                                 (64, max(1024, args.batch // 2), [16, 18, 20, 22], 64, 64)):
+                                 (64, args.batch, [16, 18, 20, 22], 64, 64)):
         snr = torch.tensor([float(snrs[i % len(snrs)]) for i in range(B)])
         d = channel.draw_device(9000 + nt + rank, snr, B, nt, 16, dev=dev)
         bt = channel.levels_to_bits(d['l'], 16)
@@ -384,7 +384,7 @@ def equal_budget(args, dev, rank, nt=64, snrs=tuple(range(10, 25, 2)), R=64):
     chosen on the first 2048 uses; then both detect the whole batch (one-stage dDI, int32 fields)."""
     import torch
     from arpeggio_b200 import channel, detector, stats
-    B = max(2048, args.batch // 4)
+    B = max(2048, args.x64_batch)
     snr = torch.tensor([float(snrs[i % len(snrs)]) for i in range(B)])
     d = channel.draw_device(6000 + rank, snr, B, nt, 16, dev=dev)
     bt = channel.levels_to_bits(d['l'], 16)
@@ -595,7 +595,8 @@ def run_ours(args):
         for name, kw, Bx, ntx, snrs in (
                 ('chord_x32', dict(policy='chord', sweeps=None, T0=0.3, T1=0.3, q=0.4, start='rand'), B, 32,
                  w['snrs']),
-                ('arpeggio_x64', dict(policy='arpeggio', sweeps=64, T0=0.1, T1=0.1, q=0.0, start='bal'), 16384, 64,
+                ('arpeggio_x64', dict(policy='arpeggio', sweeps=64, T0=0.1, T1=0.1, q=0.0, start='bal'),
+                 args.x64_batch, 64,
                  list(range(10, 25, 2)))):
             sx = torch.tensor([snrs[i % len(snrs)] for i in range(Bx)], dtype=torch.float32)
             dx = data if ntx == 32 else channel.draw_device(5678 + rank, sx, Bx, ntx, w['M'], dev=dev)
@@ -826,6 +827,8 @@ def main():
     ap.add_argument('--chunks', type=int, default=4, help='pipelined pieces of the end-to-end step')
     ap.add_argument('--latency-frames', type=int, default=2000, help='single-frame replays for p50/p99 latency')
     ap.add_argument('--mdi-batch', type=int, default=16384, help='uses of the multi-stage (MDI) line; 0 skips it')
+    ap.add_argument('--x64-batch', type=int, default=262144,
+                    help='uses of the 64-user lines (the 64 x 64 configuration: 262144 channels)')
     ap.add_argument('--no-extras', dest='extras', action='store_false', help='skip the Chord and 64-user lines')
     ap.add_argument('--no-serve', dest='serve', action='store_false', help='skip the serving-loop block')
     ap.add_argument('--mixed', type=int, default=1_000_000, help='detections of the mixed-size graph block; 0 skips')

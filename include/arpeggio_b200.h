@@ -207,6 +207,19 @@ int arp_mdi_update(const float* H, const float* y, const int32_t* idx, int n, in
 int arp_mdi_select(const int8_t* cur, const float* dist, int B, int D, int G, int M, int8_t* levels, int8_t* bits,
                    void* stream);
 
+/* Trajectory soft output on the RI map (N = 2 D spins [s_MSB; s_LSB] for 16-QAM, N = D for QPSK; N <= 128):
+ * Chord's synchronous rule as a sampler of the detection posterior, mimo.chord_soft (arpeggio/mimo/mimo.py:332-394),
+ * with Philox draws of this library ((k >> 2, i, r, inst) word k & 3; start word 0 of (2^32 - 1, i, r, inst), or the
+ * spins s0 (B, N) if non-NULL).  J (B, N, N) scaled with a zero diagonal, hf (B, N) the exploration field (h0, or
+ * the RI field h), h0 (B, N), scale and c0 (B) with ||y - H x||^2 = scale E0(s) + c0, T (B, S) per-step temperatures,
+ * q, R chains of S steps.  Outputs: per bit (B, D nb, dimension-major, MSB first) the smallest distance of a
+ * visited state with the bit 0 (m0) and 1 (m1, +inf if none), the best distance (B) and its levels (B, D).  The LLRs
+ * follow from mimo.trajectory_llr (arpeggio_b200.soft.trajectory_llr). */
+int arp_soft_trajectory(const float* J, const float* hf, const float* h0, const float* scale, const float* c0,
+                        const float* T, const int8_t* s0, float q, int S, int R, int D, int M, int B,
+                        const uint32_t* inst, uint32_t k0, uint32_t k1, float* m0, float* m1, float* best_d,
+                        int8_t* best_l, void* stream);
+
 /* Autotuner hook (no reference counterpart): warps per block (1, 2, 4 or 8; 0 restores the occupancy heuristic)
  * of the compressed-problem anneal kernels for problems of D coordinates (by 32-wide slot count), P copies,
  * policy (0 first accept, incl. the warm variant; 1 Chord round) and precision (0 int32, 1 FP32 fields).

@@ -748,3 +748,160 @@ int orc_anneal_full_f32(const float* J, const float* h, const int8_t* s0, int B,
   orc_run(full_job, &x, (long)B * R, nthreads);
   return 0;
 }
+
+/* ------------------------------------------------------------------ trajectory soft output (RI map) */
+/* The sampler of mimo.chord_soft (arpeggio/mimo/mimo.py:332-394) with this project's Philox draws, restated as the
+ * device kernel computes it (one IEEE single operation per line): per chain, u = hf + 2 (sum_j J_ji s_j in j order),
+ * E0 = -sum over lanes (in the warp's butterfly order) of the lane partials -sum_t s_i (h0_i + (u_i - hf_i)/2); per
+ * step every spin tests z = s u + q < thr = (x/2^32 - 1/2) 4T (x: word k&3 of block (k>>2, i, r, inst)), the flips
+ * commit in index order (E0 += (+-2) ((h0_j - hf_j) + u_j), u_i += (-+4) J_ji), and after a step that flips (and step
+ * 0) d = scale E0 + c0 updates the per-bit minima and the chain's best (first minimum).  Chains are independent; the
+ * problem keeps the minima over its chains and the best state by (d, step, chain). */
+typedef struct {
+  const float *J, *hf, *h0, *scale, *c0, *T;
+  const int8_t* s0;
+  float q;
+  int S, R, N, D, M, B;
+  const uint32_t* inst;
+  uint32_t k0, k1;
+  float *cm0, *cm1, *cbest; /* per (b, r): minima (nbits each) and best d */
+  int *cstep;
+  int8_t* cbs;              /* per (b, r): best spins (N) */
+} soft_ctx;
+
+static float f_add(float a, float b) { volatile float r = a + b; return r; }
+static float f_sub(float a, float b) { volatile float r = a - b; return r; }
+static float f_mul(float a, float b) { volatile float r = a * b; return r; }
+
+static void soft_job(void* vctx, long t) {
+  const soft_ctx* x = (const soft_ctx*)vctx;
+  const int N = x->N, D = x->D, S = x->S, R = x->R, nb = x->M == 16 ? 2 : 1, nbits = D * nb;
+  const long b = t / R;
+  const uint32_t r = (uint32_t)(t % R), inst = x->inst[b];
+  const float* J = x->J + (size_t)b * N * N;
+  const float* hf = x->hf + (size_t)b * N;
+  const float* h0 = x->h0 + (size_t)b * N;
+  const float* Tb = x->T + (size_t)b * S;
+  int8_t s[128], cb[128];
+  float u[128], part[32];
+  for (int i = 0; i < N; i++) {
+    if (x->s0) s[i] = x->s0[(size_t)b * N + i] > 0 ? 1 : -1;
+    else s[i] = philox_word(0xFFFFFFFFu, (uint32_t)i, r, inst, x->k0, x->k1, 0) >= 0x80000000u ? 1 : -1;
+  }
+  for (int i = 0; i < N; i++) {
+    float acc = 0.0f;
+    for (int j = 0; j < N; j++) acc = f_add(acc, f_mul(J[(size_t)j * N + i], s[j] > 0 ? 1.0f : -1.0f));
+    u[i] = f_add(hf[i], f_mul(2.0f, acc));
+  }
+  for (int l = 0; l < 32; l++) {
+    float e = 0.0f;
+    for (int tt = 0; 32 * tt + l < N; tt++) {
+      const int i = 32 * tt + l;
+      const float si = s[i] > 0 ? 1.0f : -1.0f;
+      e = f_sub(e, f_mul(si, f_add(h0[i], f_mul(0.5f, f_sub(u[i], hf[i])))));
+    }
+    part[l] = e;
+  }
+  for (int o = 1; o < 32; o <<= 1) {
+    float nx[32];
+    for (int l = 0; l < 32; l++) nx[l] = f_add(part[l], part[l ^ o]);
+    memcpy(part, nx, sizeof nx);
+  }
+  float E = part[0];
+  float* m0 = x->cm0 + (size_t)t * nbits;
+  float* m1 = x->cm1 + (size_t)t * nbits;
+  for (int k = 0; k < nbits; k++) m0[k] = m1[k] = INFINITY;
+  float best = INFINITY;
+  int bstep = INT32_MAX;
+  memcpy(cb, s, (size_t)N);
+  uint8_t F[128];
+  for (int k = 0; k < S; k++) {
+    const float A = f_mul(4.0f, Tb[k]);
+    int any = 0;
+    for (int i = 0; i < N; i++) {
+      const uint32_t w = philox_word((uint32_t)(k >> 2), (uint32_t)i, r, inst, x->k0, x->k1, k & 3);
+      const float thr = orc_thr(w, A);
+      const float su = s[i] > 0 ? u[i] : -u[i];
+      F[i] = f_add(su, x->q) < thr;
+      any |= F[i];
+    }
+    for (int j = 0; j < N; j++) {
+      if (!F[j]) continue;
+      const int up = s[j] > 0;
+      E = f_add(E, f_mul(up ? 2.0f : -2.0f, f_add(f_sub(h0[j], hf[j]), u[j])));
+      const float cf = up ? -4.0f : 4.0f;
+      for (int i = 0; i < N; i++) u[i] = f_add(u[i], f_mul(cf, J[(size_t)j * N + i]));
+    }
+    for (int j = 0; j < N; j++)
+      if (F[j]) s[j] = (int8_t)(-s[j]);
+    if (any || k == 0) {
+      const float d = f_add(f_mul(x->scale[b], E), x->c0[b]);
+      for (int j = 0; j < D; j++) {
+        const int s1 = s[j] > 0;
+        if (nb == 2) {
+          const int b2 = s1 != (s[D + j] > 0);
+          if (s1) { if (d < m1[2 * j]) m1[2 * j] = d; } else { if (d < m0[2 * j]) m0[2 * j] = d; }
+          if (b2) { if (d < m1[2 * j + 1]) m1[2 * j + 1] = d; } else { if (d < m0[2 * j + 1]) m0[2 * j + 1] = d; }
+        } else {
+          if (s1) { if (d < m1[j]) m1[j] = d; } else { if (d < m0[j]) m0[j] = d; }
+        }
+      }
+      if (d < best) {
+        best = d;
+        bstep = k;
+        memcpy(cb, s, (size_t)N);
+      }
+    }
+  }
+  x->cbest[t] = best;
+  x->cstep[t] = bstep;
+  memcpy(x->cbs + (size_t)t * N, cb, (size_t)N);
+}
+
+/* J (B, N, N), hf, h0 (B, N), scale, c0 (B), T (B, S), s0 (B, N) or NULL; N = 2 D (M = 16) or D (M = 4).  Outputs
+ * m0, m1 (B, D nb), best_d (B), best_l (B, D). */
+int orc_soft_trajectory(const float* J, const float* hf, const float* h0, const float* scale, const float* c0,
+                        const float* T, const int8_t* s0, float q, int S, int R, int D, int M, int B,
+                        const uint32_t* inst, uint32_t k0, uint32_t k1, float* m0, float* m1, float* best_d,
+                        int8_t* best_l, int nthreads) {
+  if (!(M == 4 || M == 16)) return 1;
+  const int N = M == 16 ? 2 * D : D, nb = M == 16 ? 2 : 1, nbits = D * nb;
+  if (N < 1 || N > 128 || R < 1 || S < 1 || B < 0) return 1;
+  const long BR = (long)B * R;
+  float* cm0 = (float*)malloc(sizeof(float) * (size_t)BR * nbits);
+  float* cm1 = (float*)malloc(sizeof(float) * (size_t)BR * nbits);
+  float* cbest = (float*)malloc(sizeof(float) * (size_t)BR);
+  int* cstep = (int*)malloc(sizeof(int) * (size_t)BR);
+  int8_t* cbs = (int8_t*)malloc((size_t)BR * N);
+  soft_ctx x = {J, hf, h0, scale, c0, T, s0, q, S, R, N, D, M, B, inst, k0, k1, cm0, cm1, cbest, cstep, cbs};
+  orc_run(soft_job, &x, BR, nthreads);
+  for (int b = 0; b < B; b++) {
+    int br = 0;
+    for (int k = 0; k < nbits; k++) {
+      float v0 = INFINITY, v1 = INFINITY;
+      for (int r = 0; r < R; r++) {
+        const long t = (long)b * R + r;
+        if (cm0[t * nbits + k] < v0) v0 = cm0[t * nbits + k];
+        if (cm1[t * nbits + k] < v1) v1 = cm1[t * nbits + k];
+      }
+      m0[(size_t)b * nbits + k] = v0;
+      m1[(size_t)b * nbits + k] = v1;
+    }
+    for (int r = 1; r < R; r++) {
+      const long t = (long)b * R + r, tb = (long)b * R + br;
+      if (cbest[t] < cbest[tb] || (cbest[t] == cbest[tb] && cstep[t] < cstep[tb])) br = r;
+    }
+    const long tb = (long)b * R + br;
+    best_d[b] = cbest[tb];
+    for (int j = 0; j < D; j++) {
+      const int s1 = cbs[tb * N + j];
+      best_l[(size_t)b * D + j] = (int8_t)(nb == 2 ? 2 * s1 + cbs[tb * N + D + j] : s1);
+    }
+  }
+  free(cm0);
+  free(cm1);
+  free(cbest);
+  free(cstep);
+  free(cbs);
+  return 0;
+}

@@ -53,6 +53,9 @@ def lib():
                                           ctypes.c_int, _P, _P, _P, ctypes.c_int]
         L.orc_anneal_chord_hw.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
                                           ctypes.c_int, ctypes.c_int32, _P, ctypes.c_uint64, _P, _P, _P, ctypes.c_int]
+        L.orc_soft_trajectory.argtypes = [_P, _P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, ctypes.c_uint32,
+                                          ctypes.c_uint32, _P, _P, _P, _P, ctypes.c_int]
         L.orc_anneal_chord_dd_n1.argtypes = [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P,
                                              ctypes.c_int, ctypes.c_int32, _P, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_int, _P, _P, _P, _P, ctypes.c_int]
@@ -115,6 +118,29 @@ def anneal_chord_n1(G, h, P, R, T, c, q, inst, key, start, nthreads=1):
     if rc:
         raise ValueError('orc_anneal_chord_dd_n1: unsupported shape')
     return out_s, out_de, out_st, out_n1
+
+
+def soft_trajectory(J, hf, h0, scale, c0, T, s0, q, S, R, D, M, inst, key, nthreads=1):
+    """The trajectory sampler of mimo.chord_soft (arpeggio/mimo/mimo.py:332-394) with this project's Philox draws,
+    restated operation for operation as the device computes it.  Returns m0, m1 (B, D nb), best_d (B), best_l
+    (B, D)."""
+    J = np.ascontiguousarray(J, dtype=np.float32)
+    B = J.shape[0]
+    nb = 2 if M == 16 else 1
+    arr = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    hf, h0, scale, c0, T = arr(hf), arr(h0), arr(scale), arr(c0), arr(T)
+    s0 = None if s0 is None else np.ascontiguousarray(s0, dtype=np.int8)
+    it = np.ascontiguousarray(np.asarray(inst, dtype=np.int64) & MASK, dtype=np.uint32)
+    m0 = np.zeros((B, D * nb), dtype=np.float32)
+    m1 = np.zeros((B, D * nb), dtype=np.float32)
+    bd = np.zeros(B, dtype=np.float32)
+    bl = np.zeros((B, D), dtype=np.int8)
+    rc = lib().orc_soft_trajectory(_ptr(J), _ptr(hf), _ptr(h0), _ptr(scale), _ptr(c0), _ptr(T), _ptr(s0), float(q),
+                                   S, R, D, M, B, _ptr(it), key & MASK, (key >> 32) & MASK, _ptr(m0), _ptr(m1),
+                                   _ptr(bd), _ptr(bl), nthreads)
+    if rc:
+        raise ValueError('orc_soft_trajectory: unsupported shape')
+    return m0, m1, bd, bl
 
 
 def anneal_chord_hw(G, h, P, R, T, c, q, inst, key, nthreads=1):

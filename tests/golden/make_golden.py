@@ -22,6 +22,8 @@ Fixtures (all small, numpy .npz):
                       (x16 20 dB, x32 22 dB, x64 22 dB) for the BER-inside-CI gate (`... "$ARPEGGIO_REFERENCE" a513_points`).
   golden_stats.npz    stats_chord.boot_ber (sim/stats_chord.py:58-66), a56an.boot_ratio and a56an.mcnemar
                       (sim/a56an.py:74-108) on seeded per-use error vectors (`... "$ARPEGGIO_REFERENCE" stats`).
+  golden_trajectory.npz  mimo.trajectory_llr (mimo.py:397-413) on seeded trajectory minima, 16-QAM and QPSK
+                      (`... "$ARPEGGIO_REFERENCE" trajectory`).
   golden_cycles.json  the recorded single-lane engine latencies per K (data/results/a59/A59.json) and the x16 MDI
                       point's model-F cost with its counters (data/results/a513/analysis.json P1)
                       (`... "$ARPEGGIO_REFERENCE" cycles`).
@@ -266,6 +268,36 @@ def stats_fixture():
     print('stats', lo, hi, r0, rlo, rhi, p)
 
 
+def trajectory_fixture():
+    """mimo.trajectory_llr (mimo.py:397-413, with list_llr :434-462) on seeded inputs shaped as chord_soft returns
+    them: best levels with their distances, per-bit trajectory minima m0/m1 (some bits never seen with one of their
+    values: +inf), the MMSE decision; 16-QAM and QPSK, scalar N0, clip 1e4 (softlib.BIG)."""
+    import mimo
+    out = {}
+    for M, nt in ((16, 8), (4, 16)):
+        b = arpx.draw(901 + M, 10.0, 0, 24, nt, M, dev='cpu')
+        B, D = b['H'].shape[0], b['H'].shape[2]
+        g = torch.Generator().manual_seed(31 + M)
+        lv = torch.tensor(mimo.PAM[M]['levels'], dtype=torch.float32)
+        best_l = lv[torch.randint(0, len(lv), (B, D), generator=g)]
+        mm = lv[torch.randint(0, len(lv), (B, D), generator=g)]
+        mm = torch.where(torch.rand(B, D, generator=g) < 0.7, best_l, mm)
+        best_d = mimo.dist(b, best_l[:, None, :])[:, 0]
+        nbits = D * mimo.PAM[M]['bits']
+        m0 = best_d[:, None] * (1 + 2 * torch.rand(B, nbits, generator=g))
+        m1 = best_d[:, None] * (1 + 2 * torch.rand(B, nbits, generator=g))
+        m0 = torch.where(torch.rand(B, nbits, generator=g) < 0.15, torch.full_like(m0, float('inf')), m0)
+        m1 = torch.where(torch.rand(B, nbits, generator=g) < 0.15, torch.full_like(m1, float('inf')), m1)
+        l_hat, llr = mimo.trajectory_llr(b, best_l, best_d, m0, m1, mm, clip=1e4)
+        tag = 'M%d' % M
+        for k, v in (('H', b['H']), ('y', b['y']), ('best_l', best_l), ('best_d', best_d), ('m0', m0), ('m1', m1),
+                     ('mmse', mm), ('l_hat', l_hat), ('llr', llr)):
+            out['%s/%s' % (tag, k)] = v.numpy()
+        out[tag + '/N0'] = np.array([float(b['N0'])])
+    np.savez_compressed(os.path.join(OUT, 'golden_trajectory.npz'), **out)
+    print('trajectory', {k: v.shape for k, v in out.items() if k.endswith('llr')})
+
+
 def cycles_fixture():
     """The reference's recorded engine latencies and counters behind the cost models: data/results/a59/A59.json
     (per K, RTL runs of both single-lane engines at A = 1: first-accept tests, flips and latency; Chord steps L,
@@ -284,7 +316,8 @@ def cycles_fixture():
 if __name__ == '__main__':
     if len(sys.argv) > 2:
         {'stats': stats_fixture, 'a513': a513_fixture, 'mapping': mapping_fixture,
-         'a513_points': a513_points_fixture, 'cycles': cycles_fixture}[sys.argv[2]]()
+         'a513_points': a513_points_fixture, 'cycles': cycles_fixture,
+         'trajectory': trajectory_fixture}[sys.argv[2]]()
         sys.exit(0)
     a513_fixture()
     a513_points_fixture()

@@ -318,11 +318,12 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
   float qmax = 0.0f;
   const float s2 = a.xg ? 0.0f : a.sigma2[b];  // only the MMSE solve reads sigma2 (null for a given guess)
 #pragma unroll
+  for (int i = 0; i < TB; ++i) lds_vec<TB>(Qs + (ty * TB + i) * QP + tx * TB, A[i]);  // TB floats per access
+#pragma unroll
   for (int i = 0; i < TB; ++i)
 #pragma unroll
     for (int j = 0; j < TB; ++j) {
       const int gi = ty * TB + i, gj = tx * TB + j;
-      A[i][j] = Qs[gi * QP + gj];
       qmax = fmaxf(qmax, fabsf(A[i][j]));
       if (gi == gj) A[i][j] = gi < D ? __fadd_rn(A[i][j], s2) : 1.0f;
     }
@@ -377,16 +378,14 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
       }
     }
     // ---- z = A^-1 g, mu = diag(A^-1 Q) (Q symmetric: sum_j Ainv_ij Q_ij), x_q
-    float zp[TB], mp[TB];
+    float zp[TB], mp[TB], gj[TB];
+    lds_vec<TB>(gv + tx * TB, gj);
 #pragma unroll
     for (int i = 0; i < TB; ++i) {
-      float ar[TB], gj[TB], qj[TB];
+      float ar[TB], qj[TB];
+      lds_vec<TB>(Qs + (ty * TB + i) * QP + tx * TB, qj);
 #pragma unroll
-      for (int j = 0; j < TB; ++j) {
-        ar[j] = A[i][j];
-        gj[j] = gv[tx * TB + j];
-        qj[j] = Qs[(ty * TB + i) * QP + tx * TB + j];
-      }
+      for (int j = 0; j < TB; ++j) ar[j] = A[i][j];
       zp[i] = row_dot<TB>(ar, gj);
       mp[i] = row_dot<TB>(ar, qj);
     }
@@ -466,15 +465,12 @@ __global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
     return;
   }
   // ---- h = 2 (g - Q x_q), scale = max(|h|, |Q|)
-  float hp[TB];
+  float hp[TB], xj[TB];
+  lds_vec<TB>(xv + tx * TB, xj);
 #pragma unroll
   for (int i = 0; i < TB; ++i) {
-    float qj[TB], xj[TB];
-#pragma unroll
-    for (int j = 0; j < TB; ++j) {
-      qj[j] = Qs[(ty * TB + i) * QP + tx * TB + j];
-      xj[j] = xv[tx * TB + j];
-    }
+    float qj[TB];
+    lds_vec<TB>(Qs + (ty * TB + i) * QP + tx * TB, qj);
     hp[i] = row_dot<TB>(qj, xj);
     hp[i] = __fmul_rn(2.0f, __fsub_rn(gv[ty * TB + i], hp[i]));
     if (ty * TB + i < D) qmax = fmaxf(qmax, fabsf(hp[i]));

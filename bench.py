@@ -769,9 +769,11 @@ def summary(line):
             e = {'det_per_s': _r(v['value'], 4)}
             if 'speedup_vs_plain' in v:
                 e['x_plain'] = _r(v['speedup_vs_plain'])
+            if name in ('warm_argmax', 'warm_fast') and wl == 'x64':
+                continue  # ablations and the second budget: in the full line only
             if 'ber_ratio_vs_plain' in v and name != 'warm_argmax':  # the ablation: speed-up only
                 e['ber_ratio_ci'] = {k.replace(' ', ''): [_r(c) for c in ci] for k, ci in v['ber_ratio_vs_plain'].items()}
-            if 'frame_latency' in v:
+            if 'frame_latency' in v and name in ('plain', 'warm'):
                 e['frame_us_p50_p99'] = [_r(v['frame_latency']['p50_us']), _r(v['frame_latency']['p99_us'])]
             o[name] = e
         out['warm_vs_plain_' + wl] = o

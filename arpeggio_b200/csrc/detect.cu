@@ -134,8 +134,11 @@ __device__ __forceinline__ void digits4(int32_t x, int32_t (&d)[4]) {
   d[3] = x;
 }
 
+// Register bounds for more resident blocks (the Gauss-Jordan steps are barrier-latency bound, so blocks overlap):
+// four per SM at 32 users (64 registers, a few spilled: 3.95 -> 3.73 ms per 65536 uses), two per SM at 64 users
+// (126 registers: 28.8 -> 19.3 ms per 65536 uses); the same outputs bit for bit.
 template <int TB, int GS>
-__global__ void __launch_bounds__(GS * GS) k_map_dd(const MapParams a) {
+__global__ void __launch_bounds__(GS * GS, TB == 8 ? 2 : (TB == 4 ? 4 : 1)) k_map_dd(const MapParams a) {
   constexpr int Dp = GS * TB, QP = Dp + 4, NT = GS * GS;
   constexpr int CH = kChunkRows<Dp>(), MP = kMmaM<Dp>(), KG = CH / 16, PB = kPlaneBytes<Dp>();
   constexpr uint32_t NCOL = kTmemCols<Dp>();

@@ -335,9 +335,14 @@ __device__ __forceinline__ uint32_t eng_xs32(uint32_t x) {
   return x;
 }
 
-#ifndef ARP_ANNEAL_MINB
-#define ARP_ANNEAL_MINB 1
-#endif
+// Resident 256-thread blocks per SM that the integer anneal's registers are bounded for: four slots (D > 96) at two
+// blocks (128 registers: four 4-warp blocks per SM instead of three, no spills; 64 users: 129 -> 120 ms per 32768
+// uses); one slot at P <= 4 and two slots at P = 2 at four blocks (64 registers, no spills; 32 users: anneal
+// 32.7 -> 31.7 ms per 65536 uses); the rest unbounded (64 registers would spill there).
+template <int NS, int P>
+constexpr int anneal_min_blocks() {
+  return NS >= 4 ? 2 : ((NS == 1 && P <= 4) || (NS == 2 && P == 2)) ? 4 : 1;
+}
 
 // ENG (Chord only): the engine's own numbers instead of Philox -- lane j's xorshift32 state starts from the anneal's
 // seed chain (engine_model.cpp:185-194, 170-184, 142-163), its bits 31, 30, ... give the start spins of copies
@@ -656,13 +661,36 @@ __device__ __forceinline__ void anneal_int_problem(const DDParams& a, const Phil
 }
 
 template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false, bool ENG = false>
-// Four slots (D > 96) are bounded at 128 registers: four 4-warp blocks per SM instead of three (no spills;
-// 64 users: 129 -> 120 ms per 32768 uses).
-__global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_int(const DDParams a) {
+__global__ void __launch_bounds__(256, anneal_min_blocks<NS, P>()) k_anneal_int(const DDParams a) {
   const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
   pdl_trigger();
   pdl_wait();
   anneal_int_problem<NS, P, CHORD, CACHE, WARM, ENG>(a, *reinterpret_cast<const PhiloxKeys*>(a.rk0), b, bs);
+}
+
+// The same anneal without the register bound, for batches too small to fill the GPU (a frame's chain): no other
+// block waits for the SM there, and with its registers unbounded each anneal runs faster (one 32-user frame:
+// 91.5 -> 85.2 us p50 against the bounded kernel).  The explicit minimum of one block matters: with the thread
+// bound alone ptxas settles on fewer registers and spills.
+template <int NS, int P, bool CHORD, bool CACHE, bool WARM = false, bool ENG = false>
+__global__ void __launch_bounds__(256, 1) k_anneal_int_lat(const DDParams a) {
+  const int split = a.split, b = blockIdx.x / split, bs = blockIdx.x - b * split;
+  pdl_trigger();
+  pdl_wait();
+  anneal_int_problem<NS, P, CHORD, CACHE, WARM, ENG>(a, *reinterpret_cast<const PhiloxKeys*>(a.rk0), b, bs);
+}
+
+using AnnealKernel = void (*)(const DDParams);
+
+template <int NS, int P, bool CHORD, bool FLT, bool WARM, bool ENG, bool LAT>
+static AnnealKernel anneal_kernel() {
+  constexpr bool CACHE = P * NS <= 8;
+  if constexpr (FLT)
+    return k_anneal_dd<NS, P, CHORD, true, CACHE>;
+  else if constexpr (LAT)
+    return k_anneal_int_lat<NS, P, CHORD, CACHE, WARM, ENG>;
+  else
+    return k_anneal_int<NS, P, CHORD, CACHE, WARM, ENG>;
 }
 
 // Warps per block: a block holds one problem and its warps share the anneals, so fewer warps per block let
@@ -688,10 +716,12 @@ static int pick_warps(K kern, size_t smem, int R) {
 // heuristic.  Process-wide, set through arp_anneal_tune.
 static int g_tuned_warps[5][7][2][2];
 
-template <int NS, int P, bool CHORD, bool FLT, bool WARM = false, bool ENG = false>
+template <int NS, int P, bool CHORD, bool FLT, bool WARM = false, bool ENG = false, bool LAT = false>
 static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
-  constexpr bool CACHE = P * NS <= 8;
-  auto kern = FLT ? k_anneal_dd<NS, P, CHORD, true, CACHE> : k_anneal_int<NS, P, CHORD, CACHE, WARM, ENG>;
+  if constexpr (!FLT && !LAT && anneal_min_blocks<NS, P>() > 1) {
+    if (a.B <= kPdlMaxB) return launch_ns_p<NS, P, CHORD, FLT, WARM, ENG, true>(a, warps, st);
+  }
+  const AnnealKernel kern = anneal_kernel<NS, P, CHORD, FLT, WARM, ENG, LAT>();
   const size_t smem = (size_t)a.D * NS * 32 * 4;
   // Launch settings per device (the shared-memory limit raised by cudaFuncSetAttribute applies to the current
   // device only; occupancy and SM count are per device too), behind one lock per instantiation.
@@ -940,8 +970,9 @@ struct MixedArgs {
   DDParams cls[kMaxMixed];
 };
 
+// Bounds as the per-class anneal's, but two slots unbounded: with the work loop around it, 64 registers spill there.
 template <int NS>
-__global__ void __launch_bounds__(256, NS >= 4 ? 2 : ARP_ANNEAL_MINB) k_anneal_mixed(const __grid_constant__ MixedArgs g) {
+__global__ void __launch_bounds__(256, NS == 2 ? 1 : anneal_min_blocks<NS, 2>()) k_anneal_mixed(const __grid_constant__ MixedArgs g) {
   __shared__ int s_item;
   for (;;) {
     __syncthreads();  // the previous problem's shared memory is no longer read

@@ -24,6 +24,15 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
 
+// Shared-memory descriptor of a 128-byte-swizzled operand, the layout a 2D TMA tile load with 128-byte swizzle
+// writes (rows of 128 bytes, 16-byte chunk c of row r stored at chunk c ^ (r % 8), 8-row atoms of 1024 bytes that
+// start 1024-byte aligned).  K-major: SBO = 1024 (8-row groups), LBO unused, the start advanced 32 bytes per
+// K = 16 step inside the 128-byte rows.  MN-major (rows = k, 64 elements of M or N per row): SBO = 1024 between
+// 8-k groups, LBO = the distance between 64-element blocks of M or N, the start advanced 2048 bytes per K = 16.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return sdesc(saddr, lbo, sbo) | ((uint64_t)2 << 61);
+}
+
 // Instruction descriptor, kind::f16: bf16 x bf16 -> f32 accumulate, M = 128, N (16..256, step 16).
 __host__ __device__ constexpr uint32_t idesc_bf16(int N, bool a_mn, bool b_mn) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
@@ -73,6 +82,26 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(su32(bar))
                : "memory");
+}
+
+// One 2D tiled TMA load (no multicast): the box at element coordinates (x, y) of the tensor map (a kernel
+// parameter) into shared memory at dst; completes the box's bytes on the mbarrier (zero fill outside the tensor).
+// x times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst),
+      "l"(tmap), "r"(x), "r"(y), "r"(su32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch(const void* tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
+}
+
+// One arrival on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void cp16(uint32_t dst, const void* src, bool valid) {

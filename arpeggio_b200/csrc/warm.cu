@@ -6,7 +6,9 @@
 //                 canonical no-swizzle shared-memory layouts (K-major or MN-major per operand, so forward and
 //                 both backward products use the same kernel), a 4-slot ring whose slots are released by
 //                 tcgen05.commit on per-slot mbarriers; fused epilogues (bias + ReLU to bf16, bias to f32,
-//                 ReLU-mask to bf16, f32 store, f32 accumulate for split K) read TMEM with tcgen05.ld.
+//                 ReLU-mask to bf16, f32 store, f32 accumulate for split K) read TMEM with tcgen05.ld.  It serves
+//                 the small products (M < 128, N < 64 or K < 64); the large ones go to the TMA-fed,
+//                 warp-specialised kernel of gemm_tma.cu, which shares the epilogues (gemm.cuh).
 //   k_warm_features  per-coordinate features of a mapped dDI problem (and training labels).
 //   k_warm_loss      softmax cross-entropy over the P+1 classes of the spin sum, its gradient in bf16.
 //   k_colsum_bf16    bias gradients.
@@ -18,26 +20,10 @@
 
 #include "../../include/arpeggio_b200.h"
 #include "arp_common.cuh"
+#include "gemm.cuh"
 #include "umma.cuh"
 
 namespace arp {
-
-using bf16 = __nv_bfloat16;
-
-struct GemmParams {
-  const bf16* A;
-  const bf16* B;
-  int lda, ldb;
-  int M, N, K;
-  int epi;
-  const float* bias;
-  const bf16* aux;
-  int ldaux;
-  void* C;
-  int ldc;
-  int kt_per;  // k tiles (of 64) per split
-  int32_t* status;
-};
 
 constexpr int kStages = 4;
 
@@ -66,63 +52,6 @@ __device__ __forceinline__ void load_tile(uint32_t sbase, const bf16* g, int ld,
     }
     const bool valid = mn < mnlim && k < K;
     umma::cp16(sbase + off, valid ? (const void*)src : (const void*)g, valid);
-  }
-}
-
-enum { EPI_F32 = 0, EPI_F32_ACC = 1, EPI_BIAS_RELU_BF16 = 2, EPI_BIAS_F32 = 3, EPI_MASK_BF16 = 4 };
-// Internal: split z of a split-K product stores its partial tile at C + z M ldc (summed afterwards in split order).
-constexpr int EPI_F32_PART = 5;
-
-template <int CW>
-__device__ __forceinline__ void epilogue(const GemmParams& p, int row, int n, const uint32_t (&v)[32]) {
-#pragma unroll
-  for (int g = 0; g < CW; g += 16) {
-    const int nn = n + g;
-    if (nn >= p.N) break;
-    float f[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) f[i] = __uint_as_float(v[g + i]);
-    if (p.epi == EPI_F32 || p.epi == EPI_BIAS_F32 || p.epi == EPI_F32_PART) {
-      if (p.epi == EPI_BIAS_F32)
-#pragma unroll
-        for (int i = 0; i < 16; ++i) f[i] += p.bias[nn + i];
-      float* base = reinterpret_cast<float*>(p.C);
-      if (p.epi == EPI_F32_PART) base += (size_t)blockIdx.z * p.M * p.ldc;
-      float4* o = reinterpret_cast<float4*>(base + (size_t)row * p.ldc + nn);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) o[i] = make_float4(f[4 * i], f[4 * i + 1], f[4 * i + 2], f[4 * i + 3]);
-    } else if (p.epi == EPI_F32_ACC) {
-      float* o = reinterpret_cast<float*>(p.C) + (size_t)row * p.ldc + nn;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) atomicAdd(o + i, f[i]);
-    } else {
-      if (p.epi == EPI_BIAS_RELU_BF16) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) f[i] = fmaxf(f[i] + p.bias[nn + i], 0.0f);
-      } else {  // EPI_MASK_BF16: ReLU backward through the stored activation
-        const uint4* ax = reinterpret_cast<const uint4*>(p.aux + (size_t)row * p.ldaux + nn);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const uint4 u = ax[q];
-          const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
-            if (!(__low2float(h2) > 0.0f)) f[8 * q + 2 * i] = 0.0f;
-            if (!(__high2float(h2) > 0.0f)) f[8 * q + 2 * i + 1] = 0.0f;
-          }
-        }
-      }
-      uint32_t pk[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
-        pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
-      }
-      uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(p.C) + (size_t)row * p.ldc + nn);
-      o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-      o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-    }
   }
 }
 
@@ -215,7 +144,7 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const GemmParams p) {
         umma::tmem_ld32(ta, v);
       else
         umma::tmem_ld16(ta, v);
-      if (row < p.M) epilogue<CW>(p, row, n0 + c, v);
+      if (row < p.M) epilogue<CW>(p, row, n0 + c, v, blockIdx.z);
     }
   } else if (tid == 0) {
     set_status(p.status, ARP_ERR_TIMEOUT);
@@ -231,10 +160,26 @@ __global__ void __launch_bounds__(256) k_sum_splits(const float* __restrict__ pa
   const size_t mn = (size_t)M * N;
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < mn; x += (size_t)gridDim.x * blockDim.x) {
     float acc = 0.0f;
-    for (int z = 0; z < splits; ++z) acc += part[(size_t)z * mn + x];
+    int z = 0;
+    for (; z + 8 <= splits; z += 8) {  // eight loads in flight, added in split order
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = part[(size_t)(z + u) * mn + x];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc += v[u];
+    }
+    for (; z < splits; ++z) acc += part[(size_t)z * mn + x];
     const size_t i = x / N, j = x - i * N;
     C[i * ldc + j] += acc;
   }
+}
+
+cudaError_t sum_splits(const float* ws, int splits, int M, int N, float* C, int ldc, cudaStream_t st) {
+  const size_t mn = (size_t)M * N;
+  const int th = 256;
+  const int nb = (int)((mn + th - 1) / th);
+  k_sum_splits<<<nb < 4096 ? nb : 4096, th, 0, st>>>(ws, splits, M, N, C, ldc);
+  return cudaGetLastError();
 }
 
 template <int BN, bool AMN, bool BMN>
@@ -273,12 +218,7 @@ static cudaError_t launch_gemm(GemmParams p, cudaStream_t st) {
   q.ldc = p.N;
   k_gemm_bf16<BN, AMN, BMN><<<grid, 128, smem, st>>>(q);
   e = cudaGetLastError();
-  if (e == cudaSuccess) {
-    const int th = 256;
-    const int nb = (int)((mn + th - 1) / th);
-    k_sum_splits<<<nb < 4096 ? nb : 4096, th, 0, st>>>(ws, split, p.M, p.N, reinterpret_cast<float*>(p.C), p.ldc);
-    e = cudaGetLastError();
-  }
+  if (e == cudaSuccess) e = sum_splits(ws, split, p.M, p.N, reinterpret_cast<float*>(p.C), p.ldc, st);
   const cudaError_t ef = cudaFreeAsync(ws, st);
   return e != cudaSuccess ? e : ef;
 }
@@ -884,15 +824,18 @@ extern "C" int arp_gemm_bf16(const void* A, int a_mn_major, int lda, const void*
                status};
   const bool amn = a_mn_major != 0, bmn = b_mn_major != 0;
   cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e;
-  if (N <= 16)
-    e = gemm_bn<16>(p, amn, bmn, st);
-  else if (N <= 64)
-    e = gemm_bn<64>(p, amn, bmn, st);
-  else if (N <= 128)
-    e = gemm_bn<128>(p, amn, bmn, st);
-  else
-    e = gemm_bn<256>(p, amn, bmn, st);
+  // the large products: TMA-fed, warp-specialised; the rest (or no tensor-map encoder): the cp.async kernel
+  cudaError_t e = gemm_tma_fits(p) ? gemm_tma(p, amn, bmn, st) : cudaErrorNotSupported;
+  if (e == cudaErrorNotSupported) {
+    if (N <= 16)
+      e = gemm_bn<16>(p, amn, bmn, st);
+    else if (N <= 64)
+      e = gemm_bn<64>(p, amn, bmn, st);
+    else if (N <= 128)
+      e = gemm_bn<128>(p, amn, bmn, st);
+    else
+      e = gemm_bn<256>(p, amn, bmn, st);
+  }
   return e == cudaSuccess ? ARP_OK : ARP_ERR_LAUNCH;
 }
 

@@ -377,6 +377,55 @@ def _profile_main(argv):
     print('stages ms (map, warm start, anneal, readout):', [round(ev[i].elapsed_time(ev[i + 1]), 3) for i in range(4)])
 
 
+def _gemm_main(argv):
+    """python -m arpeggio_b200.warm gemm --rows R --width W [--reps N]: times the network's three large training
+    products at R rows and hidden width W -- forward (H W^T, bias + ReLU to bf16), input gradient (dY W, ReLU mask)
+    and weight gradient (dY^T H, split-K accumulation) -- each replayed N times in a CUDA graph; prints the device
+    time and TFLOP/s of each."""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument('mode', choices=['gemm'])
+    ap.add_argument('--rows', type=int, default=32768)
+    ap.add_argument('--width', type=int, default=512)
+    ap.add_argument('--reps', type=int, default=20)
+    a = ap.parse_args(argv)
+    g = torch.Generator().manual_seed(0)
+    R, W = a.rows, a.width
+    X = (torch.randn(R, W, generator=g) * 0.5).to(torch.bfloat16).cuda()
+    Wt = (torch.randn(W, W, generator=g) * 0.05).to(torch.bfloat16).cuda()
+    dY = (torch.randn(R, W, generator=g) * 0.5).to(torch.bfloat16).cuda()
+    bias = torch.randn(W, generator=g).cuda()
+    H = torch.empty(R, W, dtype=torch.bfloat16, device='cuda')
+    Gw = torch.zeros(W, W, device='cuda')
+    st = torch.zeros(1, dtype=torch.int32, device='cuda')
+    cases = [('forward', lambda: gemm(X, 0, W, Wt, 0, W, R, W, W, EPI_RELU_BF16, H, W, bias=bias, status=st)),
+             ('input gradient', lambda: gemm(dY, 0, W, Wt, 1, W, R, W, W, EPI_MASK_BF16, H, W, aux=X, ld_aux=W,
+                                             status=st)),
+             ('weight gradient', lambda: gemm(dY, 1, W, X, 1, W, W, W, R, EPI_ACC, Gw, W, status=st))]
+    for name, f in cases:
+        for _ in range(3):
+            f()
+        torch.cuda.synchronize()
+        s = torch.cuda.Stream()
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr, stream=s):
+            for _ in range(a.reps):
+                f()
+        gr.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        gr.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        if int(st.item()) != 0:
+            raise _lib.ArpError('gemm status %d' % int(st.item()))
+        us = 1e3 * e0.elapsed_time(e1) / a.reps
+        print('%-16s %d x %d x %d: %8.1f us  %6.1f TFLOP/s' % (name, R, W, W, us, 2.0 * R * W * W / us / 1e6))
+
+
 if __name__ == '__main__':
     import sys
-    _profile_main(sys.argv[1:])
+    if sys.argv[1:2] == ['gemm']:
+        _gemm_main(sys.argv[1:])
+    else:
+        _profile_main(sys.argv[1:])

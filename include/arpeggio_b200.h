@@ -269,7 +269,9 @@ int arp_map_dd_soft(const float* H, const float* y, const float* sigma2, int B, 
  * elements, pointers 16-byte aligned.  epilogue: 0 C = acc (float), 1 C += acc (float; K is split over CTAs
  * whose partial products go to a stream-ordered workspace and are added in split order, so the result is the
  * same on every run), 2 C = bf16(max(acc + bias, 0)), 3 C = acc + bias (float), 4 C = bf16(acc if aux > 0 else
- * 0) with aux (M, N) bf16 of row stride ld_aux (the ReLU backward). */
+ * 0) with aux (M, N) bf16 of row stride ld_aux (the ReLU backward).  Products with M >= 128, N >= 64 and K >= 64
+ * run on a persistent kernel fed by TMA tensor loads with warp-specialised producer, MMA and epilogue roles; the
+ * rest on a cp.async-fed kernel.  Either way each shape gives the same result on every run. */
 int arp_gemm_bf16(const void* A, int a_mn_major, int lda, const void* B, int b_mn_major, int ldb, int M, int N, int K,
                   int epilogue, const float* bias, const void* aux, int ld_aux, void* C, int ldc, int32_t* status,
                   void* stream);

@@ -22,7 +22,8 @@ def _bf(shape, g, scale=1.0):
 
 
 @pytest.mark.parametrize('a_mn,b_mn', [(0, 0), (0, 1), (1, 0), (1, 1)])
-@pytest.mark.parametrize('M,N,K', [(256, 512, 512), (200, 48, 80), (128, 16, 16), (384, 256, 64), (136, 128, 1024)])
+@pytest.mark.parametrize('M,N,K', [(256, 512, 512), (200, 48, 80), (128, 16, 16), (384, 256, 64), (136, 128, 1024),
+                                   (328, 208, 1008)])
 def test_gemm_matches_torch_fp32(a_mn, b_mn, M, N, K):
     from arpeggio_b200 import warm
     if a_mn and M % 8:

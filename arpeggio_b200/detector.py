@@ -148,10 +148,13 @@ class Detector:
         if off == 0 and n == self.B and events is None:
             return self._run_fused(H, y, seed, inst0, stream)
         ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
-        key = (inst0, off, n)
+        key = (inst0, 0, self.B)
         if self._inst_base != key:
-            iv = (np.arange(inst0 + off, inst0 + off + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
-            self.inst[off:off + n].copy_(torch.from_numpy(iv))
+            # every slot's instance number at once (a host copy that waits for the stream), so the pieces of a
+            # pipelined batch find them in place and the host never waits between pieces
+            iv = (np.arange(inst0, inst0 + self.B, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
+            with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+                self.inst.copy_(torch.from_numpy(iv))
             self._inst_base = key
         L = _lib.lib()
         sp = _lib.stream_ptr(stream)
@@ -298,15 +301,32 @@ class Detector:
                 Hd[a:b].copy_(Hh[a:b], non_blocking=True)
                 yd[a:b].copy_(yh[a:b], non_blocking=True)
                 self._copy_events[c].record(xs)
+        # pieces alternate between `stream` and a second compute stream, so one piece's last blocks overlap the next
+        # piece's first; each piece's bits and distances go out on an output stream once the piece is done
+        if not hasattr(self, '_side_streams'):
+            self._side_streams = (torch.cuda.Stream(device=self.device), torch.cuda.Stream(device=self.device))
+            self._piece_events = []
+        cs2, os_ = self._side_streams
+        while len(self._piece_events) < chunks + 2:
+            self._piece_events.append(torch.cuda.Event())
+        start = self._piece_events[chunks + 1]
+        start.record(cs)
+        cs2.wait_event(start)  # the second compute stream starts after the work already on `stream`
         for c in range(chunks):
             a, b = edges[c], edges[c + 1]
             if b == a:
                 continue
-            cs.wait_event(self._copy_events[c])
-            bits, _, dist = self.run(Hd[a:b], yd[a:b], seed, n=b - a, inst0=inst0, stream=cs, off=a)
-            with torch.cuda.stream(cs):
+            s = cs if c % 2 == 0 else cs2
+            s.wait_event(self._copy_events[c])
+            bits, _, dist = self.run(Hd[a:b], yd[a:b], seed, n=b - a, inst0=inst0, stream=s, off=a)
+            self._piece_events[c].record(s)
+            os_.wait_event(self._piece_events[c])
+            with torch.cuda.stream(os_):
                 bits_out[a:b].copy_(bits, non_blocking=True)
                 dist_out[a:b].copy_(dist, non_blocking=True)
+        done = self._piece_events[chunks]
+        done.record(os_)
+        cs.wait_event(done)  # `stream` orders after every piece and every copy out
         if free is not None:
             free.record(cs)  # every reader of this staging buffer is on cs before this point
             k = 1 - self._staging_next

@@ -50,6 +50,8 @@ class _Lane:
         self.snrh = torch.zeros(g, dtype=torch.float32).pin_memory()
         self.bitsh = torch.empty(g, self.det.bits.shape[1], dtype=torch.int8).pin_memory()
         self.disth = torch.empty(g, dtype=torch.float32).pin_memory()
+        # numpy views of the pinned staging: the loop stages requests with plain host copies (no tensor dispatch)
+        self.np = {k: getattr(self, k).numpy() for k in ('Hh', 'yh', 'insth', 's2h', 'snrh', 'bitsh', 'disth')}
         self.graphs = {}
         kb = 1
         while kb <= g:
@@ -141,6 +143,7 @@ class Server:
               'bits': torch.empty(n, 2 * nt * PAM[M]['bits'], dtype=torch.int8).pin_memory(),
               'dist': torch.empty(n, dtype=torch.float32).pin_memory(),
               'done': np.full(n, np.nan), 'next': 0, 'batches': 0}
+        st['np'] = {k: st[k].numpy() for k in ('H', 'y', 's2', 'snr', 'rid_t', 'bits', 'dist')}
         self.streams[cls] = st
         return st
 
@@ -149,11 +152,12 @@ class Server:
         if k <= len(lane.Hh):
             # small batch: stage into the lane's pinned buffers, replay the graph of the next power of two
             kb = 1 << (k - 1).bit_length()
-            lane.Hh[:k].copy_(st['H'][a:b])
-            lane.yh[:k].copy_(st['y'][a:b])
-            lane.insth[:k].copy_(st['rid_t'][a:b])
-            lane.s2h[:k].copy_(st['s2'][a:b])
-            lane.snrh[:k].copy_(st['snr'][a:b])
+            src, dst = st['np'], lane.np
+            dst['Hh'][:k] = src['H'][a:b]
+            dst['yh'][:k] = src['y'][a:b]
+            dst['insth'][:k] = src['rid_t'][a:b]
+            dst['s2h'][:k] = src['s2'][a:b]
+            dst['snrh'][:k] = src['snr'][a:b]
             with torch.cuda.stream(lane.stream):
                 lane.graphs[kb].replay()
             lane.done.record(lane.stream)
@@ -186,8 +190,8 @@ class Server:
                 if lane.busy is not None and lane.done.query():
                     a, b, kb = lane.busy
                     if kb:  # results of a graph batch arrive in the lane's pinned staging
-                        st['bits'][a:b].copy_(lane.bitsh[:b - a])
-                        st['dist'][a:b].copy_(lane.disth[:b - a])
+                        st['np']['bits'][a:b] = lane.np['bitsh'][:b - a]
+                        st['np']['dist'][a:b] = lane.np['disth'][:b - a]
                     st['done'][a:b] = now
                     lane.busy = None
             arrived = int(np.searchsorted(st['t'], now, side='right'))

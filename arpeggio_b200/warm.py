@@ -226,14 +226,15 @@ class WarmDetector(Detector):
             raise ValueError('slots %d..%d outside the detector batch %d' % (off, off + n, self.B))
         ev = (lambda i: events[i].record(stream)) if events is not None else (lambda i: None)
         e5 = events is not None and len(events) == 5
-        key = (inst0, off, n)
+        key = (inst0, 0, self.B)
         if inst is not None:
             with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
                 self.inst[off:off + n].copy_(inst[:n], non_blocking=True)
             self._inst_base = None
-        elif self._inst_base != key:
-            iv = (np.arange(inst0 + off, inst0 + off + n, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
-            self.inst[off:off + n].copy_(torch.from_numpy(iv))
+        elif self._inst_base != key:  # every slot's instance number at once: pieces find theirs in place
+            iv = (np.arange(inst0, inst0 + self.B, dtype=np.int64) & M32).astype(np.uint32).view(np.int32)
+            with torch.cuda.stream(stream if stream is not None else torch.cuda.current_stream()):
+                self.inst.copy_(torch.from_numpy(iv))
             self._inst_base = key
         L = _lib.lib()
         sp = _lib.stream_ptr(stream)

@@ -337,11 +337,11 @@ __device__ __forceinline__ uint32_t eng_xs32(uint32_t x) {
 
 // Resident 256-thread blocks per SM that the integer anneal's registers are bounded for: four slots (D > 96) at two
 // blocks (128 registers: four 4-warp blocks per SM instead of three, no spills; 64 users: 129 -> 120 ms per 32768
-// uses); one slot at P <= 4 and two slots at P = 2 at four blocks (64 registers, no spills; 32 users: anneal
-// 32.7 -> 31.7 ms per 65536 uses); the rest unbounded (64 registers would spill there).
+// uses); two slots at P = 2 at four blocks (64 registers, no spills; 32 users: anneal 32.7 -> 31.7 ms per 65536
+// uses); the rest unbounded (64 registers would spill there, or, at one slot, made the 16-user MDI chain slower).
 template <int NS, int P>
 constexpr int anneal_min_blocks() {
-  return NS >= 4 ? 2 : ((NS == 1 && P <= 4) || (NS == 2 && P == 2)) ? 4 : 1;
+  return NS >= 4 ? 2 : (NS == 2 && P == 2) ? 4 : 1;
 }
 
 // ENG (Chord only): the engine's own numbers instead of Philox -- lane j's xorshift32 state starts from the anneal's

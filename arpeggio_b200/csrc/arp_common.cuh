@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/arpeggio_b200.h"
 
 #define ARP_FULL 0xffffffffu
@@ -36,6 +38,27 @@ inline cudaError_t launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size
   cfg.attrs = pdl ? at : nullptr;
   cfg.numAttrs = pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+// A kernel's dynamic shared-memory limit (a size fixed per kernel) raised once per device: cudaFuncSetAttribute
+// applies to the current device only.  Each launcher keeps one DeviceAttr per kernel; its lock guards the flags.
+struct DeviceAttr {
+  std::mutex mu;
+  bool done[64] = {};
+};
+template <typename K>
+inline cudaError_t smem_attr(DeviceAttr& st, K kern, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(st.mu);
+  if (!st.done[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    st.done[dev] = true;
+  }
+  return cudaSuccess;
 }
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of two 32x32->64 multiplies,

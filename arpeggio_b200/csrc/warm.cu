@@ -185,13 +185,8 @@ cudaError_t sum_splits(const float* ws, int splits, int M, int N, float* C, int 
 template <int BN, bool AMN, bool BMN>
 static cudaError_t launch_gemm(GemmParams p, cudaStream_t st) {
   constexpr size_t smem = (size_t)kStages * (128 * 128 + BN * 128);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_bf16<BN, AMN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static DeviceAttr attr;
+  if (cudaError_t e = smem_attr(attr, k_gemm_bf16<BN, AMN, BMN>, smem); e != cudaSuccess) return e;
   const int gx = (p.M + 127) / 128, gy = (p.N + BN - 1) / BN, nkt = (p.K + 63) / 64;
   int split = 1;
   if (p.epi == EPI_F32_ACC) {
@@ -1196,12 +1191,8 @@ extern "C" int arp_mlp_forward(const void* X, int rows, const void* W1, const fl
   if (rows == 0) return ARP_OK;
   if (!X || !W1 || !b1 || !W2p || !b2 || !W3t || !b3 || !logits) return ARP_ERR_ARG;
   if (!al16(X) || !al16(W1) || !al16(W2p) || !al16(W3t) || !al16(logits)) return ARP_ERR_ARG;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem) != cudaSuccess)
-      return ARP_ERR_LAUNCH;
-    attr = true;
-  }
+  static DeviceAttr attr;
+  if (smem_attr(attr, k_mlp_fused, kMlpSmem) != cudaSuccess) return ARP_ERR_LAUNCH;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -680,12 +680,13 @@ def run_ours(args):
     ops = 100.0 * blocks + 5.0 * B * R * D * Lp + 3.0 * D * st[0]
     t_anneal = stage[1] / 1e3
     peak_ops = 100.0 * peak_blocks
-    traffic = None
+    traffic, inst_per_anneal = None, None
     tf = os.path.join(ROOT, 'profiles', 'traffic.json')
     if os.path.exists(tf):
         tj = json.load(open(tf)).get('anneal_first_accept_x32')
         if tj:
             traffic = tj['bytes_per_detection'] * B
+            inst_per_anneal = tj.get('warp_instructions_per_anneal')
     alg_bytes = B * (D * D * 4 + D * 4) + B * R * (P * D + 24)
     peaks = {}
     pf = os.path.join(ROOT, 'MEASURED_PEAKS.json')
@@ -717,6 +718,13 @@ def run_ours(args):
         'roofline_hbm': {'bound': 'hbm', 'achieved': alg_bytes / t_anneal / 1e9, 'peak': hbm_peak, 'unit': 'GB/s',
                          'frac': alg_bytes / t_anneal / 1e9 / hbm_peak,
                          'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if peaks else 'fallback'},
+        'roofline_issue': None if inst_per_anneal is None else {
+            'bound': 'issue', 'achieved': inst_per_anneal * B * R / t_anneal / 1e9,
+            'peak': 4.0 * sms * sm_mhz * 1e6 / 1e9, 'unit': 'G warp-instructions/s',
+            'frac': inst_per_anneal * B * R / t_anneal / (4.0 * sms * sm_mhz * 1e6),
+            'source': 'warp-instructions per anneal from the ncu capture of profiles/anneal_first_accept_x32.md '
+                      '(profiles/traffic.json) x the anneals of this run over the measured anneal time; peak: one '
+                      'issue per clock per SM sub-partition, 4 x %d SMs x the sampled median SM clock' % sms},
         'roofline_smem': {'bound': 'smem', 'achieved': smem_bytes / t_anneal / 1e9, 'peak': smem_peak, 'unit': 'GB/s',
                           'frac': smem_bytes / t_anneal / 1e9 / smem_peak,
                           'bytes_model': 'flips x D x 4 (a flipped coordinate\'s int32 row of G, read by the rank-1 '
@@ -754,6 +762,7 @@ def summary(line):
     paired BER-ratio intervals per SNR point), frame latency p50/p99, serving p99 per class at 1e5 frames/s."""
     out = {'det_per_s': _r(line['value'], 4), 'e2e_det_per_s': _r(line['e2e']['value'], 4),
            'roofline_frac': _r(line['roofline']['frac']),
+           'issue_frac': _r((line.get('roofline_issue') or {}).get('frac')),
            'cpu_det_per_s': _r((line.get('cpu_baseline') or {}).get('value'), 4)}
     lat = line.get('latency') or {}
     out['frame_us_plain_p50_p99'] = [_r(lat.get('p50_us')), _r(lat.get('p99_us'))]

@@ -170,6 +170,42 @@ def test_anneal_vs_oracle_at_scale(D, K, R, S, start, policy):
     assert np.array_equal(st.cpu().numpy(), wst)
 
 
+@pytest.mark.parametrize('D,K,B,start,policy', [
+    (2, 1, 5, 'rand', 'arpeggio'),
+    (14, 3, 70, 'bal', 'arpeggio'),
+    (40, 1, 64, 'rand', 'arpeggio'),     # at most 64 problems: the launch without the register bound
+    (40, 1, 65, 'rand', 'arpeggio'),     # one more: the bounded kernel
+    (70, 2, 65, 'rand', 'chord'),
+    (100, 1, 33, 'bal', 'arpeggio'),
+    (126, 3, 9, 'rand', 'chord'),
+])
+def test_ragged_sizes_vs_oracle(D, K, B, start, policy):
+    """Coordinate counts that leave padding lanes (not a multiple of 32), odd batch sizes on both sides of the
+    small-batch launch, every copy count: bit-exact against the oracle."""
+    from arpeggio_b200 import arpeggiofx
+    from arpeggio_b200.detector import arpeggio_schedule, chord_schedule
+    R, S = 8, 8
+    G, h, _, _ = _random_dd(B, D, K, 12.0, 3000 + D * 7 + B)
+    P = 2 * K
+    if policy == 'arpeggio':
+        T, q, c = arpeggio_schedule(S, 0.1, 0.1, 0.0, K)
+    else:
+        T, q, c = chord_schedule(S * P, 0.3, 0.3, 0.4, kappa=0.3)
+    key = 0x5EEDF00D + D + B
+    inst = np.arange(B, dtype=np.int64) + 3
+    ws, wde, wst = O.anneal_dd(G, h, P, R, T, q, inst, key, start, policy=policy, c=c, nthreads=NTH)
+    Gt = torch.from_numpy(G).cuda().transpose(1, 2).contiguous()
+    s, de, st, status = arpeggiofx.anneal(Gt, torch.from_numpy(h).cuda(), P, R,
+                                          torch.tensor(T, dtype=torch.int32, device='cuda'), q, _u32(inst), key,
+                                          start, policy, None if c is None else
+                                          torch.tensor(c, dtype=torch.int32, device='cuda'))
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    assert np.array_equal(s.cpu().numpy(), ws)
+    assert np.array_equal(de.cpu().numpy(), wde)
+    assert np.array_equal(st.cpu().numpy(), wst)
+
+
 def _start_spins(B, R, P, D, key, start, inst):
     """Start states by the reference's counters (arpeggio_fx.cu:48-57), for the FP64 energy check."""
     k0, k1 = key & 0xFFFFFFFF, key >> 32

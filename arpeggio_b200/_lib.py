@@ -57,6 +57,7 @@ SIGNATURES = {
     'arp_warm_start_sampled': [_P, _I, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _F, _P, _F, _I, _I, _P, _P],
     'arp_anneal_first_accept_warm_sampled': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _U, _U, _P, _P, _P, _I, _P, _P,
                                              _P, _P, _P, _P],
+    'arp_serve_run': [_P, _I, _P, _I, ctypes.c_double, _P],
     'arp_detect_dd_static': [_P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P, _I, ctypes.c_double, _U, _U, _U,
                              _I, _P, _P, _P, _P, _P, _P],
 }
@@ -68,6 +69,18 @@ class MixedClass(ctypes.Structure):
     """arp_mixed_class: one size class of arp_anneal_first_accept_mixed (layout of include/arpeggio_b200.h)."""
     _fields_ = [('Gt', _P), ('h', _P), ('T', _P), ('L', _I), ('q', _I), ('R', _I), ('D', _I), ('B', _I),
                 ('inst', _P), ('start', _I), ('out_s', _P), ('out_de', _P), ('out_st', _P)]
+
+
+class ServeStream(ctypes.Structure):
+    """arp_serve_stream: one size class's request stream for arp_serve_run."""
+    _fields_ = [('H', _P), ('y', _P), ('s2', _P), ('snr', _P), ('rid', _P), ('t_arrival', _P), ('n', _I),
+                ('h_elems', _I), ('y_elems', _I), ('bits_per', _I), ('bits', _P), ('dist', _P), ('done', _P)]
+
+
+class ServeLane(ctypes.Structure):
+    """arp_serve_lane: one lane (stream, graphs per power-of-two batch, device buffers) for arp_serve_run."""
+    _fields_ = [('cls', _I), ('stream', _P), ('ngraphs', _I), ('sizes', _I * 32), ('graphs', _P * 32), ('Hd', _P), ('yd', _P),
+                ('s2d', _P), ('snrd', _P), ('instd', _P), ('bitsd', _P), ('distd', _P)]
 
 
 class ArpError(RuntimeError):

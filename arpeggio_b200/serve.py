@@ -14,6 +14,13 @@ and request ids.  The server keeps, per class, `inflight` lanes -- a preallocate
   * completion: a lane whose event has completed hands its results to the requests' rows of the class's
     output arrays and becomes free; each request's latency is completion time minus arrival time.
 
+Server.serve() runs this loop in the library by default (arp_serve_run): the same admission and completion rules,
+with each lane holding a second set of graphs -- the chain alone on the lane's device buffers, one per power-of-two
+batch up to its slots -- so the loop copies a batch's inputs straight from the class arrays to the device and its
+bits and distances straight back into the class's output rows, with no interpreter and no host-side data copies
+between a request's arrival and its completion.  The Python loop (serve(native=False) or step()) stays as the
+readable statement of the rules and as the tests' second opinion.
+
 A request's result does not depend on what it is batched with: every problem anneals with the server's Philox
 key and the request id as its instance number (the kernels' per-problem counters), and every stage works per
 problem.  Requests that arrive while others are on the GPU are taken by the next free lane."""
@@ -57,6 +64,15 @@ class _Lane:
         while kb <= g:
             self.graphs[kb] = self._capture(kb)
             kb *= 2
+        # the native loop's graphs: the chain alone on the lane's device buffers, for the batch sizes of
+        # native_sizes (inputs copied in and results out by the loop itself); padding slots hold zeros (noise
+        # variance 1) or an earlier batch's inputs
+        self.Hd.zero_()
+        self.yd.zero_()
+        self.instd.zero_()
+        self.det.sigma2.fill_(1.0)
+        self.det.snr_db.zero_()
+        self.dgraphs = [(kb, self._capture_device(kb)) for kb in native_sizes(slots)]
 
     def _body(self, kb):
         det = self.det
@@ -68,6 +84,17 @@ class _Lane:
         bits, _, dist = det.run(self.Hd[:kb], self.yd[:kb], self.key, n=kb, inst=self.instd[:kb])
         self.bitsh[:kb].copy_(bits, non_blocking=True)
         self.disth[:kb].copy_(dist, non_blocking=True)
+
+    def _capture_device(self, kb):
+        det = self.det
+        run = lambda: det.run(self.Hd[:kb], self.yd[:kb], self.key, n=kb, inst=self.instd[:kb])
+        with torch.cuda.stream(self.stream):
+            run()  # settles launch widths and kernel attributes outside the capture
+        self.stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream):
+            run()
+        return g
 
     def _capture(self, kb):
         self.Hh[:kb].zero_()
@@ -81,6 +108,17 @@ class _Lane:
         with torch.cuda.graph(g, stream=self.stream):
             self._body(kb)
         return g
+
+
+def native_sizes(slots):
+    """Batch sizes of a lane's native-loop graphs: powers of two to 64, then steps of about a quarter (multiples
+    of 32) up to the lane's slots, so a batch pads at most ~25 % beyond 64 requests (at most 32 sizes)."""
+    sizes = [kb for kb in (1, 2, 4, 8, 16, 32, 64) if kb <= slots]
+    kb = 64
+    while kb < slots and len(sizes) < 32:  # beyond 32 sizes the lane takes at most the last one per batch
+        kb = min(slots, max(kb + 32, (int(kb * 1.25) + 31) // 32 * 32))
+        sizes.append(kb)
+    return sizes
 
 
 def shared_bytes(cls, anneals):
@@ -178,6 +216,18 @@ class Server:
         lane.busy = (a, b, 0)
         st['batches'] += 1
 
+    def _serve_native(self, timeout):
+        cls_list, streams, lanes = _native_streams(self)
+        batches = np.zeros(max(1, len(cls_list)), dtype=np.int64)
+        rc = _lib.lib().arp_serve_run(streams, len(cls_list), lanes, len(lanes), float(timeout), batches.ctypes.data)
+        if rc == 5:  # ARP_ERR_TIMEOUT
+            raise TimeoutError('serving loop did not drain within %.0f s' % timeout)
+        _lib.check(rc, 'serve')
+        for i, cls in enumerate(cls_list):
+            st = self.streams[cls]
+            st['batches'] += int(batches[i])
+            st['next'] = len(st['t'])
+
     def step(self, now):
         """One pass of the loop at time `now` (seconds on the arrival clock): completions, then admissions.
         Returns the number of requests still pending or in flight."""
@@ -204,17 +254,27 @@ class Server:
             left += (len(st['t']) - st['next']) + sum(1 for ln in lanes if ln.busy is not None)
         return left
 
-    def serve(self, clock=None, timeout=120.0):
+    def serve(self, clock=None, timeout=120.0, native=None):
         """Runs the loop until every registered request is done.  clock(): seconds on the arrival clock
-        (default: wall time since the call).  Returns per-class latency statistics."""
-        t0 = time.perf_counter()
-        clock = clock or (lambda: time.perf_counter() - t0)
-        while True:
-            now = clock()
-            if self.step(now) == 0:
-                break
-            if time.perf_counter() - t0 > timeout:
-                raise TimeoutError('serving loop did not drain within %.0f s' % timeout)
+        (default: wall time since the call).  native (default: when no clock is given): the same loop in the
+        library (arp_serve_run: admission, copies, graph replay and completion polling without the interpreter,
+        a graph per power-of-two batch up to the lane's slots); else this module's step() loop.  Returns
+        per-class latency statistics."""
+        if native is None:
+            native = clock is None
+        if native:
+            if clock is not None:
+                raise ValueError('the native loop keeps its own clock (seconds since the call)')
+            self._serve_native(timeout)
+        else:
+            t0 = time.perf_counter()
+            clock = clock or (lambda: time.perf_counter() - t0)
+            while True:
+                now = clock()
+                if self.step(now) == 0:
+                    break
+                if time.perf_counter() - t0 > timeout:
+                    raise TimeoutError('serving loop did not drain within %.0f s' % timeout)
         for lanes in self.lanes.values():
             for lane in lanes:
                 lane.stream.synchronize()
@@ -227,6 +287,35 @@ class Server:
                 'p50_us': float(np.percentile(lat, 50)), 'p99_us': float(np.percentile(lat, 99)),
                 'max_us': float(lat.max())}
         return out
+
+
+def _native_streams(server):
+    """The arp_serve_stream and arp_serve_lane tables of a server's opened classes (stream index = class order)."""
+    import ctypes
+    cls_list = [c for c in server.lanes if c in server.streams]
+    streams = (_lib.ServeStream * len(cls_list))()
+    lanes = []
+    for i, cls in enumerate(cls_list):
+        st = server.streams[cls]
+        n = len(st['t'])
+        st['t_c'] = np.ascontiguousarray(st['t'], dtype=np.float64)
+        for k in ('H', 'y', 's2', 'snr', 'rid_t', 'bits', 'dist'):
+            if not st[k].is_contiguous():
+                raise ValueError('request stream %s of class %s must be contiguous' % (k, cls))
+        streams[i] = _lib.ServeStream(st['H'].data_ptr(), st['y'].data_ptr(), st['s2'].data_ptr(),
+                                      st['snr'].data_ptr(), st['rid_t'].data_ptr(), st['t_c'].ctypes.data, n,
+                                      int(st['H'][0].numel()) if n else 1, int(st['y'][0].numel()) if n else 1,
+                                      int(st['bits'].shape[1]), st['bits'].data_ptr(), st['dist'].data_ptr(),
+                                      st['done'].ctypes.data)
+        for lane in server.lanes[cls]:
+            det = lane.det
+            n_g = len(lane.dgraphs)
+            sizes = (ctypes.c_int * 32)(*([kb for kb, _ in lane.dgraphs] + [0] * (32 - n_g)))
+            g = (ctypes.c_void_p * 32)(*([gr.raw_cuda_graph_exec() for _, gr in lane.dgraphs] + [None] * (32 - n_g)))
+            lanes.append(_lib.ServeLane(i, lane.stream.cuda_stream, n_g, sizes, g, lane.Hd.data_ptr(),
+                                        lane.yd.data_ptr(), det.sigma2.data_ptr(), det.snr_db.data_ptr(),
+                                        lane.instd.data_ptr(), det.bits.data_ptr(), det.dist.data_ptr()))
+    return cls_list, streams, (_lib.ServeLane * len(lanes))(*lanes)
 
 
 def poisson_arrivals(n, rate, rng):

@@ -359,6 +359,51 @@ int arp_anneal_first_accept_warm_sampled(const int32_t* Gt, const int32_t* h, co
                                          const int32_t* ra, int8_t* out_s, int64_t* out_de, int64_t* out_st,
                                          int32_t* status, void* stream);
 
+/* Native serving loop (no counterpart in the reference; arpeggio_b200.serve.Server drives it).  A request
+ * stream per size class: its requests' inputs in host memory (pinned, for the staging copies to overlap), their
+ * arrival times in seconds on the loop's clock (ascending), and outputs.  h_elems / y_elems / bits_per are the
+ * floats of one request's H and y and the bytes of its hard bits. */
+typedef struct {
+  const float* H;
+  const float* y;
+  const float* s2;          /* noise variance per real dimension */
+  const float* snr;         /* SNR in dB (the warm start's feature) */
+  const int32_t* rid;       /* instance numbers (a request's result depends on its id alone) */
+  const double* t_arrival;  /* n, seconds, ascending */
+  int n, h_elems, y_elems, bits_per;
+  int8_t* bits;             /* n x bits_per */
+  float* dist;              /* n */
+  double* done;             /* n: completion time on the loop's clock */
+} arp_serve_stream;
+
+/* A lane: one detector of its class, the stream its work runs on, and captured CUDA graphs for ngraphs <= 32 batch
+ * sizes (sizes ascending; graphs[i] detects the first sizes[i] slots of the lane's device buffers): inputs H, y,
+ * noise variance, SNR and instance numbers, outputs bits and distances. */
+typedef struct {
+  int cls;
+  void* stream;
+  int ngraphs;
+  int sizes[32];
+  void* graphs[32]; /* cudaGraphExec_t */
+  float *Hd, *yd, *s2d, *snrd;
+  int32_t* instd;
+  const int8_t* bitsd;
+  const float* distd;
+} arp_serve_lane;
+
+/* Runs the continuous-batching loop on the calling thread until every request of every stream is done, polling
+ * the clock (steady, seconds since the call): a lane whose last batch has completed records its requests'
+ * completion time and becomes free; a free lane takes every request of its class that has arrived and is not
+ * taken yet, up to its largest graph, copies their inputs from the stream's host arrays to its device buffers,
+ * replays the graph of the smallest size that holds them (the padding slots are detected and discarded), copies bits and
+ * distances straight into the stream's output rows and records an event -- all on the lane's stream, so the
+ * batches of different lanes overlap on the GPU.  batches (nstreams, may be NULL) counts the batches per stream.
+ * ARP_ERR_TIMEOUT if the requests are not all done within timeout_s (the batches in flight are waited for
+ * first); ARP_ERR_LAUNCH on a CUDA error.  The host side of arpeggio_b200.serve's Python loop without the
+ * interpreter in the polling path. */
+int arp_serve_run(const arp_serve_stream* streams, int nstreams, const arp_serve_lane* lanes, int nlanes,
+                  double timeout_s, int64_t* batches);
+
 /* arp_detect_dd without a workspace argument, for callers that cannot allocate device memory: a receive
  * chain with a hard per-frame latency budget cannot call cudaMalloc on the frame path (it synchronises the
  * device and takes unbounded time), and a plugin inside a host program that owns all device memory may not

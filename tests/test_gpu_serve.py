@@ -50,6 +50,30 @@ def test_each_result_is_the_same_alone_and_in_the_mix(warm_start, slots, burst):
             assert float(dist[0]) == float(st['dist'][i]), (cls, i)
 
 
+def test_native_loop_equals_the_python_loop():
+    """The library's loop (arp_serve_run) and this module's step() loop give every request the same bits and
+    distance, and both finish every request."""
+    from arpeggio_b200 import serve
+    streams = _streams(200, 9)
+    res = {}
+    for native in (True, False):
+        srv = serve.Server(CLASSES, anneals=8, sweeps=8, slots=64, inflight=2, hbm_budget=1 << 30)
+        for cls, (H, y, N0, t, rid) in streams.items():
+            srv.open(cls, H, y, N0, t, rid)
+        stats = srv.serve(native=native)
+        for cls in streams:
+            st = srv.streams[cls]
+            assert stats['%dx%d %d-QAM' % cls]['requests'] == 200
+            assert not np.isnan(st['done']).any()
+        res[native] = {cls: (srv.streams[cls]['bits'].clone(), srv.streams[cls]['dist'].clone()) for cls in streams}
+        del srv
+    for cls in streams:
+        assert torch.equal(res[True][cls][0], res[False][cls][0]), cls
+        assert torch.equal(res[True][cls][1], res[False][cls][1]), cls
+    with pytest.raises(ValueError):
+        serve.Server(CLASSES[:1], anneals=8, sweeps=8, slots=4).serve(clock=lambda: 0.0, native=True)
+
+
 def test_server_rejects_classes_beyond_shared_memory():
     from arpeggio_b200 import serve
     with pytest.raises(ValueError):

@@ -54,6 +54,20 @@ def test_host_rejects_bad_shapes_without_gpu():
     # empty batch is a no-op
     assert L.arp_anneal_first_accept(None, None, None, 1, 0, 2, 1, 32, 0, None, 0, 0, 0, None, None, None, None,
                                      None) == 0
+    # the native serving loop checks its tables before any CUDA call: bad counts, a stream with null buffers,
+    # requests that no lane can take; nothing to serve is a no-op
+    assert L.arp_serve_run(None, -1, None, 0, 1.0, None) == 3
+    bad = (_lib.ServeStream * 1)()
+    bad[0].n, bad[0].h_elems, bad[0].y_elems, bad[0].bits_per = 2, 4, 2, 2
+    assert L.arp_serve_run(bad, 1, None, 0, 1.0, None) == 3
+    H, y, f, rid = (np.zeros(8, np.float32), np.zeros(4, np.float32), np.zeros(2, np.float32),
+                    np.zeros(2, np.int32))
+    t, bits, done = np.zeros(2), np.zeros(4, np.int8), np.zeros(2)
+    ok = (_lib.ServeStream * 1)(_lib.ServeStream(H.ctypes.data, y.ctypes.data, f.ctypes.data, f.ctypes.data,
+                                                 rid.ctypes.data, t.ctypes.data, 2, 4, 2, 2, bits.ctypes.data,
+                                                 f.ctypes.data, done.ctypes.data))
+    assert L.arp_serve_run(ok, 1, None, 0, 1.0, None) == 3
+    assert L.arp_serve_run(None, 0, None, 0, 1.0, None) == 0
 
 
 def test_draw_matches_reference(golden):

@@ -72,6 +72,12 @@ def test_native_loop_equals_the_python_loop():
         assert torch.equal(res[True][cls][1], res[False][cls][1]), cls
     with pytest.raises(ValueError):
         serve.Server(CLASSES[:1], anneals=8, sweeps=8, slots=4).serve(clock=lambda: 0.0, native=True)
+    # requests that arrive after the time limit: the library loop gives up and reports it, with nothing in flight
+    srv = serve.Server(CLASSES[:1], anneals=8, sweeps=8, slots=4)
+    H, y, N0, t, rid = streams[CLASSES[0]]
+    srv.open(CLASSES[0], H, y, N0, t + 1e6, rid)
+    with pytest.raises(TimeoutError):
+        srv.serve(native=True, timeout=0.05)
 
 
 def test_server_rejects_classes_beyond_shared_memory():

@@ -7,7 +7,7 @@
 //   tcgen05.mma kind::i8 forms the digit products d_a^T d_b with exact s32 accumulation in TMEM, grouped by
 //   weight a + b (classes 6, 5, 4, 3; the dropped lower classes move an entry by ~2^-26 of the largest |Q|, well
 //   below the FP32 rounding of the reference's own product), and the epilogue
-//   sums the classes exactly in double and rounds once to float.  Q is exactly symmetric (an exact integer
+//   sums the classes exactly as a 64-bit integer and rounds once to float.  Q is exactly symmetric (an exact integer
 //   sum), as the symmetrised J of to_fixed.  g = H^T y as an ordered fma chain per coordinate;
 //   A = Q + sigma2 I inverted in shared memory (Gauss-Jordan; A is SPD), z = A^-1 g, mu = diag(A^-1 Q),
 //   x_q = nearest level of z / mu (first level on ties);
@@ -122,17 +122,6 @@ __host__ __device__ constexpr int kTmemCols() {  // four class accumulators of D
 __constant__ int8_t kPairA[10] = {3, 3, 2, 3, 1, 2, 3, 0, 2, 1};
 __constant__ int8_t kPairB[10] = {3, 2, 3, 1, 3, 2, 0, 3, 1, 2};
 __constant__ int8_t kPairC[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};  // accumulator: class 6 - c
-
-// Signed base-256 digits of x (|x| < 2^30): x = d0 + 2^8 d1 + 2^16 d2 + 2^24 d3, each in [-128, 127].
-__device__ __forceinline__ void digits4(int32_t x, int32_t (&d)[4]) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const int32_t lo = (int32_t)(int8_t)(x & 0xFF);
-    d[a] = lo;
-    x = (x - lo) >> 8;
-  }
-  d[3] = x;
-}
 
 // Register bounds for more resident blocks (the Gauss-Jordan steps are barrier-latency bound, so blocks overlap):
 // four per SM at 32 users (64 registers, a few spilled: 3.95 -> 3.73 ms per 65536 uses), two per SM at 64 users
@@ -293,6 +282,9 @@ __global__ void __launch_bounds__(GS * GS, TB == 8 ? 2 : (TB == 4 ? 4 : 1)) k_ma
     const int m = MP == 128 ? wq * 32 + lane : wq * 16 + lane;
     const bool valid = (MP == 128 || lane < 16) && m < Dp;
     const int e2 = 24 - 2 * s_exp;
+    // scaling by 2^e2 as one multiply where 2^e2 is a normal float (the same correctly rounded product as ldexpf)
+    const bool fast_e2 = e2 >= -126 && e2 <= 127;
+    const float f2 = fast_e2 ? __int_as_float((e2 + 127) << 23) : 1.0f;
     constexpr int CW = Dp >= 16 ? Dp / 2 : Dp;
 #pragma unroll 1
     for (int c0 = half * CW; c0 < (half + 1) * CW && c0 < Dp; c0 += 8) {
@@ -308,7 +300,8 @@ __global__ void __launch_bounds__(GS * GS, TB == 8 ? 2 : (TB == 4 ? 4 : 1)) k_ma
         for (int j = 0; j < 8; ++j) {
           const long long q = ((((long long)(int32_t)v6[j] * 256 + (int32_t)v5[j]) * 256 + (int32_t)v4[j]) * 256) +
                               (int32_t)v3[j];
-          Qs[m * QP + c0 + j] = ldexpf(__ll2float_rn(q), e2);
+          const float qf = __ll2float_rn(q);
+          Qs[m * QP + c0 + j] = fast_e2 ? __fmul_rn(qf, f2) : ldexpf(qf, e2);
         }
       }
     }

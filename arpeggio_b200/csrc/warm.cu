@@ -958,24 +958,26 @@ extern "C" int arp_warm_start(const float* logits, int ldl, const void* G, const
 }
 
 // ------------------------------------------------------------------------------------------------ fused inference
-// The whole network for a 128-row tile in one CTA (persistent over tiles, 8 warps, one CTA per SM):
-//   L1: D[0:512) = X W1^T      (X tile 128 x 16 and W1 staged in shared memory; two N = 256 MMAs)
-//   epilogue 1: TMEM -> bias + ReLU -> bf16 -> H tile (128 x 512, K-major canonical layout, shared memory)
-//   L2: D[0:512) = H1 W2^T     W2 streamed in 32 chunks (256 rows x 32 k, 16 KB each, one bulk copy from the packed
-//                              copy W2p) through a 4-slot ring: thread 0 produces (full barrier with the byte
-//                              count), thread 32 issues the MMAs and releases each slot with tcgen05.commit on
-//                              its empty barrier
-//   epilogue 2: TMEM -> bias + ReLU -> bf16 -> the same H tile (every L2 MMA has completed)
-//   L3: D[0:16) = H2 W3        (W3t (512 x 16) staged MN-major; 32 MMAs of K = 16)
-//   epilogue 3: TMEM -> + b3 -> logits (rows, 16) float in global memory
-// Only X and the logits touch HBM; the weights come from L2.  Shared memory: H 128 KB + X 4 KB + ring 64 KB.
-// Slot layout of a W2 chunk (K-major, no swizzle): byte(n, k) = (k / 8) 4096 + n 16 + (k % 8) 2, i.e. SBO 128 B
-// between 8-row groups and LBO 4096 B between k-groups; arp_mlp_pack_w2 writes W2 in this order once per weight
-// update, so a chunk is one contiguous 16 KB copy (whole L2 sectors, no gather).
+// The whole network for a 128-row tile in one CTA (persistent over tiles, one CTA per SM; eight epilogue warps and
+// one MMA warp), every weight resident in shared memory for the whole launch:
+//   L1: acc1 = X W1^T              (X tile 128 x 16; one N = 256 MMA into TMEM columns 256..511)
+//   epilogue 1: acc1 -> bias + ReLU -> bf16 -> H tile (128 x 256, K-major canonical layout), 32 columns at a time,
+//               each chunk announced on its mbarrier
+//   L2: acc2 = H1 W2^T             (TMEM columns 0..255; the two MMAs of k-chunk t issued as soon as chunk t of H1
+//                                   is in place, so layer 2 runs behind epilogue 1)
+//   epilogue 2: acc2 -> bias + ReLU -> bf16 -> the same H tile (every L2 MMA has completed), chunk by chunk
+//   L3: acc1[0:16) = H2 W3         (W3t (256 x 16) MN-major; its MMAs behind epilogue 2)
+//   epilogue 3: acc1[0:16) + b3 -> logits (rows, 16) float in global memory
+// Only X and the logits touch HBM.  Shared memory: W2 128 KB + H 64 KB + X 4 KB + W1 and W3t 8 KB each.
+// W2's order in shared memory (K-major, no swizzle): byte(n, k) = (k / 32) 16384 + ((k % 32) / 8) 4096 + n 16 +
+// (k % 8) 2; arp_mlp_pack_w2 writes W2 in this order once per weight update, so it arrives by eight contiguous
+// 16 KB bulk copies (whole L2 sectors, no gather).
 namespace arp {
 
 constexpr int kNH = 256;  // hidden width of the warm-start network
-constexpr int kMlpThreads = 256;
+constexpr int kMlpEpiWarps = 8;                       // epilogue warps (TMEM lane quarter w % 4, column half w / 4)
+constexpr int kMlpThreads = 32 * (kMlpEpiWarps + 1);  // and one MMA warp
+constexpr uint32_t kMlpCols = 2 * kNH;                // two accumulators: layer 2, and layers 1 and 3
 // Shared memory of the fused forward: W2 resident for the whole launch (8 chunks of 256 rows x 32 k, 128 KB),
 // the H tile (128 rows x 256, H1 then H2), the X tile, W1 and W3t resident (8 KB each).
 constexpr uint32_t kW2Bytes = kNH * kNH * 2, kHsBytes = 128 * kNH * 2, kXsBytes = 128 * 16 * 2;
@@ -1003,49 +1005,52 @@ __global__ void __launch_bounds__(256) k_pack_w2(const bf16* __restrict__ W2, bf
   reinterpret_cast<uint4*>(W2p)[i] = *reinterpret_cast<const uint4*>(W2 + (size_t)n * kNH + k);
 }
 
-// TMEM -> bias (shared memory) + ReLU -> bf16 -> H tile (K-major, 8-row groups 4096 B apart); warp w drains
-// rows 32 (w % 4) .. and columns [128 (w / 4), +128).
-__device__ __forceinline__ void mlp_epi_hidden(uint32_t tmem, uint32_t hs, const float* bias, int warp, int lane) {
-  const int m = (warp & 3) * 32 + lane, half = warp >> 2;
-#pragma unroll 1
-  for (int cc = 0; cc < 4; ++cc) {
-    const int c0 = half * 128 + cc * 32;
-    uint32_t v[32];
-    umma::tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0, v);
+// One 32-column chunk t of a hidden layer: TMEM (the accumulator's columns 32 t ..) -> bias (shared memory) + ReLU
+// -> bf16 -> the H tile (K-major, 8-row groups 4096 B apart).  Warp w (of the eight epilogue warps) takes rows
+// 32 (w % 4) .. + 31 and 16 of the chunk's columns (half w / 4), so the eight warps finish chunk t together and
+// the next layer's MMAs over k-chunk t can start right behind them.
+__device__ __forceinline__ void mlp_epi_chunk(uint32_t acc, uint32_t hs, const float* bias, int t, int warp,
+                                              int lane) {
+  const int m = (warp & 3) * 32 + lane, c0 = t * 32 + (warp >> 2) * 16;
+  uint32_t v[32];
+  umma::tmem_ld16(acc + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0, v);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float4 bl = *reinterpret_cast<const float4*>(bias + c0 + q * 8);
-      const float4 bh = *reinterpret_cast<const float4*>(bias + c0 + q * 8 + 4);
-      const float bb[8] = {bl.x, bl.y, bl.z, bl.w, bh.x, bh.y, bh.z, bh.w};
-      uint32_t pk[4];
+  for (int q = 0; q < 2; ++q) {
+    const float4 bl = *reinterpret_cast<const float4*>(bias + c0 + q * 8);
+    const float4 bh = *reinterpret_cast<const float4*>(bias + c0 + q * 8 + 4);
+    const float bb[8] = {bl.x, bl.y, bl.z, bl.w, bh.x, bh.y, bh.z, bh.w};
+    uint32_t pk[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int j = q * 8 + 2 * i;
-        const float a = fmaxf(__uint_as_float(v[j]) + bb[2 * i], 0.0f);
-        const float b = fmaxf(__uint_as_float(v[j + 1]) + bb[2 * i + 1], 0.0f);
-        const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
-        pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
-      }
-      const uint32_t addr = hs + (uint32_t)((m >> 3) * 4096 + ((c0 >> 3) + q) * 128 + (m & 7) * 16);
-      asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
-                   "r"(pk[3])
-                   : "memory");
+    for (int i = 0; i < 4; ++i) {
+      const int j = q * 8 + 2 * i;
+      const float a = fmaxf(__uint_as_float(v[j]) + bb[2 * i], 0.0f);
+      const float b = fmaxf(__uint_as_float(v[j + 1]) + bb[2 * i + 1], 0.0f);
+      const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+      pk[i] = *reinterpret_cast<const uint32_t*>(&h2);
     }
+    const uint32_t addr = hs + (uint32_t)((m >> 3) * 4096 + ((c0 >> 3) + q) * 128 + (m & 7) * 16);
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
+                 "r"(pk[3])
+                 : "memory");
   }
 }
 
 // The whole network per 128-row tile, one persistent CTA per SM: the weights are loaded once per launch (W2 by
-// eight bulk copies on one mbarrier, W1, W3t and the biases by cp.async) and stay in shared memory; per tile,
-// layer 1 (one MMA, N = 256), its epilogue into the H tile, layer 2 (16 MMAs from the resident W2), its
-// epilogue over H1, layer 3 (16 MMAs, N = 16), logits + b3 to global.  The next tile's X is fetched as soon as
-// layer 1 has read the current one.  Same roundings and summation order as the layer-by-layer GEMMs.
+// eight bulk copies on one mbarrier, W1, W3t and the biases by cp.async) and stay in shared memory.  Per tile:
+// layer 1 (one MMA, N = 256) into the accumulator at TMEM columns 256..511; the eight epilogue warps drain it chunk
+// by chunk (32 hidden units) into the H tile, arriving on the chunk's mbarrier, while the MMA warp issues layer 2's
+// two MMAs of each k-chunk as soon as that chunk is in place (accumulator at columns 0..255); the epilogue warps
+// then drain layer 2 chunk by chunk over H1 (every layer-2 MMA has completed) while the MMA warp issues layer 3's
+// MMAs (N = 16, accumulator at columns 256..271) behind them; logits + b3 to global.  The next tile's X is fetched
+// as soon as layer 1 has read the current one.  Same roundings and summation order as the layer-by-layer GEMMs.
 __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bar_w, bar_l1, bar_l2, bar_l3;
+  __shared__ __align__(8) uint64_t bar_w, bar_l1, bar_l2, bar_l3, bar_done, bar_h1[kNH / 32], bar_h2[kNH / 32];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   __shared__ __align__(16) float s_b1[kNH], s_b2[kNH];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool mma_warp = warp == kMlpEpiWarps;
   const int ntiles = (p.rows + 127) / 128;
   if ((int)blockIdx.x >= ntiles) return;
   pdl_trigger();
@@ -1057,17 +1062,22 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
     umma::mbar_init(&bar_l1, 1);
     umma::mbar_init(&bar_l2, 1);
     umma::mbar_init(&bar_l3, 1);
+    umma::mbar_init(&bar_done, 1);
+    for (int t = 0; t < kNH / 32; ++t) {
+      umma::mbar_init(&bar_h1[t], kMlpEpiWarps);
+      umma::mbar_init(&bar_h2[t], kMlpEpiWarps);
+    }
     umma::fence_mbar_init();
     s_abort = 0;
   }
-  if (warp == 0) umma::tmem_alloc(&s_tmem, kNH);
+  if (warp == 0) umma::tmem_alloc(&s_tmem, kMlpCols);
   umma::tc_before_sync();
   __syncthreads();
   umma::tc_after_sync();
-  const uint32_t tmem = s_tmem;
+  const uint32_t acc2 = s_tmem, acc1 = s_tmem + kNH;  // layer 2 at columns 0..255; layers 1 and 3 at 256..
   pdl_wait();  // everything above touches no global memory
 
-  auto load_x = [&](int tile) {  // 128 x 16: one 16-byte chunk per thread
+  auto load_x = [&](int tile) {  // 128 x 16: one 16-byte chunk per epilogue thread
     const int row = tid >> 1, kc = tid & 1, m = tile * 128 + row;
     const bool ok = m < p.rows;
     umma::cp16(xs + (uint32_t)((row >> 3) * 256 + kc * 128 + (row & 7) * 16),
@@ -1075,16 +1085,19 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
   };
   // weights, once: W2 by bulk copies (thread 0), W1 (256 x 16, K-major, SBO 256) and W3t (256 k x 16 n,
   // MN-major: LBO 256 between k-groups, SBO 128) and the biases by cp.async
+  constexpr int E = kMlpEpiWarps * 32;  // epilogue threads
   if (tid == 0) {
     umma::expect_tx(&bar_w, kW2Bytes);
     for (int t = 0; t < kNH / 32; ++t)
       umma::bulk_g2s(w2s + (uint32_t)t * kChunkBytes, p.W2p + (size_t)t * (kChunkBytes / 2), kChunkBytes, &bar_w);
   }
+  if (tid < E) {
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int c = tid + i * kMlpThreads, r = c >> 1, h = c & 1;
-    umma::cp16(w1s + (uint32_t)((r >> 3) * 256 + h * 128 + (r & 7) * 16), p.W1 + (size_t)r * 16 + h * 8, true);
-    umma::cp16(w3s + (uint32_t)((r >> 3) * 256 + h * 128 + (r & 7) * 16), p.W3t + (size_t)r * 16 + h * 8, true);
+    for (int i = 0; i < 2; ++i) {
+      const int c = tid + i * E, r = c >> 1, h = c & 1;
+      umma::cp16(w1s + (uint32_t)((r >> 3) * 256 + h * 128 + (r & 7) * 16), p.W1 + (size_t)r * 16 + h * 8, true);
+      umma::cp16(w3s + (uint32_t)((r >> 3) * 256 + h * 128 + (r & 7) * 16), p.W3t + (size_t)r * 16 + h * 8, true);
+    }
   }
   if (p.bias16) {
     if (tid < 2 * kNH / 4)
@@ -1096,90 +1109,105 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_fused(const MlpParams p)
       s_b2[i] = p.b2[i];
     }
   }
-  load_x(blockIdx.x);
+  if (tid < E) load_x(blockIdx.x);
   umma::cp_commit();
   bool w2_ready = false;
   int it = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    // ---- layer 1 (X landed; the previous tile's TMEM reads are done)
+    const uint32_t ph = (uint32_t)(it & 1);
+    // ---- layer 1 (X landed; the previous tile's TMEM reads and layer-3 MMAs are done)
     umma::cp_wait<0>();
     umma::fence_async_smem();
     umma::tc_before_sync();
     __syncthreads();
     if (s_abort) break;
-    if (tid == 32) {
-      umma::tc_after_sync();
-      umma::mma(tmem, umma::sdesc(xs, 128, 256), umma::sdesc(w1s, 128, 256), ID_HID, 0u);
-      umma::commit(&bar_l1);
-    }
-    if (!umma::mbar_wait(&bar_l1, it & 1)) s_abort = 1;
-    if (tile + (int)gridDim.x < ntiles) load_x(tile + gridDim.x);  // layer 1 has read X
-    umma::cp_commit();
-    umma::tc_after_sync();
-    mlp_epi_hidden(tmem, hs, s_b1, warp, lane);
-    umma::fence_async_smem();
-    umma::tc_before_sync();
-    __syncthreads();
-    if (s_abort) break;
-    // ---- layer 2: A = H1 (K-major, SBO 4096), B = the resident W2 chunk t (LBO 4096, SBO 128)
-    if (tid == 32) {
-      umma::tc_after_sync();
-      bool ok = true;
-      if (!w2_ready) ok = umma::mbar_wait(&bar_w, 0);
-      if (ok) {
-#pragma unroll 1
-        for (int t = 0; t < kNH / 32; ++t)
+    if (mma_warp) {
+      if (lane == 0) {
+        umma::tc_after_sync();
+        umma::mma(acc1, umma::sdesc(xs, 128, 256), umma::sdesc(w1s, 128, 256), ID_HID, 0u);
+        umma::commit(&bar_l1);
+        // ---- layer 2, k-chunk by k-chunk behind epilogue 1: A = H1 (K-major, SBO 4096), B = the resident W2
+        bool ok = w2_ready || umma::mbar_wait(&bar_w, 0);
+        for (int t = 0; t < kNH / 32 && ok; ++t) {
+          if (!umma::mbar_wait(&bar_h1[t], ph)) {
+            ok = false;
+            break;
+          }
+          umma::tc_after_sync();
 #pragma unroll
           for (int kk = 0; kk < 2; ++kk)
-            umma::mma(tmem, umma::sdesc(hs + (uint32_t)((t * 4 + kk * 2) * 128), 128, 4096),
+            umma::mma(acc2, umma::sdesc(hs + (uint32_t)((t * 4 + kk * 2) * 128), 128, 4096),
                       umma::sdesc(w2s + (uint32_t)t * kChunkBytes + (uint32_t)(kk * 8192), 4096, 128), ID_HID,
                       (t > 0 || kk > 0) ? 1u : 0u);
-        umma::commit(&bar_l2);
-      } else {
-        s_abort = 1;
-        umma::commit(&bar_l2);  // nothing issued: completes at once, so no thread waits for the full bound
-      }
-    }
-    w2_ready = true;
-    __syncwarp();
-    if (!umma::mbar_wait(&bar_l2, it & 1)) s_abort = 1;
-    umma::tc_after_sync();
-    mlp_epi_hidden(tmem, hs, s_b2, warp, lane);  // H2 over H1: every layer-2 MMA has completed
-    umma::fence_async_smem();
-    umma::tc_before_sync();
-    __syncthreads();
-    if (s_abort) break;
-    // ---- layer 3: A = H2, B = W3t (MN-major)
-    if (tid == 32) {
-      umma::tc_after_sync();
-#pragma unroll 4
-      for (int kk = 0; kk < kNH / 16; ++kk)
-        umma::mma(tmem, umma::sdesc(hs + (uint32_t)(kk * 256), 128, 4096), umma::sdesc(w3s + (uint32_t)(kk * 512), 256, 128),
-                  ID_OUT, kk > 0 ? 1u : 0u);
-      umma::commit(&bar_l3);
-    }
-    if (!umma::mbar_wait(&bar_l3, it & 1)) s_abort = 1;
-    umma::tc_after_sync();
-    if (warp < 4) {
-      uint32_t v[32];
-      umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
-      const int row = tile * 128 + warp * 32 + lane;
-      if (row < p.rows && !s_abort) {
-        float4* o = reinterpret_cast<float4*>(p.logits + (size_t)row * 16);
+        }
+        umma::commit(&bar_l2);  // also when nothing was issued: it completes at once, nobody waits out the bound
+        // ---- layer 3, behind epilogue 2: A = H2, B = W3t (MN-major), accumulator over layer 1's columns
+        for (int t = 0; t < kNH / 32 && ok; ++t) {
+          if (!umma::mbar_wait(&bar_h2[t], ph)) {
+            ok = false;
+            break;
+          }
+          umma::tc_after_sync();
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-          o[i] = make_float4(__uint_as_float(v[4 * i]) + __ldg(p.b3 + 4 * i),
-                             __uint_as_float(v[4 * i + 1]) + __ldg(p.b3 + 4 * i + 1),
-                             __uint_as_float(v[4 * i + 2]) + __ldg(p.b3 + 4 * i + 2),
-                             __uint_as_float(v[4 * i + 3]) + __ldg(p.b3 + 4 * i + 3));
+          for (int k2 = 0; k2 < 2; ++k2) {
+            const int kk = 2 * t + k2;
+            umma::mma(acc1, umma::sdesc(hs + (uint32_t)(kk * 256), 128, 4096),
+                      umma::sdesc(w3s + (uint32_t)(kk * 512), 256, 128), ID_OUT, kk > 0 ? 1u : 0u);
+          }
+        }
+        umma::commit(&bar_l3);
+        if (!ok) s_abort = 1;
+      }
+      w2_ready = true;
+      __syncwarp();
+    } else {
+      if (!umma::mbar_wait(&bar_l1, ph)) s_abort = 1;
+      if (tile + (int)gridDim.x < ntiles) load_x(tile + gridDim.x);  // layer 1 has read X
+      umma::cp_commit();
+      umma::tc_after_sync();
+      for (int t = 0; t < kNH / 32; ++t) {  // epilogue 1, chunk by chunk
+        mlp_epi_chunk(acc1, hs, s_b1, t, warp, lane);
+        umma::fence_async_smem();
+        umma::tc_before_sync();
+        __syncwarp();
+        if (lane == 0) umma::mbar_arrive(&bar_h1[t]);
+      }
+      if (!umma::mbar_wait(&bar_l2, ph)) s_abort = 1;
+      umma::tc_after_sync();
+      for (int t = 0; t < kNH / 32; ++t) {  // epilogue 2 over H1, chunk by chunk
+        mlp_epi_chunk(acc2, hs, s_b2, t, warp, lane);
+        umma::fence_async_smem();
+        umma::tc_before_sync();
+        __syncwarp();
+        if (lane == 0) umma::mbar_arrive(&bar_h2[t]);
+      }
+      if (warp < 4) {
+        if (!umma::mbar_wait(&bar_l3, ph)) s_abort = 1;
+        umma::tc_after_sync();
+        uint32_t v[32];
+        umma::tmem_ld16(acc1 + ((uint32_t)(warp * 32) << 16), v);
+        const int row = tile * 128 + warp * 32 + lane;
+        if (row < p.rows && !s_abort) {
+          float4* o = reinterpret_cast<float4*>(p.logits + (size_t)row * 16);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            o[i] = make_float4(__uint_as_float(v[4 * i]) + __ldg(p.b3 + 4 * i),
+                               __uint_as_float(v[4 * i + 1]) + __ldg(p.b3 + 4 * i + 1),
+                               __uint_as_float(v[4 * i + 2]) + __ldg(p.b3 + 4 * i + 2),
+                               __uint_as_float(v[4 * i + 3]) + __ldg(p.b3 + 4 * i + 3));
+        }
       }
     }
+  }
+  if (mma_warp && lane == 0) {  // every MMA issued has completed before TMEM is released (bounded)
+    umma::commit(&bar_done);
+    if (!umma::mbar_wait(&bar_done, 0)) s_abort = 1;
   }
   umma::cp_wait<0>();
   umma::tc_before_sync();
   __syncthreads();
   if (s_abort && tid == 0) set_status(p.status, ARP_ERR_TIMEOUT);
-  if (warp == 0) umma::tmem_free(tmem, kNH);
+  if (warp == 0) umma::tmem_free(s_tmem, kMlpCols);
 }
 
 }  // namespace arp

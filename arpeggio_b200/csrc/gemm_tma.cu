@@ -16,7 +16,7 @@
 // Every wait is bounded (ARP_ERR_TIMEOUT).  After a timeout every role stops issuing; before TMEM is released the
 // producer waits (bounded) for the loads it has in flight and the MMA lane for the MMAs it has issued.
 //
-// Shared-memory layouts (no multicast anywhere): a K-major operand box {64 k, R rows} lands as R rows of 128 bytes
+// Shared-memory layouts (every load fills this CTA's own shared memory only): a K-major operand box {64 k, R rows} lands as R rows of 128 bytes
 // (SBO 1024); an MN-major operand is loaded as boxes {64 of M or N, 64 k}, 64 rows of 128 bytes each (SBO 1024
 // between 8-k groups, LBO 8192 between the 64-element blocks).
 #include <cuda.h>

@@ -76,7 +76,7 @@ __device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
 }
 
-// One contiguous global -> shared bulk copy (no tensor map, no multicast): both addresses 16-byte aligned, `bytes`
+// One contiguous global -> shared bulk copy into this CTA's shared memory (no tensor map): both addresses 16-byte aligned, `bytes`
 // a multiple of 16; completes `bytes` on the mbarrier.
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -84,7 +84,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                : "memory");
 }
 
-// One 2D tiled TMA load (no multicast): the box at element coordinates (x, y) of the tensor map (a kernel
+// One 2D tiled TMA load into this CTA's shared memory: the box at element coordinates (x, y) of the tensor map (a kernel
 // parameter) into shared memory at dst; completes the box's bytes on the mbarrier (zero fill outside the tensor).
 // x times the element size must be a multiple of 16 bytes.
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y, uint64_t* bar) {

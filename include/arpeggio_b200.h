@@ -2,8 +2,10 @@
  * arpeggio_b200 -- C ABI of the B200 (sm_100a) delta-encoded Ising MIMO detector path.
  *
  * Plain pointers and sizes; every array argument is DEVICE memory unless stated otherwise.  No entry
- * point allocates memory.  Every entry point is stream-ordered on `stream` (a cudaStream_t, or NULL
- * for the legacy default stream) and returns without synchronising.  Return value: ARP_OK or an
+ * point of the detection path allocates memory; two training routines take stream-ordered workspaces
+ * (cudaMallocAsync, freed on the same stream): arp_gemm_bf16 with split K and arp_colsum_bf16.  Every entry
+ * point is stream-ordered on `stream` (a cudaStream_t, or NULL for the legacy default stream) and returns
+ * without synchronising, except arp_serve_run, a host loop that returns when its requests are done.  Return value: ARP_OK or an
  * ARP_ERR_* code for errors found on the host (shapes, arguments, launch).  Errors that only the
  * device can see (coefficients beyond the exact 32-bit field range) are written to `status`
  * (one int32 in device memory, may be NULL; set to the first error code, never cleared here).

@@ -137,6 +137,15 @@ def test_serving_admission_and_mixed_classes():
     assert serve.shared_bytes((64, 128, 16), 32) > serve.shared_bytes((64, 64, 16), 32)
     arrivals = serve.poisson_arrivals(10000, 1e5, np.random.default_rng(0))
     assert np.all(np.diff(arrivals) > 0) and abs(arrivals[-1] - 0.1) < 0.01
+    # the library loop's graph sizes: powers of two to 64, then steps of about a quarter, at most 32 sizes; a batch
+    # of k requests pads to the next size by at most ~25 % beyond 64
+    for slots in (1, 5, 64, 100, 4096, 100000):
+        sz = serve.native_sizes(slots)
+        assert sz[0] == 1 and len(sz) <= 32 and all(b > a for a, b in zip(sz, sz[1:])) and sz[-1] <= slots
+        assert sz[-1] == slots or len(sz) == 32 or slots < 64  # below 64: the largest power of two
+        for k in range(65, sz[-1] + 1, 97):
+            kb = next(v for v in sz if v >= k)
+            assert kb <= max(k + 32, 1.25 * k + 32)
 
 
 def test_oracle_anneal_counts_skip_exactly_the_late_anneals():

@@ -712,9 +712,9 @@ static int pick_warps(K kern, size_t smem, int R) {
   return best_w;
 }
 
-// Warps per block chosen by a caller's autotuner per (slots NS, copies P, policy, FP32 fields); 0 = occupancy
-// heuristic.  Process-wide, set through arp_anneal_tune.
-static int g_tuned_warps[5][7][2][2];
+// Warps per block chosen by a caller's autotuner per (slots NS, copies P, policy: first accept, Chord round, warm
+// first accept, FP32 fields); 0 = occupancy heuristic.  Process-wide, set through arp_anneal_tune.
+static int g_tuned_warps[5][7][3][2];
 
 template <int NS, int P, bool CHORD, bool FLT, bool WARM = false, bool ENG = false, bool LAT = false>
 static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
@@ -755,7 +755,7 @@ static cudaError_t launch_ns_p(const DDParams& a, int warps, cudaStream_t st) {
     sms = sl.sms;
     if (warps <= 0) {
       warps = sl.cached_w;
-      const int tw = g_tuned_warps[NS][P][CHORD ? 1 : 0][FLT ? 1 : 0];
+      const int tw = g_tuned_warps[NS][P][WARM ? 2 : (CHORD ? 1 : 0)][FLT ? 1 : 0];
       if (tw > 0 && tw != warps) {  // same resident warps per SM, another width
         per_sm = sl.cached_nb * sl.cached_w / tw > 0 ? sl.cached_nb * sl.cached_w / tw : 1;
         warps = tw;
@@ -1029,8 +1029,8 @@ static cudaError_t launch_mixed(MixedArgs& g, int Dmax, int warps, int* counter,
 }
 
 extern "C" int arp_anneal_tune(int D, int P, int policy, int precision, int warps) {
-  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || (policy != 0 && policy != 1) ||
-      (precision != 0 && precision != 1))
+  if (D < 1 || D > 128 || !(P == 2 || P == 4 || P == 6) || policy < 0 || policy > 2 ||
+      (precision != 0 && precision != 1) || (policy == 2 && (P != 2 || precision != 0)))
     return ARP_ERR_SHAPE;
   if (!(warps == 0 || warps == 1 || warps == 2 || warps == 4 || warps == 8)) return ARP_ERR_ARG;
   g_tuned_warps[(D + 31) / 32][P][policy][precision] = warps;

@@ -179,8 +179,8 @@ class WarmDetector(Detector):
     anneal from the plain MMSE start ('bal') in index order.  With tau set, anneal 0 starts from the argmax and
     every other warm anneal draws its start from softmax(tau z) of the network's logits (a different start per
     anneal, from the anneal's own Philox counters).  With conf_min also set, problems whose kept start has
-    confidence sum_j log max_c p_jc above conf_min run only r_easy anneals (default: one per warp of the anneal's
-    block, 8), the others all R.  With mlp=None it is the plain MMSE-started detector that also records the
+    confidence sum_j log max_c p_jc above conf_min run only r_easy anneals (default 8), the others all R, and the
+    warm anneal's blocks are r_easy warps wide (the largest power of two up to 8), so an easy problem fills one.  With mlp=None it is the plain MMSE-started detector that also records the
     features' inputs (used to make training labels)."""
 
     def __init__(self, B, nt, nr=None, M=16, anneals=32, sweeps=None, mlp=None, T0=None, T1=None, q=None,
@@ -205,6 +205,13 @@ class WarmDetector(Detector):
             raise ValueError('per-problem anneal counts need the sampled start (tau)')
         self.conf_min, self.r_easy = conf_min, min(r_easy, anneals)
         self.ra = torch.full((B,), anneals, dtype=torch.int32, device=dev) if conf_min is not None else None
+        if self.ra is not None:
+            # an easy problem's anneals fill its block: the warm anneal runs blocks of the largest power of two
+            # <= r_easy warps (at most 8; arp_anneal_tune, per coordinate-slot count, results unchanged)
+            w = 1
+            while w * 2 <= min(self.r_easy, 8):
+                w *= 2
+            _lib.check(_lib.lib().arp_anneal_tune(self.D, 2, 2, 0, w), 'anneal_tune')
 
     def set_noise(self, snr_db=None, N0=None, n=None):
         super().set_noise(snr_db, N0, n)

@@ -224,8 +224,9 @@ int arp_soft_trajectory(const float* J, const float* hf, const float* h0, const 
 
 /* Autotuner hook (no reference counterpart): warps per block (1, 2, 4 or 8; 0 restores the occupancy heuristic)
  * of the compressed-problem anneal kernels for problems of D coordinates (by 32-wide slot count), P copies,
- * policy (0 first accept, incl. the warm variant; 1 Chord round) and precision (0 int32, 1 FP32 fields).
- * Process-wide; results do not depend on it (anneals are independent of their block). */
+ * policy (0 first accept, 1 Chord round, 2 the warm-started first accept of arp_anneal_first_accept_warm*, P = 2
+ * and int32 only) and precision (0 int32, 1 FP32 fields).  Process-wide; results do not depend on it (anneals are
+ * independent of their block). */
 int arp_anneal_tune(int D, int P, int policy, int precision, int warps);
 
 /* One size class of a mixed batch for arp_anneal_first_accept_mixed: the arguments of arp_anneal_first_accept for

@@ -68,6 +68,10 @@ def test_host_rejects_bad_shapes_without_gpu():
                                                  f.ctypes.data, done.ctypes.data))
     assert L.arp_serve_run(ok, 1, None, 0, 1.0, None) == 3
     assert L.arp_serve_run(None, 0, None, 0, 1.0, None) == 0
+    # the autotuner hook: policy 2 (the warm-started first accept) exists for P = 2, int32 only
+    assert L.arp_anneal_tune(64, 4, 2, 0, 4) == 1 and L.arp_anneal_tune(64, 2, 2, 1, 4) == 1
+    assert L.arp_anneal_tune(64, 2, 3, 0, 4) == 1 and L.arp_anneal_tune(64, 2, 2, 0, 3) == 3
+    assert L.arp_anneal_tune(64, 2, 2, 0, 4) == 0 and L.arp_anneal_tune(64, 2, 2, 0, 0) == 0
 
 
 def test_draw_matches_reference(golden):

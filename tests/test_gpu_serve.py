@@ -50,20 +50,22 @@ def test_each_result_is_the_same_alone_and_in_the_mix(warm_start, slots, burst):
             assert float(dist[0]) == float(st['dist'][i]), (cls, i)
 
 
-def test_native_loop_equals_the_python_loop():
+@pytest.mark.parametrize('slots,burst', [(64, False), (256, True)])
+def test_native_loop_equals_the_python_loop(slots, burst):
     """The library's loop (arp_serve_run) and this module's step() loop give every request the same bits and
-    distance, and both finish every request."""
+    distance, and both finish every request: Poisson arrivals (small batches), and one burst that the library
+    loop takes in batches up to 256 (its graphs beyond 64 uses)."""
     from arpeggio_b200 import serve
-    streams = _streams(200, 9)
+    streams = _streams(200 if not burst else 600, 9, burst)
     res = {}
     for native in (True, False):
-        srv = serve.Server(CLASSES, anneals=8, sweeps=8, slots=64, inflight=2, hbm_budget=1 << 30)
+        srv = serve.Server(CLASSES, anneals=8, sweeps=8, slots=slots, inflight=2, hbm_budget=1 << 30)
         for cls, (H, y, N0, t, rid) in streams.items():
             srv.open(cls, H, y, N0, t, rid)
         stats = srv.serve(native=native)
         for cls in streams:
             st = srv.streams[cls]
-            assert stats['%dx%d %d-QAM' % cls]['requests'] == 200
+            assert stats['%dx%d %d-QAM' % cls]['requests'] == (200 if not burst else 600)
             assert not np.isnan(st['done']).any()
         res[native] = {cls: (srv.streams[cls]['bits'].clone(), srv.streams[cls]['dist'].clone()) for cls in streams}
         del srv
